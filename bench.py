@@ -1,0 +1,361 @@
+"""Benchmark: 30-qubit random brickwork circuit (complex64, depth 20) on one B200.
+
+Metric (lower is better): circuit seconds of the tensor-core + learned-fusion plan, with the
+plain GPU paths (unfused, greedy-fused on CUDA cores at k=2..6) measured beside it and the
+infidelity 1-F of the result against an FP64 (complex128) run of the same circuit.
+
+A step = one execution of the circuit from |0..0> (init + every sweep) on a resident 8 GiB state
+(larger than L2, so no flush is needed). Timing: CUDA events on the engine's stream, W warm-up
+steps, K timed steps bracketed by barrier + synchronize, max over ranks. With N GPUs every rank
+runs its own replica (the single-state path does not shard): value = max step time / N.
+
+``--impl reference`` times the CPU restatement of qsv's CpuBackend (OpenMP over all host cores)
+on a bounded sample of the same workload and extrapolates to the full circuit.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "30q circuit sec: TC+learned fusion vs plain GPU at 1-F<=1e-5; HBM GB/s/peak"
+N_QUBITS, DEPTH, SEED = 30, 20, 0
+WORKLOAD = f"random brickwork {N_QUBITS}q depth {DEPTH}, complex64, Haar SU(2) + CZ, seed {SEED}"
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# ------------------------------------------------------------------ clocks sampling
+class ClockSampler:
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax = float(parts[1])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[4:8]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ CPU baseline (oracle CpuBackend)
+def cpu_baseline(circuit, budget_s: float = 15.0) -> dict:
+    """Time the CpuBackend restatement (OpenMP, all host threads) on the reference-fused circuit
+    (FusionConfig default max_qubits=4, composed in f32 as qsv does for Circuit<f32>); run ops
+    until the time budget is spent and extrapolate to the whole circuit."""
+    import oracle
+    from rustatevec_b200.circuit import Circuit
+    n = circuit.n_qubits()
+    arity, qubits, mats = oracle.fuse(circuit, 4, oracle.F32)
+    nops = len(arity)
+    L = oracle.lib()
+    cores = int(L.orc_max_threads())
+    re = np.zeros(1 << n, dtype=np.float32)
+    im = np.zeros(1 << n, dtype=np.float32)
+    re[0] = 1.0
+    offs_q = np.concatenate([[0], np.cumsum(arity)]).astype(np.int64)
+    offs_m = np.concatenate([[0], np.cumsum([2 * (1 << (2 * int(m))) for m in arity])]).astype(np.int64)
+
+    def run_op(i):
+        m = int(arity[i])
+        L.orc_apply(oracle.CPU_PARALLEL, oracle.F32, n, re.ctypes.data, im.ctypes.data,
+                    np.ascontiguousarray(mats[offs_m[i]:offs_m[i + 1]]),
+                    np.ascontiguousarray(qubits[offs_q[i]:offs_q[i + 1]]), m)
+
+    run_op(0)  # first touch of the pages, untimed
+    t0 = time.perf_counter()
+    done = 0
+    for i in range(1, nops):
+        run_op(i)
+        done += 1
+        if time.perf_counter() - t0 > budget_s:
+            break
+    dt = time.perf_counter() - t0
+    per_op = dt / max(done, 1)
+    return {"value": per_op * nops, "unit": "s", "cores": cores, "kind": "port",
+            "sample": f"{done} of {nops} fused ops (qsv fuse, max_qubits=4, f32) of the {n}q circuit timed "
+                      f"({dt:.1f} s, OpenMP x{cores}); value = mean per op x {nops} ops"}
+
+
+# ------------------------------------------------------------------ GPU
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def allreduce_max(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def run_gpu(args):
+    import torch
+    from rustatevec_b200 import (B200Backend, Plan, PLAN_AS_GIVEN, PLAN_GREEDY, PLAN_LEARNED, PLAN_WINDOW,
+                                 ENGINE_AUTO, ENGINE_CUDA_CORE, ENGINE_TENSOR_CORE)
+    from rustatevec_b200 import _lib as L
+    from rustatevec_b200.circuits import brickwork
+
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    be = B200Backend(local, precision="f32")
+    stream = torch.cuda.ExternalStream(be.stream(), device=torch.device("cuda", local))
+    circuit = brickwork(N_QUBITS, DEPTH, SEED)
+    state = be.alloc(N_QUBITS)
+
+    def timed(plan, steps, warmup):
+        for _ in range(warmup):
+            be.init_basis(state, 0)
+            plan.run(state)
+        be.synchronize()
+        barrier(world)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            be.init_basis(state, 0)
+            plan.run(state)
+        e1.record(stream)
+        e1.synchronize()
+        torch.cuda.synchronize()
+        barrier(world)
+        return e0.elapsed_time(e1) * 1e-3 / steps
+
+    methods = {
+        "unfused": L.make_opts(PLAN_AS_GIVEN, 1, ENGINE_CUDA_CORE),
+        **{f"greedy_k{k}_cuda": L.make_opts(PLAN_GREEDY, k, ENGINE_CUDA_CORE) for k in (2, 3, 4, 5, 6)},
+        "window_k4_cuda": L.make_opts(PLAN_WINDOW, 4, ENGINE_CUDA_CORE),
+        "learned_cuda": L.make_opts(PLAN_LEARNED, 6, ENGINE_CUDA_CORE),
+        "greedy_k6_tc": L.make_opts(PLAN_GREEDY, 6, ENGINE_TENSOR_CORE),
+        "learned_tc": L.make_opts(PLAN_LEARNED, 6, ENGINE_AUTO),
+    }
+    headline = "learned_tc"
+    results = {}
+    plans = {}
+    for name, o in methods.items():
+        p = Plan(be, circuit, o)
+        plans[name] = p
+        if name == headline or args.quick:
+            continue
+        t = timed(p, steps=2, warmup=1)
+        st = p.stats()
+        results[name] = {"seconds": allreduce_max(t, world), "sweeps": st["n_sweeps"], "by_kind": st["by_kind"]}
+
+    hp = plans[headline]
+    clocks = ClockSampler(local)
+    clocks.start()
+    t_step = timed(hp, args.steps, args.warmup)
+    clk = clocks.stop()
+    t_step = allreduce_max(t_step, world)
+    hst = hp.stats()
+    results[headline] = {"seconds": t_step, "sweeps": hst["n_sweeps"], "by_kind": hst["by_kind"]}
+
+    out = None
+    if rank == 0:
+        plain = {k: v["seconds"] for k, v in results.items() if k.endswith("_cuda") or k == "unfused"}
+        best_plain = min(plain.items(), key=lambda kv: kv[1]) if plain else (None, None)
+
+        # fidelity of the headline state against an FP64 run of the same circuit
+        be.init_basis(state, 0)
+        hp.run(state)
+        be64 = B200Backend(local, precision="f64")
+        s64 = be64.alloc(N_QUBITS)
+        be64.init_basis(s64, 0)
+        be64.run(s64, circuit, L.make_opts(PLAN_GREEDY, 4, ENGINE_CUDA_CORE))
+        be64.synchronize()
+        ip = np.zeros(2)
+        import ctypes as C
+        L.check(L.lib().qsvb_inner_product(be.ctx, state.handle, s64.handle, ip.ctypes.data_as(L._dp)))
+        n32 = be.norm_sqr(state)
+        fid = (ip[0] ** 2 + ip[1] ** 2) / n32
+        s64.free()
+        be64.close()
+
+        # roofline of the dominant kernel: per-sweep device times of the headline plan
+        sweeps = hp.sweeps()
+        per = hp.profile(state, reps=2)
+        by_kind = {}
+        for s, t in zip(sweeps, per):
+            d = by_kind.setdefault(s["kind"], {"time": 0.0, "bytes": 0.0, "flops": 0.0, "launches": 0})
+            d["time"] += t
+            d["bytes"] += s["algorithmic_bytes"]
+            d["flops"] += s["flops"]
+            d["launches"] += 1
+        dom = max(by_kind, key=lambda k: by_kind[k]["time"])
+        d = by_kind[dom]
+        peak, peak_kind = peaks()
+        achieved = d["bytes"] / d["time"] / 1e9
+        roofline = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak,
+                    "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": None,
+                    "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback",
+                    "avg_launch_us": round(d["time"] / d["launches"] * 1e6, 1),
+                    "algorithmic_bytes_per_launch": d["bytes"] / d["launches"],
+                    "share_of_step": round(d["time"] / max(sum(v["time"] for v in by_kind.values()), 1e-30), 3),
+                    "by_kind": {k: {"launches": v["launches"], "seconds": round(v["time"], 5),
+                                    "GB/s": round(v["bytes"] / v["time"] / 1e9, 1) if v["time"] else None}
+                                for k, v in by_kind.items()}}
+
+        # end to end through the public API: host circuit -> execute -> <Z_0> back on the host
+        e2e_steps = max(2, min(args.steps, 4))
+        pc_bytes = sum(2 * 8 * (1 << (2 * len(op.qubits))) for op in circuit.ops())
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        be.synchronize()
+        e0.record(stream)
+        for _ in range(e2e_steps):
+            be.init_basis(state, 0)
+            be.run(state, circuit, methods[headline])
+            _ = be.expectation_z(state, 1)
+        e1.record(stream)
+        e1.synchronize()
+        e2e = e0.elapsed_time(e1) * 1e-3 / e2e_steps
+
+        cpu = cpu_baseline(circuit, budget_s=args.cpu_budget) if not args.no_cpu else None
+        n_launch = args.steps * (hst["n_sweeps"] + 1)
+        out = {
+            "metric": METRIC, "value": round(t_step / world, 6), "unit": "s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(t_step * 1e3, 3),
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 state (complex64); k>=5 dense sweeps on tcgen05 bf16 hi/lo, fp32 accumulate",
+            "data": "synthetic (seeded brickwork circuit)",
+            "config": {"workload": WORKLOAD, "n_qubits": N_QUBITS, "depth": DEPTH, "gates": len(circuit),
+                       "plan": headline, "plan_sweeps": hst["n_sweeps"], "plan_by_kind": hst["by_kind"],
+                       "l2": "state is 8 GiB (> 126 MB L2): no flush needed",
+                       "parallelism": "replicas" if world > 1 else "single GPU"},
+            "infidelity_vs_fp64": float(1.0 - fid),
+            "methods_seconds": {k: round(v["seconds"], 5) for k, v in results.items()},
+            "methods_sweeps": {k: v["sweeps"] for k, v in results.items()},
+            "best_plain_gpu": {"method": best_plain[0], "seconds": best_plain[1],
+                               "speedup_of_headline": (best_plain[1] / t_step) if best_plain[1] else None},
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "e2e": {"value": round(e2e, 6), "unit": "s", "h2d_bytes_per_step": pc_bytes, "d2h_bytes_per_step": 16,
+                    "path": "B200Backend.run(host circuit) -> qsvb_execute (plan + matrix upload + graph) -> "
+                            "expectation_z(mask=1) read back"},
+            "gpu_launches": n_launch,
+            "clocks": clk,
+        }
+        print(json.dumps(out), flush=True)
+    state.free()
+    be.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def run_reference(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from rustatevec_b200.circuits import brickwork
+    circuit = brickwork(N_QUBITS, DEPTH, SEED)
+    vals = []
+    last = None
+    for i in range(args.warmup + args.steps):
+        r = cpu_baseline(circuit, budget_s=args.ref_budget)
+        if i >= args.warmup:
+            vals.append(r["value"])
+        last = r
+    v = float(np.mean(vals))
+    out = {"impl": "reference", "metric": METRIC, "value": round(v, 3), "unit": "s", "n_gpus": world,
+           "steps": args.steps, "warmup": args.warmup, "higher_is_better": False, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f32 (complex64)", "data": "synthetic (seeded brickwork circuit)",
+           "config": {"workload": WORKLOAD, "n_qubits": N_QUBITS, "depth": DEPTH},
+           "cpu_baseline": {"value": round(v, 3), "unit": "s", "cores": last["cores"], "kind": last["kind"],
+                            "sample": last["sample"]},
+           "e2e": {"value": round(v, 3), "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--quick", action="store_true", help="headline plan only")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-budget", type=float, default=15.0)
+    ap.add_argument("--ref-budget", type=float, default=6.0)
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_gpu(args)
+
+
+if __name__ == "__main__":
+    main()

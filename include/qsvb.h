@@ -1,0 +1,193 @@
+/* qsvb.h — C ABI of the B200 statevector engine (libqsvb.so).
+ *
+ * This is the drop-in boundary for qsv's `Backend<R>` trait
+ * (crates/qsv-core/src/backend/mod.rs:31-74). A thin host shim (Rust `impl Backend<f32>` /
+ * `impl Backend<f64>`, or the Python mirror in rustatevec_b200/backend.py) forwards each trait
+ * method to one call below and turns a non-zero status into the trait's panic.
+ *
+ * Conventions
+ *  - Every entry point returns an `int` status: QSVB_OK (0) or a negative QSVB_E_* code. No C++
+ *    exception crosses this boundary. qsvb_last_error() returns the message of the calling
+ *    thread's most recent failure.
+ *  - States are opaque handles owned by the caller (alloc/free). Pointers passed in are borrowed
+ *    for the duration of the call.
+ *  - Work is queued on the context's CUDA stream. Calls that return data to the host
+ *    (download, probabilities, amplitude, reductions) synchronize that stream first.
+ *  - Gate convention (crates/qsv-core/src/gate.rs:8-13): bit j of a gate's row/column index is
+ *    state bit qubits[j]; controlled gates list the control first.
+ *  - Matrices are row-major 2^m x 2^m, complex as interleaved (re, im) FP64. A complex64 state
+ *    rounds them to f32 on use (the rounding of Cplx::from_f64); fused gates are composed in FP64.
+ *  - A context is not thread-safe: use one context per host thread.
+ */
+#ifndef QSVB_H
+#define QSVB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define QSVB_OK 0
+#define QSVB_E_INVALID -1     /* bad argument: qubit out of range, repeated qubit, arity, null */
+#define QSVB_E_CUDA -2        /* a CUDA runtime/driver call failed */
+#define QSVB_E_OOM -3         /* device memory exhausted */
+#define QSVB_E_UNSUPPORTED -4 /* valid request this build cannot serve */
+#define QSVB_E_TIMEOUT -5     /* a bounded device-side wait ran out (persistent runner) */
+
+#define QSVB_MAX_GATE_QUBITS 6
+#define QSVB_MAX_QUBITS 34
+
+typedef enum qsvb_dtype { QSVB_C64 = 0, QSVB_C128 = 1 } qsvb_dtype;
+
+typedef struct qsvb_ctx qsvb_ctx;
+typedef struct qsvb_state qsvb_state;
+typedef struct qsvb_plan qsvb_plan;
+
+/* One gate application (crates/qsv-core/src/circuit.rs:13-16 GateOp). */
+typedef struct qsvb_gate {
+  uint32_t n_qubits;                       /* m, 1..6 */
+  uint32_t qubits[QSVB_MAX_GATE_QUBITS];   /* gate order; entries >= m are ignored */
+  const double* matrix;                    /* 2^m x 2^m, row-major, interleaved (re, im) */
+} qsvb_gate;
+
+/* A circuit (crates/qsv-core/src/circuit.rs:31-34). */
+typedef struct qsvb_circuit {
+  uint32_t n_qubits;
+  size_t n_gates;
+  const qsvb_gate* gates;
+} qsvb_circuit;
+
+/* Planner choices for qsvb_execute / qsvb_plan_create. */
+typedef enum qsvb_planner {
+  QSVB_PLAN_AS_GIVEN = 0, /* one sweep per gate, in order (the trait's default execute loop) */
+  QSVB_PLAN_GREEDY = 1,   /* qsv fuse semantics (fusion.rs:39-77), composition in FP64 */
+  QSVB_PLAN_WINDOW = 2,   /* commutation-aware windows: gates on disjoint qubits reorder */
+  QSVB_PLAN_LEARNED = 3   /* cost-model planner (MLP cost model; greedy fallback) */
+} qsvb_planner;
+
+typedef enum qsvb_engine {
+  QSVB_ENGINE_AUTO = 0,        /* tensor cores for k>=5 complex64 sweeps, CUDA cores otherwise */
+  QSVB_ENGINE_CUDA_CORE = 1,   /* all dense sweeps on CUDA cores (FP32 / FP64) */
+  QSVB_ENGINE_TENSOR_CORE = 2  /* dense complex64 sweeps with k>=4 on tcgen05 (BF16 hi/lo) */
+} qsvb_engine;
+
+typedef struct qsvb_plan_opts {
+  uint32_t planner;          /* qsvb_planner */
+  uint32_t max_fused_qubits; /* fusion width cap, 1..6 (ignored by AS_GIVEN) */
+  uint32_t engine;           /* qsvb_engine */
+  uint32_t use_graph;        /* capture the sweep sequence in a CUDA graph */
+  uint32_t reserved[4];
+} qsvb_plan_opts;
+
+/* What a plan does, for reports and rooflines. */
+typedef struct qsvb_plan_stats {
+  uint64_t n_gates_in;        /* gates in the input circuit */
+  uint64_t n_sweeps;          /* kernel sweeps launched per run */
+  uint64_t n_sweeps_by_kind[8]; /* 1q, ctrl1q, diag, phase, dense CUDA-core, dense TC, swap, other */
+  double algorithmic_bytes;   /* sum over sweeps of 2 * (amplitudes the sweep may change) * bytes/amp */
+  double full_sweep_bytes;    /* sum over sweeps of 2 * 2^n * bytes/amp */
+  double flops;               /* complex-MAC flops of the dense sweeps (8 * 2^k per amplitude) */
+  double predicted_seconds;   /* planner's cost-model estimate */
+} qsvb_plan_stats;
+
+/* ---------------------------------------------------------------- lifecycle */
+/* Backend construction (crates/qsv-cuda/src/lib.rs:57-77 CudaBackend::new). */
+int qsvb_create(int device_ordinal, qsvb_ctx** out);
+int qsvb_destroy(qsvb_ctx* ctx);
+const char* qsvb_last_error(void);
+int qsvb_synchronize(qsvb_ctx* ctx);
+/* Library version string, e.g. "qsvb 0.1 sm_100a". */
+const char* qsvb_version(void);
+/* The context's CUDA stream (a cudaStream_t), so callers can order their own work and record
+ * CUDA events against the engine's queue. */
+int qsvb_stream(qsvb_ctx* ctx, void** stream_out);
+
+/* Backend::alloc (mod.rs:36; lib.rs:100-107). Contents unspecified until init/upload. */
+int qsvb_state_alloc(qsvb_ctx* ctx, uint32_t n_qubits, int dtype, qsvb_state** out);
+int qsvb_state_free(qsvb_ctx* ctx, qsvb_state* st);
+/* Shape of a state and its device SoA pointers (re[2^n], im[2^n]). */
+int qsvb_state_info(const qsvb_state* st, uint32_t* n_qubits, int* dtype, void** d_re, void** d_im);
+
+/* ---------------------------------------------------------------- state preparation */
+/* Backend::init_basis (mod.rs:39; lib.rs:109-119). */
+int qsvb_init_basis(qsvb_ctx* ctx, qsvb_state* st, uint64_t basis);
+/* Arbitrary-state upload from host SoA arrays in the state's precision (no trait counterpart). */
+int qsvb_upload(qsvb_ctx* ctx, qsvb_state* st, const void* re, const void* im);
+/* Seeded i.i.d. complex Gaussian amplitudes normalised in FP64 (no trait counterpart). */
+int qsvb_init_gaussian(qsvb_ctx* ctx, qsvb_state* st, uint64_t seed);
+
+/* ---------------------------------------------------------------- gate application */
+/* Backend::apply (mod.rs:42; lib.rs:121-200): one gate, dispatched to a fast path. */
+int qsvb_apply(qsvb_ctx* ctx, qsvb_state* st, const double* matrix, const uint32_t* qubits,
+               uint32_t n_qubits);
+/* Backend::execute (mod.rs:66-73) on an initialised state: plans, uploads matrices once, and
+ * queues every sweep (as one CUDA graph when opts->use_graph). opts may be NULL (greedy, k=4,
+ * auto engine, graph on). stats may be NULL. */
+int qsvb_execute(qsvb_ctx* ctx, qsvb_state* st, const qsvb_circuit* circuit,
+                 const qsvb_plan_opts* opts, qsvb_plan_stats* stats);
+
+/* Reusable plans: plan once, run many times (the graph is instantiated on first run). */
+int qsvb_plan_create(qsvb_ctx* ctx, const qsvb_circuit* circuit, int dtype,
+                     const qsvb_plan_opts* opts, qsvb_plan** out);
+int qsvb_plan_run(qsvb_ctx* ctx, qsvb_plan* plan, qsvb_state* st);
+int qsvb_plan_stats_get(const qsvb_plan* plan, qsvb_plan_stats* out);
+int qsvb_plan_free(qsvb_ctx* ctx, qsvb_plan* plan);
+
+/* One sweep of a plan, as the planner and the cost model see it. */
+typedef struct qsvb_sweep_info {
+  uint32_t kind;                  /* 0 1q, 1 ctrl1q, 2 diag, 3 phase, 4 dense CUDA-core, 5 dense TC */
+  uint32_t n_qubits;              /* matrix qubits (dense/diag) */
+  uint32_t qubits[QSVB_MAX_GATE_QUBITS];
+  uint32_t target;                /* butterflies */
+  uint32_t n_ctrl;                /* controls (ctrl1q) or skipped identity halves (diag) */
+  uint32_t ctrl[QSVB_MAX_GATE_QUBITS];
+  uint32_t n_terms;               /* phase polynomial terms */
+  uint64_t n_gates;               /* input gates this sweep covers */
+  double algorithmic_bytes;       /* 2 * (amplitudes it may change) * bytes per amplitude */
+  double flops;                   /* 8 * 2^k per amplitude for dense sweeps */
+  float features[16];             /* cost-model input vector */
+} qsvb_sweep_info;
+int qsvb_plan_sweep_info(const qsvb_plan* plan, size_t index, qsvb_sweep_info* out);
+/* Device time of each sweep of `plan` on `st`: CUDA events around `reps` back-to-back launches of
+ * each sweep; out_seconds[i] = mean seconds per launch of sweep i. The state is overwritten. */
+int qsvb_plan_profile(qsvb_ctx* ctx, qsvb_plan* plan, qsvb_state* st, int reps, double* out_seconds);
+/* Fused gate list a planner produces (crates/qsv-core/src/fusion.rs:39 fuse). Call with
+ * out_gates == NULL to get the count in *n_out; matrices are written to out_mats (FP64
+ * interleaved) with out_gates[i].matrix pointing into it. Needs no device. */
+int qsvb_fuse(const qsvb_circuit* circuit, const qsvb_plan_opts* opts, qsvb_gate* out_gates,
+              size_t* n_out, double* out_mats, size_t out_mats_cap);
+
+/* ---------------------------------------------------------------- read-out */
+/* Backend::download (mod.rs:62; lib.rs:218-227): SoA copy into host buffers of the state's
+ * precision. */
+int qsvb_download(qsvb_ctx* ctx, const qsvb_state* st, void* re, void* im);
+/* Backend::amplitude (mod.rs:45): one element (not the whole state as lib.rs:202-205 does). */
+int qsvb_amplitude(qsvb_ctx* ctx, const qsvb_state* st, uint64_t index, double out[2]);
+/* Backend::probabilities (mod.rs:48; lib.rs:207-216 k_abs2). |psi_i|^2 computed in FP64;
+ * written to host `out` as f64 (out_dtype QSVB_C128) or rounded to f32 (QSVB_C64). */
+int qsvb_probabilities(qsvb_ctx* ctx, const qsvb_state* st, void* out, int out_dtype);
+/* Backend::expectation_z (mod.rs:57-59; sample.rs:177-200), FP64 on device. */
+int qsvb_expectation_z(qsvb_ctx* ctx, const qsvb_state* st, uint64_t mask, double* out);
+/* StateVector::norm_sqr (crates/qsv-core/src/state/mod.rs:112-118), FP64 on device. */
+int qsvb_norm_sqr(qsvb_ctx* ctx, const qsvb_state* st, double* out);
+/* <a|b> in FP64 (no trait counterpart). a and b may differ in precision (complex64 vs complex128),
+ * which is how a complex64 run is scored against its FP64 twin. */
+int qsvb_inner_product(qsvb_ctx* ctx, const qsvb_state* a, const qsvb_state* b, double out[2]);
+/* |<a|b>|^2 in FP64 (no trait counterpart). */
+int qsvb_fidelity(qsvb_ctx* ctx, const qsvb_state* a, const qsvb_state* b, double* out);
+
+/* ---------------------------------------------------------------- batched circuits */
+/* Many small independent circuits (each n <= 20) in one persistent kernel. For circuit i the
+ * engine writes <Z_0> to z0_out[i] and, when probs_out != NULL, its 2^n_i FP64 probabilities
+ * at probs_out + probs_offset[i] (host memory; offsets supplied by the caller). Each circuit
+ * starts from |0..0>. No trait counterpart. */
+int qsvb_execute_batch(qsvb_ctx* ctx, const qsvb_circuit* circuits, size_t n_circuits, int dtype,
+                       double* z0_out, double* probs_out, const uint64_t* probs_offset,
+                       qsvb_plan_stats* stats);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* QSVB_H */

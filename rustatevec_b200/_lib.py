@@ -1,0 +1,175 @@
+"""ctypes binding of libqsvb.so (the C ABI declared in include/qsvb.h).
+
+The shared library is built in-tree (``rustatevec_b200/libqsvb.so``) by
+``__graft_entry__.build()`` / ``make -C rustatevec_b200/csrc``. There is no fallback: if the
+library is missing or fails to load, importing the backend raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libqsvb.so")
+
+QSVB_OK = 0
+QSVB_E_INVALID = -1
+QSVB_E_CUDA = -2
+QSVB_E_OOM = -3
+QSVB_E_UNSUPPORTED = -4
+QSVB_E_TIMEOUT = -5
+
+C64, C128 = 0, 1
+PLAN_AS_GIVEN, PLAN_GREEDY, PLAN_WINDOW, PLAN_LEARNED = 0, 1, 2, 3
+ENGINE_AUTO, ENGINE_CUDA_CORE, ENGINE_TENSOR_CORE = 0, 1, 2
+MAX_GATE_QUBITS = 6
+
+SWEEP_KINDS = ("1q", "ctrl1q", "diag", "phase", "dense", "dense_tc", "swap", "other")
+
+
+class QsvbError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"qsvb error {code}: {msg}")
+        self.code = code
+
+
+class Gate(C.Structure):
+    _fields_ = [("n_qubits", C.c_uint32), ("qubits", C.c_uint32 * MAX_GATE_QUBITS),
+                ("matrix", C.POINTER(C.c_double))]
+
+
+class CircuitS(C.Structure):
+    _fields_ = [("n_qubits", C.c_uint32), ("n_gates", C.c_size_t), ("gates", C.POINTER(Gate))]
+
+
+class PlanOpts(C.Structure):
+    _fields_ = [("planner", C.c_uint32), ("max_fused_qubits", C.c_uint32), ("engine", C.c_uint32),
+                ("use_graph", C.c_uint32), ("reserved", C.c_uint32 * 4)]
+
+
+class PlanStats(C.Structure):
+    _fields_ = [("n_gates_in", C.c_uint64), ("n_sweeps", C.c_uint64),
+                ("n_sweeps_by_kind", C.c_uint64 * 8), ("algorithmic_bytes", C.c_double),
+                ("full_sweep_bytes", C.c_double), ("flops", C.c_double),
+                ("predicted_seconds", C.c_double)]
+
+    def to_dict(self) -> dict:
+        return {
+            "n_gates_in": int(self.n_gates_in), "n_sweeps": int(self.n_sweeps),
+            "by_kind": {k: int(v) for k, v in zip(SWEEP_KINDS, self.n_sweeps_by_kind) if v},
+            "algorithmic_bytes": float(self.algorithmic_bytes),
+            "full_sweep_bytes": float(self.full_sweep_bytes), "flops": float(self.flops),
+            "predicted_seconds": float(self.predicted_seconds),
+        }
+
+
+class SweepInfo(C.Structure):
+    _fields_ = [("kind", C.c_uint32), ("n_qubits", C.c_uint32), ("qubits", C.c_uint32 * MAX_GATE_QUBITS),
+                ("target", C.c_uint32), ("n_ctrl", C.c_uint32), ("ctrl", C.c_uint32 * MAX_GATE_QUBITS),
+                ("n_terms", C.c_uint32), ("n_gates", C.c_uint64), ("algorithmic_bytes", C.c_double),
+                ("flops", C.c_double), ("features", C.c_float * 16)]
+
+    def to_dict(self) -> dict:
+        return {"kind": SWEEP_KINDS[self.kind], "k": int(self.n_qubits),
+                "qubits": [int(self.qubits[j]) for j in range(self.n_qubits)],
+                "target": int(self.target), "ctrl": [int(self.ctrl[j]) for j in range(self.n_ctrl)],
+                "n_terms": int(self.n_terms), "n_gates": int(self.n_gates),
+                "algorithmic_bytes": float(self.algorithmic_bytes), "flops": float(self.flops),
+                "features": [float(x) for x in self.features]}
+
+
+# Every exported symbol, with (restype, argtypes). Kept in the order of include/qsvb.h.
+_vp, _u32, _u64, _i, _sz, _d = C.c_void_p, C.c_uint32, C.c_uint64, C.c_int, C.c_size_t, C.c_double
+_dp = C.POINTER(C.c_double)
+SIGNATURES = {
+    "qsvb_create": (_i, [_i, C.POINTER(_vp)]),
+    "qsvb_destroy": (_i, [_vp]),
+    "qsvb_last_error": (C.c_char_p, []),
+    "qsvb_synchronize": (_i, [_vp]),
+    "qsvb_version": (C.c_char_p, []),
+    "qsvb_stream": (_i, [_vp, C.POINTER(_vp)]),
+    "qsvb_state_alloc": (_i, [_vp, _u32, _i, C.POINTER(_vp)]),
+    "qsvb_state_free": (_i, [_vp, _vp]),
+    "qsvb_state_info": (_i, [_vp, C.POINTER(_u32), C.POINTER(_i), C.POINTER(_vp), C.POINTER(_vp)]),
+    "qsvb_init_basis": (_i, [_vp, _vp, _u64]),
+    "qsvb_upload": (_i, [_vp, _vp, _vp, _vp]),
+    "qsvb_init_gaussian": (_i, [_vp, _vp, _u64]),
+    "qsvb_apply": (_i, [_vp, _vp, _dp, C.POINTER(_u32), _u32]),
+    "qsvb_execute": (_i, [_vp, _vp, C.POINTER(CircuitS), C.POINTER(PlanOpts), C.POINTER(PlanStats)]),
+    "qsvb_plan_create": (_i, [_vp, C.POINTER(CircuitS), _i, C.POINTER(PlanOpts), C.POINTER(_vp)]),
+    "qsvb_plan_run": (_i, [_vp, _vp, _vp]),
+    "qsvb_plan_stats_get": (_i, [_vp, C.POINTER(PlanStats)]),
+    "qsvb_plan_free": (_i, [_vp, _vp]),
+    "qsvb_plan_sweep_info": (_i, [_vp, _sz, C.c_void_p]),
+    "qsvb_plan_profile": (_i, [_vp, _vp, _vp, _i, _dp]),
+    "qsvb_fuse": (_i, [C.POINTER(CircuitS), C.POINTER(PlanOpts), C.POINTER(Gate), C.POINTER(_sz), _dp, _sz]),
+    "qsvb_download": (_i, [_vp, _vp, _vp, _vp]),
+    "qsvb_amplitude": (_i, [_vp, _vp, _u64, _dp]),
+    "qsvb_probabilities": (_i, [_vp, _vp, _vp, _i]),
+    "qsvb_expectation_z": (_i, [_vp, _vp, _u64, _dp]),
+    "qsvb_norm_sqr": (_i, [_vp, _vp, _dp]),
+    "qsvb_inner_product": (_i, [_vp, _vp, _vp, _dp]),
+    "qsvb_fidelity": (_i, [_vp, _vp, _vp, _dp]),
+    "qsvb_execute_batch": (_i, [_vp, C.POINTER(CircuitS), _sz, _i, _dp, _dp, C.POINTER(_u64),
+                                C.POINTER(PlanStats)]),
+}
+
+_lib = None
+
+
+def lib():
+    """Load libqsvb.so (once). Raises if it is missing: there is no CPU fallback."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: build it with `make -C rustatevec_b200/csrc` "
+                              "(or __graft_entry__.build())")
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name, None)
+            if fn is None:
+                continue
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(rc: int):
+    if rc != QSVB_OK:
+        raise QsvbError(rc, lib().qsvb_last_error().decode(errors="replace"))
+
+
+class PackedCircuit:
+    """A circuit packed into the C structs; keeps the matrix buffer alive."""
+
+    def __init__(self, circuit):
+        arity, qubits, mats = circuit.flatten()
+        self.mats = np.ascontiguousarray(mats, dtype=np.float64)
+        n = len(arity)
+        self.gates = (Gate * max(n, 1))()
+        base = self.mats.ctypes.data
+        qo = mo = 0
+        for i, m in enumerate(arity.tolist()):
+            g = self.gates[i]
+            g.n_qubits = m
+            for j in range(m):
+                g.qubits[j] = int(qubits[qo + j])
+            g.matrix = C.cast(base + 8 * mo, _dp)
+            qo += m
+            mo += 2 * (1 << (2 * m))
+        self.struct = CircuitS(circuit.n_qubits(), n, C.cast(self.gates, C.POINTER(Gate)))
+
+    def ref(self):
+        return C.byref(self.struct)
+
+
+def make_opts(planner=PLAN_GREEDY, max_fused_qubits=4, engine=ENGINE_AUTO, use_graph=True) -> PlanOpts:
+    o = PlanOpts()
+    o.planner = planner
+    o.max_fused_qubits = max_fused_qubits
+    o.engine = engine
+    o.use_graph = 1 if use_graph else 0
+    return o

@@ -1,0 +1,145 @@
+// Sweep cost model and the learned planner (see cost_model.h).
+
+#include "cost_model.h"
+
+#include <algorithm>
+#include <cmath>
+#include <mutex>
+
+namespace qsvb {
+
+namespace {
+std::mutex g_model_mu;
+MlpModel g_model;
+
+// Roofline constants for one B200 (measured copy bandwidth ~6.5 TB/s; sustained fractions).
+constexpr double kHbmBytesPerSec = 6.0e12;
+constexpr double kFp32FmaFlops = 40.0e12;   // CUDA-core complex GEMM, achieved
+constexpr double kFp64FmaFlops = 25.0e12;
+constexpr double kTcFlops = 1.2e15;         // bf16 tcgen05, achieved
+constexpr double kLaunchSeconds = 2.5e-6;
+
+int lowest_bit(const Sweep& s) {
+  uint32_t lo = 64;
+  for (uint32_t j = 0; j < s.m; ++j) lo = std::min(lo, s.q[j]);
+  if (s.kind == SK_1Q || s.kind == SK_CTRL) lo = s.target;
+  return int(lo);
+}
+}  // namespace
+
+void sweep_features(const Sweep& s, uint32_t n, int dtype, float* f) {
+  std::fill(f, f + kNumFeatures, 0.0f);
+  const int kind = std::min<int>(s.kind, 6);
+  f[kind] = 1.0f;                                    // 0..6 one-hot kind
+  f[7] = float(n);
+  f[8] = dtype == QSVB_C128 ? 1.0f : 0.0f;
+  uint32_t k = s.m;
+  if (s.kind == SK_1Q || s.kind == SK_CTRL) k = 1 + s.nctrl;
+  if (s.kind == SK_PHASE) k = 0;
+  f[9] = float(k);
+  f[10] = float(s.nctrl);
+  int lo = lowest_bit(s), hi = 0;
+  for (uint32_t j = 0; j < s.m; ++j) hi = std::max<int>(hi, int(s.q[j]));
+  if (s.kind == SK_1Q || s.kind == SK_CTRL) hi = std::max<int>(hi, int(s.target));
+  f[11] = float(std::min(lo, 40));
+  f[12] = float(hi);
+  f[13] = float(s.terms.size()) / 16.0f;
+  uint32_t nlow = 0;
+  for (uint32_t j = 0; j < s.m; ++j) nlow += s.q[j] < 7;
+  f[14] = float(nlow);
+  f[15] = float(std::log2(analytic_sweep_seconds(s, n, dtype)));
+}
+
+double analytic_sweep_seconds(const Sweep& s, uint32_t n, int dtype) {
+  const double b = dtype == QSVB_C128 ? 16.0 : 8.0;
+  const double dim = std::ldexp(1.0, int(n));
+  double amps = dim;
+  const int sector_bits = dtype == QSVB_C128 ? 2 : 3;  // a 32-byte sector holds 2^bits amplitudes
+  uint32_t skip = 0;
+  for (uint32_t i = 0; i < s.nctrl; ++i) skip += int(s.ctrl[i]) >= sector_bits;
+  if (s.kind == SK_CTRL || s.kind == SK_DIAG) amps = std::ldexp(dim, -int(skip));
+  double mem = 2.0 * amps * b / kHbmBytesPerSec;
+  double comp = 0.0;
+  if (s.kind == SK_DENSE)
+    comp = 8.0 * std::ldexp(1.0, int(s.m)) * dim / (dtype == QSVB_C128 ? kFp64FmaFlops : kFp32FmaFlops);
+  if (s.kind == SK_DENSE_TC) comp = 3.0 * 8.0 * std::ldexp(1.0, int(s.m)) * dim / kTcFlops;
+  if (s.kind == SK_PHASE) comp = double(s.terms.size()) * 4.0 * dim / 30.0e12 + 40.0 * dim / kFp64FmaFlops;
+  return std::max(mem, comp) + kLaunchSeconds;
+}
+
+const MlpModel& installed_model() { return g_model; }
+
+void install_model(const MlpModel& m) {
+  std::lock_guard<std::mutex> lk(g_model_mu);
+  g_model = m;
+}
+
+float mlp_forward_host(const MlpModel& m, const float* feat) {
+  const int H = m.hidden;
+  std::vector<float> x(kNumFeatures), h1(H), h2(H);
+  for (int i = 0; i < kNumFeatures; ++i) x[i] = (feat[i] - m.mean[i]) * m.scale[i];
+  for (int j = 0; j < H; ++j) {
+    float a = m.b1[j];
+    for (int i = 0; i < kNumFeatures; ++i) a += m.w1[j * kNumFeatures + i] * x[i];
+    h1[j] = a > 0 ? a : 0;
+  }
+  for (int j = 0; j < H; ++j) {
+    float a = m.b2[j];
+    for (int i = 0; i < H; ++i) a += m.w2[j * H + i] * h1[i];
+    h2[j] = a > 0 ? a : 0;
+  }
+  float y = m.b3[0];
+  for (int i = 0; i < H; ++i) y += m.w3[i] * h2[i];
+  return y * m.y_scale + m.y_mean;
+}
+
+double predict_sweep_seconds(const Sweep& s, uint32_t n, int dtype) {
+  const MlpModel& m = g_model;
+  if (m.hidden > 0) {
+    float f[kNumFeatures];
+    sweep_features(s, n, dtype, f);
+    return std::exp2(double(mlp_forward_host(m, f)));
+  }
+  return analytic_sweep_seconds(s, n, dtype);
+}
+
+double predict_plan_seconds(const std::vector<Sweep>& sw, uint32_t n, int dtype) {
+  double t = 0;
+  for (const Sweep& s : sw) t += predict_sweep_seconds(s, n, dtype);
+  return t;
+}
+
+void select_engines(std::vector<Sweep>& sw, uint32_t n, const qsvb_plan_opts& o, int dtype) {
+  for (Sweep& s : sw) {
+    if (s.kind != SK_DENSE) continue;
+    const bool want_tc = dtype == QSVB_C64 && ((o.engine == QSVB_ENGINE_TENSOR_CORE && s.m >= 4) ||
+                                               (o.engine == QSVB_ENGINE_AUTO && s.m >= 5));
+    if (want_tc && tc_dense_supported(s, n)) s.kind = SK_DENSE_TC;
+  }
+}
+
+std::vector<Gate> learned_fuse(const std::vector<Gate>& seg, uint32_t n, const qsvb_plan_opts& o, int dtype) {
+  std::vector<Gate> best;
+  double best_t = 1e300;
+  const uint32_t cap = std::max<uint32_t>(1, o.max_fused_qubits);
+  for (int strategy = 0; strategy < 2; ++strategy) {
+    for (uint32_t k = 1; k <= cap; ++k) {
+      std::vector<Gate> cand = strategy == 0 ? fuse_greedy_public(seg, k) : fuse_window_public(seg, k);
+      std::vector<Sweep> sw;
+      sw.reserve(cand.size());
+      for (const Gate& g : cand) {
+        Sweep s = classify_gate(g);
+        if (s.kind != SK_NONE) sw.push_back(std::move(s));
+      }
+      select_engines(sw, n, o, dtype);
+      const double t = predict_plan_seconds(sw, n, dtype);
+      if (t < best_t) {
+        best_t = t;
+        best = std::move(cand);
+      }
+    }
+  }
+  return best;
+}
+
+}  // namespace qsvb

@@ -1,0 +1,370 @@
+// Host planner: input gates -> fused gates -> classified sweeps.
+//
+// * GREEDY follows qsv's fuse (crates/qsv-core/src/fusion.rs:39-100): consecutive-only grouping
+//   while the union of qubits stays <= max; single-gate groups pass through unchanged, larger
+//   groups are composed onto their sorted qubit set (fusion.rs:102-140). Composition here is FP64
+//   whatever the state precision.
+// * WINDOW grows each group past gates it cannot absorb, as long as every absorbed gate acts on
+//   qubits disjoint from all gates it jumps over (such gates commute, so the result is exact).
+// * LEARNED picks, per circuit, the cheapest of the candidate plans under the cost model
+//   (cost_model.cpp); GREEDY at the requested width is always among the candidates.
+// * Runs of >= 3 consecutive diagonal gates of <= 2 qubits whose qubit union exceeds the fusion
+//   width become one phase-polynomial sweep (WINDOW and LEARNED).
+//
+// classify_gate mirrors the dispatch of qsv's CudaBackend::apply / CpuBackend::apply
+// (crates/qsv-cuda/src/lib.rs:121-200, crates/qsv-core/src/backend/cpu.rs:281-290): diagonal ->
+// diagonal sweep, one qubit -> butterfly, else dense, with one addition: a gate that is the
+// identity whenever some of its qubits are 0 and a 2x2 on the one remaining qubit is a controlled
+// butterfly that only visits the control=1 subspace.
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+
+#include "cost_model.h"
+#include "qsvb_internal.h"
+
+namespace qsvb {
+
+qsvb_plan_opts default_opts() {
+  qsvb_plan_opts o{};
+  o.planner = QSVB_PLAN_GREEDY;
+  o.max_fused_qubits = 4;
+  o.engine = QSVB_ENGINE_AUTO;
+  o.use_graph = 1;
+  return o;
+}
+
+void validate_circuit(const qsvb_circuit* c) {
+  QSVB_REQUIRE(c != nullptr, "null circuit");
+  QSVB_REQUIRE(c->n_qubits >= 1 && c->n_qubits <= QSVB_MAX_QUBITS, "circuit qubit count out of range");
+  QSVB_REQUIRE(c->n_gates == 0 || c->gates != nullptr, "null gate array");
+  for (size_t i = 0; i < c->n_gates; ++i) {
+    const qsvb_gate& g = c->gates[i];
+    QSVB_REQUIRE(g.n_qubits >= 1 && g.n_qubits <= QSVB_MAX_GATE_QUBITS,
+                 "gate " + std::to_string(i) + ": arity must be 1..6");
+    QSVB_REQUIRE(g.n_qubits <= c->n_qubits, "gate " + std::to_string(i) + ": more qubits than the register");
+    QSVB_REQUIRE(g.matrix != nullptr, "gate " + std::to_string(i) + ": null matrix");
+    for (uint32_t j = 0; j < g.n_qubits; ++j) {
+      QSVB_REQUIRE(g.qubits[j] < c->n_qubits, "gate " + std::to_string(i) + ": qubit " +
+                                                  std::to_string(g.qubits[j]) + " out of range for " +
+                                                  std::to_string(c->n_qubits) + " qubits");
+      for (uint32_t k = j + 1; k < g.n_qubits; ++k)
+        QSVB_REQUIRE(g.qubits[j] != g.qubits[k], "gate " + std::to_string(i) + ": repeated qubit in gate");
+    }
+  }
+}
+
+std::vector<Gate> gates_from_circuit(const qsvb_circuit* c) {
+  std::vector<Gate> out(c->n_gates);
+  for (size_t i = 0; i < c->n_gates; ++i) {
+    const qsvb_gate& g = c->gates[i];
+    Gate& o = out[i];
+    o.m = g.n_qubits;
+    for (uint32_t j = 0; j < o.m; ++j) o.q[j] = g.qubits[j];
+    const size_t d = size_t(1) << o.m;
+    o.a.resize(d * d);
+    for (size_t k = 0; k < d * d; ++k) o.a[k] = cd(g.matrix[2 * k], g.matrix[2 * k + 1]);
+  }
+  return out;
+}
+
+namespace {
+
+uint64_t qmask(const Gate& g) {
+  uint64_t m = 0;
+  for (uint32_t j = 0; j < g.m; ++j) m |= 1ull << g.q[j];
+  return m;
+}
+
+bool is_diag(const Gate& g) {
+  const size_t d = size_t(1) << g.m;
+  for (size_t r = 0; r < d; ++r)
+    for (size_t c = 0; c < d; ++c)
+      if (r != c && g.a[r * d + c] != cd(0.0, 0.0)) return false;
+  return true;
+}
+
+// Compose `ops` (applied in order) onto the sorted qubit list `q` in FP64: new = E(g) * mat, the
+// embedding qsv's build_fused uses (fusion.rs:102-140).
+Gate compose(const std::vector<uint32_t>& q, const std::vector<const Gate*>& ops) {
+  const size_t m = q.size(), dim = size_t(1) << m;
+  std::vector<cd> mat(dim * dim, cd(0, 0)), nw(dim * dim);
+  for (size_t i = 0; i < dim; ++i) mat[i * dim + i] = cd(1, 0);
+  for (const Gate* g : ops) {
+    uint32_t local[6];
+    for (uint32_t j = 0; j < g->m; ++j)
+      local[j] = uint32_t(std::find(q.begin(), q.end(), g->q[j]) - q.begin());
+    const size_t nsub = size_t(1) << g->m, gd = nsub;
+    std::fill(nw.begin(), nw.end(), cd(0, 0));
+    for (size_t r = 0; r < dim; ++r) {
+      size_t rs = 0;
+      for (uint32_t j = 0; j < g->m; ++j) rs |= ((r >> local[j]) & 1u) << j;
+      for (size_t ks = 0; ks < nsub; ++ks) {
+        const cd e = g->a[rs * gd + ks];
+        if (e == cd(0, 0)) continue;
+        size_t k = r;
+        for (uint32_t j = 0; j < g->m; ++j) k = (k & ~(size_t(1) << local[j])) | (((ks >> j) & 1u) << local[j]);
+        const cd* src = &mat[k * dim];
+        cd* dst = &nw[r * dim];
+        for (size_t c = 0; c < dim; ++c) dst[c] += e * src[c];
+      }
+    }
+    mat.swap(nw);
+  }
+  Gate out;
+  out.m = uint32_t(m);
+  for (size_t j = 0; j < m; ++j) out.q[j] = q[j];
+  out.a = std::move(mat);
+  return out;
+}
+
+void emit_group(std::vector<Gate>& out, const std::vector<const Gate*>& grp) {
+  if (grp.empty()) return;
+  if (grp.size() == 1) {
+    out.push_back(*grp[0]);
+    return;
+  }
+  uint64_t mask = 0;
+  for (const Gate* g : grp) mask |= qmask(*g);
+  std::vector<uint32_t> q;
+  for (uint32_t b = 0; b < 64; ++b)
+    if ((mask >> b) & 1) q.push_back(b);
+  out.push_back(compose(q, grp));
+}
+
+// fusion.rs:39-77 — consecutive-only greedy.
+std::vector<Gate> fuse_greedy(const std::vector<Gate>& in, uint32_t maxq) {
+  maxq = std::max<uint32_t>(maxq, 1);
+  std::vector<Gate> out;
+  std::vector<const Gate*> grp;
+  std::vector<uint32_t> gq;  // insertion order, as the reference keeps it
+  for (const Gate& g : in) {
+    if (g.m > maxq) {
+      emit_group(out, grp);
+      grp.clear();
+      gq.clear();
+      out.push_back(g);
+      continue;
+    }
+    std::vector<uint32_t> uni = gq;
+    for (uint32_t j = 0; j < g.m; ++j)
+      if (std::find(uni.begin(), uni.end(), g.q[j]) == uni.end()) uni.push_back(g.q[j]);
+    if (grp.empty()) {
+      gq.assign(g.q, g.q + g.m);
+      grp.push_back(&g);
+    } else if (uni.size() <= maxq) {
+      gq = uni;
+      grp.push_back(&g);
+    } else {
+      emit_group(out, grp);
+      grp.clear();
+      gq.assign(g.q, g.q + g.m);
+      grp.push_back(&g);
+    }
+  }
+  emit_group(out, grp);
+  return out;
+}
+
+// Commutation-aware window fusion: a later gate may join the open group when its qubits are
+// disjoint from every not-yet-emitted gate it would jump over.
+std::vector<Gate> fuse_window(const std::vector<Gate>& in, uint32_t maxq, size_t lookahead = 1024) {
+  maxq = std::max<uint32_t>(maxq, 1);
+  std::vector<char> done(in.size(), 0);
+  std::vector<Gate> out;
+  size_t first = 0;
+  std::vector<const Gate*> grp;
+  while (true) {
+    while (first < in.size() && done[first]) ++first;
+    if (first == in.size()) break;
+    done[first] = 1;
+    const Gate& g0 = in[first];
+    if (g0.m > maxq) {
+      out.push_back(g0);
+      continue;
+    }
+    grp.assign(1, &g0);
+    uint64_t gmask = qmask(g0), blocked = 0;
+    size_t scanned = 0;
+    for (size_t i = first + 1; i < in.size() && scanned < lookahead; ++i) {
+      if (done[i]) continue;
+      ++scanned;
+      const uint64_t m = qmask(in[i]);
+      if ((m & blocked) == 0 && uint32_t(__builtin_popcountll(gmask | m)) <= maxq) {
+        grp.push_back(&in[i]);
+        done[i] = 1;
+        gmask |= m;
+      } else {
+        blocked |= m;
+        // nothing can join once every qubit of a full group is blocked
+        if (uint32_t(__builtin_popcountll(gmask)) == maxq && (gmask & ~blocked) == 0) break;
+      }
+    }
+    emit_group(out, grp);
+  }
+  return out;
+}
+
+bool phase_representable(const Gate& g) {
+  if (g.m > 2 || !is_diag(g)) return false;
+  const size_t d = size_t(1) << g.m;
+  for (size_t i = 0; i < d; ++i)
+    if (std::abs(std::abs(g.a[i * d + i]) - 1.0) > 1e-12) return false;
+  return true;
+}
+
+}  // namespace
+
+std::vector<Gate> fuse_greedy_public(const std::vector<Gate>& in, uint32_t maxq) { return fuse_greedy(in, maxq); }
+std::vector<Gate> fuse_window_public(const std::vector<Gate>& in, uint32_t maxq) { return fuse_window(in, maxq); }
+
+std::vector<Gate> fuse_gates(const std::vector<Gate>& in, uint32_t n, const qsvb_plan_opts& o, int dtype) {
+  (void)n;
+  (void)dtype;
+  switch (o.planner) {
+    case QSVB_PLAN_AS_GIVEN: return in;
+    case QSVB_PLAN_GREEDY: return fuse_greedy(in, o.max_fused_qubits);
+    case QSVB_PLAN_WINDOW: return fuse_window(in, o.max_fused_qubits);
+    default: return fuse_window(in, o.max_fused_qubits);
+  }
+}
+
+Sweep classify_gate(const Gate& g) {
+  Sweep s;
+  s.m = g.m;
+  for (uint32_t j = 0; j < g.m; ++j) s.q[j] = g.q[j];
+  s.n_gates = 1;
+  const size_t d = size_t(1) << g.m;
+  auto at = [&](size_t r, size_t c) { return g.a[r * d + c]; };
+  if (is_diag(g)) {
+    bool ident = true;
+    for (size_t i = 0; i < d; ++i) ident = ident && at(i, i) == cd(1, 0);
+    if (ident) {
+      s.kind = SK_NONE;
+      return s;
+    }
+    s.kind = SK_DIAG;
+    s.mat.resize(d);
+    for (size_t i = 0; i < d; ++i) s.mat[i] = at(i, i);
+    for (uint32_t j = 0; j < g.m; ++j) {  // qubit j is skippable when its 0-half is all ones
+      bool ok = true;
+      for (size_t i = 0; i < d && ok; ++i)
+        if (((i >> j) & 1) == 0 && at(i, i) != cd(1, 0)) ok = false;
+      if (ok) s.ctrl[s.nctrl++] = g.q[j];
+    }
+    return s;
+  }
+  if (g.m == 1) {
+    s.kind = SK_1Q;
+    s.target = g.q[0];
+    s.mat = {at(0, 0), at(0, 1), at(1, 0), at(1, 1)};
+    return s;
+  }
+  // control detection: qubit j is a control when the gate is the identity on its 0-half and
+  // never mixes its 0- and 1-halves
+  uint32_t ctrl_local = 0;
+  for (uint32_t j = 0; j < g.m; ++j) {
+    bool ok = true;
+    for (size_t r = 0; r < d && ok; ++r)
+      for (size_t c = 0; c < d && ok; ++c) {
+        const size_t rb = (r >> j) & 1, cb = (c >> j) & 1;
+        if (rb != cb) ok = at(r, c) == cd(0, 0);
+        else if (rb == 0) ok = at(r, c) == (r == c ? cd(1, 0) : cd(0, 0));
+      }
+    if (ok) ctrl_local |= 1u << j;
+  }
+  if (__builtin_popcount(ctrl_local) == int(g.m) - 1) {
+    uint32_t tl = 0;
+    while ((ctrl_local >> tl) & 1) ++tl;
+    s.kind = SK_CTRL;
+    s.target = g.q[tl];
+    for (uint32_t j = 0; j < g.m; ++j)
+      if ((ctrl_local >> j) & 1) s.ctrl[s.nctrl++] = g.q[j];
+    const size_t r0 = ctrl_local, r1 = ctrl_local | (size_t(1) << tl);
+    s.mat = {at(r0, r0), at(r0, r1), at(r1, r0), at(r1, r1)};
+    return s;
+  }
+  s.kind = SK_DENSE;
+  s.mat = g.a;
+  return s;
+}
+
+std::vector<Sweep> plan_sweeps(const std::vector<Gate>& in, uint32_t n, const qsvb_plan_opts& o0, int dtype) {
+  qsvb_plan_opts o = o0;
+  if (o.max_fused_qubits == 0) o.max_fused_qubits = 1;
+  o.max_fused_qubits = std::min<uint32_t>(o.max_fused_qubits, std::min<uint32_t>(QSVB_MAX_GATE_QUBITS, n));
+  const bool phase_runs = o.planner == QSVB_PLAN_WINDOW || o.planner == QSVB_PLAN_LEARNED;
+
+  // split into segments: phase-polynomial runs vs ordinary gates
+  std::vector<Sweep> out;
+  auto run_segment = [&](const std::vector<Gate>& seg) {
+    if (seg.empty()) return;
+    std::vector<Gate> fused;
+    if (o.planner == QSVB_PLAN_LEARNED) fused = learned_fuse(seg, n, o, dtype);
+    else fused = fuse_gates(seg, n, o, dtype);
+    for (const Gate& g : fused) {
+      Sweep s = classify_gate(g);
+      if (s.kind == SK_NONE) continue;
+      out.push_back(std::move(s));
+    }
+  };
+  std::vector<Gate> seg;
+  size_t i = 0;
+  while (i < in.size()) {
+    if (phase_runs && phase_representable(in[i])) {
+      size_t j = i;
+      uint64_t mask = 0;
+      while (j < in.size() && phase_representable(in[j])) mask |= qmask(in[j++]);
+      if (j - i >= 3 && uint32_t(__builtin_popcountll(mask)) > o.max_fused_qubits) {
+        run_segment(seg);
+        seg.clear();
+        Sweep s;
+        s.kind = SK_PHASE;
+        s.n_gates = j - i;
+        for (size_t k = i; k < j; ++k) {
+          const Gate& g = in[k];
+          PhaseTerm t{};
+          t.m = g.m;
+          for (uint32_t a = 0; a < g.m; ++a) t.q[a] = g.q[a];
+          const size_t d = size_t(1) << g.m;
+          for (size_t e = 0; e < 4; ++e) t.ang[e] = e < d ? std::arg(g.a[e * d + e]) : 0.0;
+          s.terms.push_back(t);
+        }
+        out.push_back(std::move(s));
+        i = j;
+        continue;
+      }
+      for (size_t k = i; k < j; ++k) seg.push_back(in[k]);
+      i = j;
+      continue;
+    }
+    seg.push_back(in[i++]);
+  }
+  run_segment(seg);
+
+  select_engines(out, n, o, dtype);
+  return out;
+}
+
+void sweep_costs(const std::vector<Sweep>& sw, uint32_t n, int dtype, qsvb_plan_stats* st) {
+  const double b = dtype == QSVB_C128 ? 16.0 : 8.0;
+  const double dim = std::ldexp(1.0, int(n));
+  st->n_sweeps = sw.size();
+  for (auto& k : st->n_sweeps_by_kind) k = 0;
+  st->algorithmic_bytes = st->full_sweep_bytes = st->flops = 0;
+  for (const Sweep& s : sw) {
+    int kind = s.kind;
+    st->n_sweeps_by_kind[kind < 8 ? kind : 7]++;
+    double amps = dim;
+    if (s.kind == SK_CTRL) amps = std::ldexp(dim, -int(s.nctrl));
+    if (s.kind == SK_DIAG) amps = std::ldexp(dim, -int(s.nctrl));
+    st->algorithmic_bytes += 2.0 * amps * b;
+    st->full_sweep_bytes += 2.0 * dim * b;
+    if (s.kind == SK_DENSE || s.kind == SK_DENSE_TC) st->flops += 8.0 * std::ldexp(1.0, int(s.m)) * dim;
+  }
+  st->predicted_seconds = predict_plan_seconds(sw, n, dtype);
+}
+
+}  // namespace qsvb

@@ -1,0 +1,163 @@
+// Internal declarations shared by the qsvb translation units (not part of the C ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <complex>
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/qsvb.h"
+
+namespace qsvb {
+
+using cd = std::complex<double>;
+
+// ------------------------------------------------------------------ errors
+struct Error : std::runtime_error {
+  int code;
+  Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+[[noreturn]] void throw_cuda(cudaError_t e, const char* what, const char* file, int line);
+#define QSVB_CK(x)                                                        \
+  do {                                                                    \
+    cudaError_t _qe = (x);                                                \
+    if (_qe != cudaSuccess) ::qsvb::throw_cuda(_qe, #x, __FILE__, __LINE__); \
+  } while (0)
+#define QSVB_REQUIRE(cond, msg)                                 \
+  do {                                                          \
+    if (!(cond)) throw ::qsvb::Error(QSVB_E_INVALID, (msg));    \
+  } while (0)
+
+// ------------------------------------------------------------------ sweeps (planner output)
+// A sweep is one pass of one kernel over the state.
+enum SweepKind : int {
+  SK_1Q = 0,        // dense 2x2 on one target
+  SK_CTRL = 1,      // 2x2 on one target, only where all control bits are 1 (half/quarter skip)
+  SK_DIAG = 2,      // diagonal table over <= 6 qubits; "skip" qubits whose 0-half is identity
+  SK_PHASE = 3,     // phase polynomial: product of many <= 2-qubit diagonal terms
+  SK_DENSE = 4,     // dense 2^k x 2^k on CUDA cores
+  SK_DENSE_TC = 5,  // dense 2^k x 2^k on tcgen05 tensor cores (complex64 only)
+  SK_SWAP = 6,      // reserved
+  SK_NONE = 7       // identity (dropped)
+};
+
+struct PhaseTerm {
+  uint32_t m;         // 1 or 2 qubits
+  uint32_t q[2];
+  double ang[4];      // phase angle per sub-index (bit j <-> q[j])
+};
+
+struct Sweep {
+  SweepKind kind = SK_NONE;
+  uint32_t m = 0;                 // qubits of the matrix (dense/diag), gate order
+  uint32_t q[6] = {0, 0, 0, 0, 0, 0};
+  std::vector<cd> mat;            // dense: row-major; diag: the diagonal; 1q/ctrl: 2x2
+  uint32_t target = 0;            // 1q / ctrl
+  uint32_t nctrl = 0;
+  uint32_t ctrl[6] = {0, 0, 0, 0, 0, 0};
+  std::vector<PhaseTerm> terms;   // phase polynomial
+  uint64_t n_gates = 0;           // input gates covered
+};
+
+struct Gate {  // host copy of an input gate, FP64
+  uint32_t m = 0;
+  uint32_t q[6] = {0, 0, 0, 0, 0, 0};
+  std::vector<cd> a;  // row-major 2^m x 2^m
+};
+
+std::vector<Gate> gates_from_circuit(const qsvb_circuit* c);
+void validate_circuit(const qsvb_circuit* c);
+
+// Planner entry: input gates -> fused gate list (greedy/window/learned) -> classified sweeps.
+std::vector<Gate> fuse_gates(const std::vector<Gate>& in, uint32_t n_qubits, const qsvb_plan_opts& o,
+                             int dtype);
+std::vector<Sweep> plan_sweeps(const std::vector<Gate>& in, uint32_t n_qubits,
+                               const qsvb_plan_opts& o, int dtype);
+Sweep classify_gate(const Gate& g);
+void sweep_costs(const std::vector<Sweep>& sw, uint32_t n, int dtype, qsvb_plan_stats* st);
+qsvb_plan_opts default_opts();
+
+// ------------------------------------------------------------------ kernel launchers
+// All launchers enqueue on `s`; none synchronizes. `R` is float (complex64) or double.
+struct LaunchEnv {
+  cudaStream_t stream;
+  int num_sms;
+};
+
+template <class R> void launch_init_basis(const LaunchEnv& e, R* re, R* im, uint32_t n, uint64_t basis);
+template <class R> void launch_init_gaussian(const LaunchEnv& e, R* re, R* im, uint32_t n, uint64_t seed);
+template <class R> void launch_scale(const LaunchEnv& e, R* re, R* im, uint32_t n, const double* d_norm);
+
+// One sweep. `dev_mat` points to the sweep's device-side matrix block (dense kinds only) laid out
+// by pack_dense_matrix(); other kinds carry their coefficients by value.
+template <class R>
+void launch_sweep(const LaunchEnv& e, R* re, R* im, uint32_t n, const Sweep& s, const void* dev_mat);
+// Device bytes the sweep's matrix block needs (0 when the coefficients travel by value).
+size_t sweep_matrix_bytes(const Sweep& s, int dtype);
+void pack_sweep_matrix(const Sweep& s, int dtype, void* host_dst);
+
+// Reductions (FP64). `partials` holds >= reduce_partials_needed() doubles; results land in
+// d_out (2 doubles).
+size_t reduce_partials_needed(int num_sms);
+template <class R>
+void launch_reduce(const LaunchEnv& e, int op, const R* re, const R* im, const R* re2, const R* im2,
+                   uint32_t n, uint64_t mask, double* partials, double* d_out);
+enum ReduceOp { RED_NORM = 0, RED_EXPZ = 1, RED_INNER = 2 };
+template <class RA, class RB>
+void launch_inner_mixed(const LaunchEnv& e, const RA* are, const RA* aim, const RB* bre, const RB* bim, uint32_t n,
+                        double* partials, double* d_out);
+template <class R>
+void launch_probabilities(const LaunchEnv& e, const R* re, const R* im, uint64_t offset, uint64_t count,
+                          void* out, int out_f64);
+
+// Tensor-core dense sweep (complex64): implemented in tc_dense.cu.
+bool tc_dense_supported(const Sweep& s, uint32_t n);
+size_t tc_matrix_bytes(const Sweep& s);
+void tc_pack_matrix(const Sweep& s, void* host_dst);
+void launch_tc_dense(const LaunchEnv& e, float* re, float* im, uint32_t n, const Sweep& s,
+                     const void* dev_mat);
+
+}  // namespace qsvb
+
+// ------------------------------------------------------------------ C ABI objects
+struct qsvb_state {
+  uint32_t n_qubits;
+  int dtype;
+  int device;
+  void* re;
+  void* im;
+};
+
+struct qsvb_ctx {
+  int device = 0;
+  int num_sms = 148;
+  cudaStream_t stream = nullptr;
+  double* d_partials = nullptr;   // reduction partials
+  double* d_result = nullptr;     // 2 doubles
+  char* d_mat_ring = nullptr;     // per-apply matrix uploads
+  size_t mat_ring_cap = 0;
+  size_t mat_ring_pos = 0;
+  void* d_prob = nullptr;         // probability staging chunk
+  size_t prob_cap = 0;
+  qsvb::LaunchEnv env() const { return {stream, num_sms}; }
+};
+
+void run_batch(qsvb_ctx* c, const qsvb_circuit* circuits, size_t n_circuits, int dtype, double* z0_out,
+               double* probs_out, const uint64_t* probs_offset, qsvb_plan_stats* stats);
+
+struct qsvb_plan {
+  uint32_t n_qubits = 0;
+  int dtype = 0;
+  qsvb_plan_opts opts{};
+  std::vector<qsvb::Sweep> sweeps;
+  std::vector<size_t> mat_offset;   // byte offset of each sweep's matrix block in d_mats
+  char* d_mats = nullptr;
+  size_t mats_bytes = 0;
+  qsvb_plan_stats stats{};
+  cudaGraphExec_t graph = nullptr;
+  void* graph_re = nullptr;         // state the graph was captured for
+  void* graph_im = nullptr;
+};
