@@ -57,6 +57,18 @@ struct DeviceGuard {
 };
 
 void check_ctx(const qsvb_ctx* c) { QSVB_REQUIRE(c != nullptr, "null context"); }
+
+// Synchronize the context stream and surface a device-side bounded-wait timeout (the flag is
+// cleared so the context stays usable).
+void sync_and_check(qsvb_ctx* c) {
+  QSVB_CK(cudaStreamSynchronize(c->stream));
+  int flag = 0;
+  QSVB_CK(cudaMemcpy(&flag, c->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (flag) {
+    QSVB_CK(cudaMemset(c->d_err, 0, sizeof(int)));
+    throw Error(QSVB_E_TIMEOUT, "a device-side wait ran out of its iteration budget; results are invalid");
+  }
+}
 void check_state(const qsvb_ctx* c, const qsvb_state* s) {
   check_ctx(c);
   QSVB_REQUIRE(s != nullptr, "null state");
@@ -177,7 +189,7 @@ double reduce(qsvb_ctx* c, int op, const qsvb_state* a, const qsvb_state* b, uin
   });
   double h[2];
   QSVB_CK(cudaMemcpyAsync(h, c->d_result, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
-  QSVB_CK(cudaStreamSynchronize(c->stream));
+  sync_and_check(c);
   if (second) *second = h[1];
   return h[0];
 }
@@ -210,6 +222,8 @@ int qsvb_create(int device_ordinal, qsvb_ctx** out) {
     QSVB_CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
     QSVB_CK(cudaMalloc(&c->d_partials, reduce_partials_needed(c->num_sms) * sizeof(double)));
     QSVB_CK(cudaMalloc(&c->d_result, 2 * sizeof(double)));
+    QSVB_CK(cudaMalloc(&c->d_err, sizeof(int)));
+    QSVB_CK(cudaMemset(c->d_err, 0, sizeof(int)));
     *out = c.release();
   });
 }
@@ -223,6 +237,7 @@ int qsvb_destroy(qsvb_ctx* c) {
     if (c->d_result) cudaFree(c->d_result);
     if (c->d_mat_ring) cudaFree(c->d_mat_ring);
     if (c->d_prob) cudaFree(c->d_prob);
+    if (c->d_err) cudaFree(c->d_err);
     cudaStreamDestroy(c->stream);
     delete c;
   });
@@ -240,7 +255,7 @@ int qsvb_synchronize(qsvb_ctx* c) {
   return guarded([&] {
     check_ctx(c);
     DeviceGuard dg(c->device);
-    QSVB_CK(cudaStreamSynchronize(c->stream));
+    sync_and_check(c);
   });
 }
 
@@ -457,7 +472,7 @@ int qsvb_execute(qsvb_ctx* c, qsvb_state* s, const qsvb_circuit* circ, const qsv
     run_plan(c, p.get(), s);
     if (stats) *stats = p->stats;
     // the plan's device matrices and graph must outlive the queued work
-    QSVB_CK(cudaStreamSynchronize(c->stream));
+    sync_and_check(c);
   });
 }
 

@@ -286,8 +286,21 @@ Sweep classify_gate(const Gate& g) {
     s.mat = {at(r0, r0), at(r0, r1), at(r1, r0), at(r1, r1)};
     return s;
   }
+  // dense: canonical ascending qubit order (bit i of the index <-> i-th smallest qubit), so the
+  // kernels can rely on the gate's lowest qubits being the low bits of the sub-index
   s.kind = SK_DENSE;
-  s.mat = g.a;
+  uint32_t order[6];
+  for (uint32_t i = 0; i < g.m; ++i) order[i] = i;
+  std::sort(order, order + g.m, [&](uint32_t a, uint32_t b) { return g.q[a] < g.q[b]; });
+  for (uint32_t i = 0; i < g.m; ++i) s.q[i] = g.q[order[i]];
+  auto remap = [&](size_t sidx) {  // sorted-order index -> gate-order index
+    size_t o = 0;
+    for (uint32_t i = 0; i < g.m; ++i) o |= ((sidx >> i) & 1u) << order[i];
+    return o;
+  };
+  s.mat.resize(d * d);
+  for (size_t r = 0; r < d; ++r)
+    for (size_t c = 0; c < d; ++c) s.mat[r * d + c] = at(remap(r), remap(c));
   return s;
 }
 

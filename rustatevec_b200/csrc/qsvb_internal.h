@@ -85,6 +85,7 @@ qsvb_plan_opts default_opts();
 struct LaunchEnv {
   cudaStream_t stream;
   int num_sms;
+  int* err_flag;  // device flag a kernel sets when a bounded wait runs out
 };
 
 template <class R> void launch_init_basis(const LaunchEnv& e, R* re, R* im, uint32_t n, uint64_t basis);
@@ -142,7 +143,8 @@ struct qsvb_ctx {
   size_t mat_ring_pos = 0;
   void* d_prob = nullptr;         // probability staging chunk
   size_t prob_cap = 0;
-  qsvb::LaunchEnv env() const { return {stream, num_sms}; }
+  int* d_err = nullptr;           // device error flag (bounded waits)
+  qsvb::LaunchEnv env() const { return {stream, num_sms, d_err}; }
 };
 
 void run_batch(qsvb_ctx* c, const qsvb_circuit* circuits, size_t n_circuits, int dtype, double* z0_out,

@@ -229,8 +229,10 @@ def test_ghz24_chain_probabilities_c128(be64):
 
 def test_reductions(be):
     st = be.execute(ghz(5))
-    for mask, want in zip([1, 3, 15, 31], [0.0, 1.0, 1.0, 0.0]):  # sampling.rs:49-58
-        assert abs(be.expectation_z(st, mask) - want) < 1e-9
+    # sampling.rs:49-58 asserts 1e-9 on an f64 state; a complex64 state holds 1/sqrt(2) to 2^-24
+    tol = 1e-9 if be.precision == "f64" else 1e-6
+    for mask, want in zip([1, 3, 15, 31], [0.0, 1.0, 1.0, 0.0]):
+        assert abs(be.expectation_z(st, mask) - want) < tol
     c = random_circuit(12, 80, 77)
     a = be.execute(c)
     want = ref_state(c)

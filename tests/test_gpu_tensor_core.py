@@ -1,0 +1,106 @@
+"""Tensor-core (tcgen05, BF16 hi/lo split, FP32 accumulate) dense sweeps vs the FP64 oracle.
+
+Tolerances: one sweep keeps ~16 significant bits per product, so max |d amp| <= 1e-5 holds for
+complex64 states, and whole circuits stay within 1-F <= 1e-5 of the FP64 run."""
+import math
+
+import numpy as np
+import pytest
+
+import oracle
+from rustatevec_b200 import B200Backend, Plan, PLAN_AS_GIVEN, PLAN_LEARNED, PLAN_WINDOW, ENGINE_TENSOR_CORE
+from rustatevec_b200 import _lib as L
+from rustatevec_b200 import gate as G
+from rustatevec_b200.circuit import Circuit
+from rustatevec_b200.circuits import brickwork, random_circuit
+
+from helpers import infidelity, max_abs_diff
+
+pytestmark = pytest.mark.gpu
+
+
+def haar(k, seed):
+    rng = np.random.default_rng(seed)
+    z = (rng.normal(size=(1 << k, 1 << k)) + 1j * rng.normal(size=(1 << k, 1 << k))) / math.sqrt(2)
+    q, r = np.linalg.qr(z)
+    return q * (np.diag(r) / np.abs(np.diag(r)))
+
+
+def random_state(n, seed):
+    rng = np.random.default_rng(seed)
+    v = rng.normal(size=1 << n) + 1j * rng.normal(size=1 << n)
+    return v / np.linalg.norm(v)
+
+
+@pytest.fixture(scope="module")
+def be(built):
+    b = B200Backend(0, precision="f32")
+    yield b
+    b.close()
+
+
+def run_tc(be, c, psi, planner=PLAN_AS_GIVEN, k=6):
+    st = be.alloc(c.n_qubits())
+    be.upload(st, psi.real, psi.imag)
+    p = Plan(be, c, L.make_opts(planner, k, ENGINE_TENSOR_CORE))
+    p.run(st)
+    kinds = p.stats()["by_kind"]
+    return be.download(st).as_complex(), kinds
+
+
+QSETS = {
+    "high": lambda n, k: list(range(n - k, n)),           # B MN-major (state bits 0-1 are columns)
+    "low": lambda n, k: list(range(k)),                   # B K-major (gate owns bits 0-1)
+    "mid": lambda n, k: list(range(3, 3 + k)),
+    "mixed": lambda n, k: [0] + list(range(5, 4 + k)),    # scalar B stores (bit 0 gate, bit 1 column)
+    "mixed2": lambda n, k: [1] + list(range(7, 6 + k)),
+    "spread": lambda n, k: [2, 4, 7, 9, 11, 13][:k],
+    "unsorted": lambda n, k: list(reversed(range(n - k, n))),
+}
+
+
+@pytest.mark.parametrize("k", [4, 5, 6])
+@pytest.mark.parametrize("qset", sorted(QSETS))
+@pytest.mark.parametrize("n", [12, 15])
+def test_single_tc_sweep(be, k, qset, n):
+    qs = QSETS[qset](n, k)
+    psi = random_state(n, 100 * k + n)
+    c = Circuit(n)
+    c.push(G.DenseGate(k, haar(k, 7 * k + n)), qs)
+    got, kinds = run_tc(be, c, psi)
+    assert kinds.get("dense_tc", 0) == 1, kinds
+    re, im = oracle.run(c, oracle.REF, oracle.F64, state=(psi.real.copy(), psi.imag.copy()))
+    want = re + 1j * im
+    err = max_abs_diff(want, got)
+    assert err < 1e-5, (qset, k, n, err)
+    assert infidelity(want, got) < 1e-8
+
+
+@pytest.mark.parametrize("planner", [PLAN_WINDOW, PLAN_LEARNED])
+def test_tc_circuits_match_oracle(be, planner):
+    for seed in range(6):
+        n = 12 + seed % 4
+        c = random_circuit(n, 120, 31337 + seed)
+        psi = random_state(n, seed)
+        got, kinds = run_tc(be, c, psi, planner, 6)
+        re, im = oracle.run(c, oracle.REF, oracle.F64, state=(psi.real.copy(), psi.imag.copy()))
+        want = re + 1j * im
+        assert max_abs_diff(want, got) < 1e-5, (seed, kinds)
+        assert infidelity(want, got) < 1e-6
+
+
+def test_tc_brickwork_fidelity_vs_fp64(be, be64):
+    n = 20
+    c = brickwork(n, 20, 3)
+    st = be.alloc(n)
+    be.init_basis(st, 0)
+    p = Plan(be, c, L.make_opts(PLAN_LEARNED, 6, ENGINE_TENSOR_CORE))
+    p.run(st)
+    assert p.stats()["by_kind"].get("dense_tc", 0) > 0
+    ref = be64.alloc(n)
+    be64.init_basis(ref, 0)
+    be64.run(ref, c, L.make_opts(PLAN_AS_GIVEN, 1))
+    ip = np.zeros(2)
+    L.check(L.lib().qsvb_inner_product(be.ctx, st.handle, ref.handle, ip.ctypes.data_as(L._dp)))
+    fid = (ip[0] ** 2 + ip[1] ** 2) / be.norm_sqr(st)
+    assert 1.0 - fid < 1e-5, 1.0 - fid
