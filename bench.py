@@ -340,8 +340,75 @@ def run_reference(args):
     print(json.dumps(out), flush=True)
 
 
+KERNEL_CASES = {
+    # name: (precision, builder(n) -> circuit with one sweep of that kind, engine)
+    "1q_low": ("f32", lambda n: [("h", [1])]),
+    "1q_mid": ("f32", lambda n: [("h", [4])]),
+    "1q_high": ("f32", lambda n: [("h", [n - 1])]),
+    "cx_high": ("f32", lambda n: [("cx", [n - 1, n - 2])]),
+    "cz_high": ("f32", lambda n: [("cz", [n - 1, n - 2])]),
+    "dense4_cuda": ("f32", lambda n: [("u4", [0, 1, 2, 3])]),
+    "dense6_cuda": ("f32", lambda n: [("u6", list(range(6)))]),
+    "tc4": ("f32", lambda n: [("u4", [0, 1, 2, 3])]),
+    "tc6": ("f32", lambda n: [("u6", list(range(6)))]),
+    "tc6_high": ("f32", lambda n: [("u6", list(range(n - 6, n)))]),
+    "phase15": ("f32", lambda n: [("cz", [i, i + 1]) for i in range(0, n - 1, 2)]),
+    "1q_low_c128": ("f64", lambda n: [("h", [1])]),
+    "dense4_c128": ("f64", lambda n: [("u4", [0, 1, 2, 3])]),
+}
+
+
+def run_kernel_case(args):
+    """One sweep of one kernel, repeated: per-launch device time and achieved bandwidth."""
+    import torch
+    from rustatevec_b200 import (B200Backend, Plan, PLAN_AS_GIVEN, PLAN_LEARNED, ENGINE_CUDA_CORE,
+                                 ENGINE_TENSOR_CORE)
+    from rustatevec_b200 import _lib as L
+    from rustatevec_b200 import gate as G
+    from rustatevec_b200.circuit import Circuit
+    prec, build = KERNEL_CASES[args.kernel_case]
+    n = args.qubits
+    c = Circuit(n)
+    rng = np.random.default_rng(7)
+    for name, qs in build(n):
+        if name.startswith("u"):
+            k = int(name[1:])
+            z = rng.normal(size=(1 << k, 1 << k)) + 1j * rng.normal(size=(1 << k, 1 << k))
+            q, r = np.linalg.qr(z)
+            c.push(G.DenseGate(k, q), qs)
+        else:
+            c.push(G.LIBRARY[name](), qs)
+    engine = ENGINE_TENSOR_CORE if args.kernel_case.startswith("tc") else ENGINE_CUDA_CORE
+    planner = PLAN_LEARNED if args.kernel_case.startswith("phase") else PLAN_AS_GIVEN
+    be = B200Backend(0, precision=prec)
+    st = be.alloc(n)
+    be.init_basis(st, 0)
+    p = Plan(be, c, L.make_opts(planner, 2, engine, use_graph=False))
+    info = p.sweeps()
+    stream = torch.cuda.ExternalStream(be.stream())
+    for _ in range(2):
+        p.run(st)
+    be.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.reps):
+        p.run(st)
+    e1.record(stream)
+    e1.synchronize()
+    t = e0.elapsed_time(e1) * 1e-3 / args.reps
+    nbytes = sum(s["algorithmic_bytes"] for s in info)
+    peak, kind = peaks()
+    print(json.dumps({"kernel_case": args.kernel_case, "qubits": n, "precision": prec,
+                      "sweeps": [s["kind"] for s in info], "us_per_launch": round(t * 1e6, 2),
+                      "algorithmic_bytes": nbytes, "GB/s": round(nbytes / t / 1e9, 1),
+                      "frac_of_peak": round(nbytes / t / 1e9 / peak, 4), "peak": f"{peak} ({kind})"}))
+
+
 def main():
     ap = argparse.ArgumentParser()
+    ap.add_argument("--kernel-case", choices=sorted(KERNEL_CASES))
+    ap.add_argument("--qubits", type=int, default=30)
+    ap.add_argument("--reps", type=int, default=10)
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
@@ -351,7 +418,9 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--ref-budget", type=float, default=6.0)
     args = ap.parse_args()
-    if args.impl == "reference":
+    if args.kernel_case:
+        run_kernel_case(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_gpu(args)

@@ -304,11 +304,24 @@ Sweep classify_gate(const Gate& g) {
   return s;
 }
 
+namespace {
+std::vector<Sweep> plan_with(const std::vector<Gate>& in, uint32_t n, const qsvb_plan_opts& o, int dtype,
+                             bool phase_runs);
+}
+
 std::vector<Sweep> plan_sweeps(const std::vector<Gate>& in, uint32_t n, const qsvb_plan_opts& o0, int dtype) {
   qsvb_plan_opts o = o0;
   if (o.max_fused_qubits == 0) o.max_fused_qubits = 1;
   o.max_fused_qubits = std::min<uint32_t>(o.max_fused_qubits, std::min<uint32_t>(QSVB_MAX_GATE_QUBITS, n));
-  const bool phase_runs = o.planner == QSVB_PLAN_WINDOW || o.planner == QSVB_PLAN_LEARNED;
+  if (o.planner != QSVB_PLAN_LEARNED) return plan_with(in, n, o, dtype, false);
+  // learned: merging long diagonal runs into phase-polynomial sweeps is itself a candidate choice
+  std::vector<Sweep> a = plan_with(in, n, o, dtype, true), b = plan_with(in, n, o, dtype, false);
+  return predict_plan_seconds(a, n, dtype) <= predict_plan_seconds(b, n, dtype) ? a : b;
+}
+
+namespace {
+std::vector<Sweep> plan_with(const std::vector<Gate>& in, uint32_t n, const qsvb_plan_opts& o, int dtype,
+                             bool phase_runs) {
 
   // split into segments: phase-polynomial runs vs ordinary gates
   std::vector<Sweep> out;
@@ -360,6 +373,7 @@ std::vector<Sweep> plan_sweeps(const std::vector<Gate>& in, uint32_t n, const qs
   select_engines(out, n, o, dtype);
   return out;
 }
+}  // namespace
 
 void sweep_costs(const std::vector<Sweep>& sw, uint32_t n, int dtype, qsvb_plan_stats* st) {
   const double b = dtype == QSVB_C128 ? 16.0 : 8.0;

@@ -180,7 +180,11 @@ __global__ void __launch_bounds__(kTcThreads) k_tc_dense(float* __restrict__ re,
 
   uint32_t phase = 0;
   bool failed = false;
-  for (uint64_t tile = blockIdx.x; tile < ntiles && !failed; tile += gridDim.x) {
+  // Each thread owns V float4 of each component per tile. The next tile's loads are issued right
+  // after the current tile's MMAs, so they are in flight during the MMA wait, the epilogue and the
+  // write-back (32 KB per CTA for k = 6).
+  constexpr int V = TILE / 4 / kTcThreads;
+  auto tile_base = [&](uint64_t tile) {
     uint64_t base = tile << kTcColBits;
 #pragma unroll
     for (int j = 0; j < KQ; ++j) {
@@ -188,12 +192,26 @@ __global__ void __launch_bounds__(kTcThreads) k_tc_dense(float* __restrict__ re,
       const uint64_t lo = base & ((1ull << b) - 1ull);
       base = ((base - lo) << 1) | lo;
     }
-    // ---- gather + split into B (bf16 hi/lo)
-    for (int v = tid; v < TILE / 4; v += kTcThreads) {
-      const int t = v * 4, tlo = t & (kTcCols - 1), thi = t >> kTcColBits;
+    return base;
+  };
+  float4 pr[V], pim[V];
+  auto load_tile = [&](uint64_t base) {
+#pragma unroll
+    for (int j = 0; j < V; ++j) {
+      const int t = (tid + j * kTcThreads) * 4, tlo = t & (kTcCols - 1), thi = t >> kTcColBits;
       const uint64_t a = base + s_hioff[thi] + uint64_t(tlo);
-      const float4 xr = *reinterpret_cast<const float4*>(re + a);
-      const float4 xi = *reinterpret_cast<const float4*>(im + a);
+      pr[j] = __ldcs(reinterpret_cast<const float4*>(re + a));
+      pim[j] = __ldcs(reinterpret_cast<const float4*>(im + a));
+    }
+  };
+  if (uint64_t(blockIdx.x) < ntiles) load_tile(tile_base(blockIdx.x));
+  for (uint64_t tile = blockIdx.x; tile < ntiles && !failed; tile += gridDim.x) {
+    const uint64_t base = tile_base(tile);
+    // ---- split the prefetched tile into B (bf16 hi/lo)
+#pragma unroll
+    for (int j = 0; j < V; ++j) {
+      const int t = (tid + j * kTcThreads) * 4, tlo = t & (kTcCols - 1), thi = t >> kTcColBits;
+      const float4 xr = pr[j], xi = pim[j];
       const float vr[4] = {xr.x, xr.y, xr.z, xr.w}, vi[4] = {xi.x, xi.y, xi.z, xi.w};
       if (p.bmode == 2) {
 #pragma unroll
@@ -253,6 +271,8 @@ __global__ void __launch_bounds__(kTcThreads) k_tc_dense(float* __restrict__ re,
       }
       mma_commit(bar);
     }
+    // ---- prefetch the next tile while the tensor cores work
+    if (tile + gridDim.x < ntiles) load_tile(tile_base(tile + gridDim.x));
     // ---- bounded wait for the MMAs
     {
       const long long t0 = clock64();
@@ -292,12 +312,13 @@ __global__ void __launch_bounds__(kTcThreads) k_tc_dense(float* __restrict__ re,
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     // ---- coalesced write-back to the addresses the tile came from
-    for (int v = tid; v < TILE / 4; v += kTcThreads) {
-      const int t = v * 4, tlo = t & (kTcCols - 1), thi = t >> kTcColBits;
+#pragma unroll
+    for (int j = 0; j < V; ++j) {
+      const int t = (tid + j * kTcThreads) * 4, tlo = t & (kTcCols - 1), thi = t >> kTcColBits;
       const uint64_t a = base + s_hioff[thi] + uint64_t(tlo);
       const uint32_t si = stage_idx(uint32_t(t));
-      *reinterpret_cast<float4*>(re + a) = *reinterpret_cast<const float4*>(stage + si);
-      *reinterpret_cast<float4*>(im + a) = *reinterpret_cast<const float4*>(stage + TILE + si);
+      __stcs(reinterpret_cast<float4*>(re + a), *reinterpret_cast<const float4*>(stage + si));
+      __stcs(reinterpret_cast<float4*>(im + a), *reinterpret_cast<const float4*>(stage + TILE + si));
     }
     __syncthreads();
   }
