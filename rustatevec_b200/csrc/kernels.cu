@@ -807,6 +807,8 @@ void launch_dense_k(const LaunchEnv& env, R* re, R* im, uint32_t n, const Sweep&
   const uint64_t ntiles = 1ull << (n - K - NCB);
   const size_t smem = dense_smem_bytes<R, K>();
   QSVB_CK(cudaFuncSetAttribute(k_dense<R, K, NCB>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+  QSVB_CK(cudaFuncSetAttribute(k_dense<R, K, NCB>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                               int(cudaSharedmemCarveoutMaxShared)));
   int occ = 1;
   QSVB_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_dense<R, K, NCB>, kThreads, smem));
   const unsigned grid = unsigned(std::max<uint64_t>(1, std::min<uint64_t>(ntiles, uint64_t(env.num_sms) * std::max(occ, 1))));
