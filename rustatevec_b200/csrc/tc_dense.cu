@@ -2,26 +2,30 @@
 //
 // The sweep is the contraction Y = U X, X the state viewed as 2^k gate rows x 2^(n-k) columns.
 // It runs as a real GEMM on the embedding
-//     [Yr; Yi] = W [Xr; Xi],   W = [[Ur, -Ui], [Ui, Ur]]   (2^(k+1) x 2^(k+1))
+//     [Yr; Yi] = W [Xr; Xi],   W = [[Ur, -Ui], [Ui, Ur]]   (KR x KR, KR = 2^(k+1))
 // with BF16 hi/lo split operands and an FP32 accumulator in tensor memory:
 //     W X ~= Wlo Xhi + Whi Xlo + Whi Xhi      (x = hi + lo, hi = bf16(x), lo = bf16(x - hi))
 // which keeps about 16 significant bits per product (relative error ~1e-5 per sweep).
 //
-// A tile is 2^k gate rows x 64 columns, the columns being the 6 lowest non-gate state bits, so
-// every global access is a contiguous run of >= 64 amplitudes; tiles are disjoint and updated in
-// place. One persistent CTA per SM runs a warp-specialized pipeline:
-//   loader warps (8): keep R tiles of loads in flight in a register ring, split each tile into
-//     bf16 hi/lo and store it into one of two B buffers (128-byte swizzle; MN-major when state
-//     bits 0-1 are tile columns, K-major when they are the gate's two lowest qubits);
-//   MMA warp (1, one elected lane): 3 * 2^(k+1)/16 tcgen05.mma per tile into one of two TMEM
-//     accumulators (128 lanes x 64 fp32 columns); tcgen05.commit frees the B buffer and hands the
-//     accumulator to the epilogue;
+// Every k uses the same MMA shape, M = 128, K = 128, N = 64: the A operand is W repeated
+// nblk = 128 / KR times on the diagonal, and the B operand stacks nblk blocks of 64 state
+// columns along K. A tile is therefore always 4096 amplitudes (2^k gate rows x 64 * nblk
+// columns, the columns being the 12 - k lowest non-gate state bits, so every global access is a
+// contiguous run of >= 64 amplitudes) and all 128 accumulator lanes carry results.
+//
+// One persistent CTA per SM runs a warp-specialized pipeline:
+//   loader warps (8): keep 2 tiles of loads in flight in registers, split each tile into bf16
+//     hi/lo and store it into one of three B buffers (128-byte swizzle; MN-major when state bits
+//     0-1 are tile columns, K-major when they are the gate's two lowest qubits);
+//   MMA warp (1, one lane): 24 tcgen05.mma per tile into one of two TMEM accumulators
+//     (128 lanes x 64 fp32 columns); tcgen05.commit frees the B buffer and hands the accumulator
+//     to the epilogue;
 //   epilogue warps (4, one per TMEM lane quadrant): tcgen05.ld the accumulator, stage it in
 //     address order (16-byte XOR swizzle), release the accumulator, then write the tile back with
-//     coalesced 16-byte streaming stores.
-// A (Whi, Wlo; M = 128 rows, K-major, 128-byte swizzle) is packed on the host in the exact
-// shared-memory byte layout and copied in once per CTA. Every mbarrier wait is bounded: a wait
-// that runs out sets the context error flag and that role stops; the host reports QSVB_E_TIMEOUT.
+//     coalesced 16-byte streaming stores to the addresses it was read from.
+// A (Whi, Wlo; K-major, 128-byte swizzle) is packed on the host in the exact shared-memory byte
+// layout and copied in once per CTA. Every mbarrier wait is bounded: a wait that runs out sets the
+// context error flag and that role stops; the host reports QSVB_E_TIMEOUT.
 
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
@@ -36,25 +40,36 @@ namespace qsvb {
 
 namespace {
 
-constexpr int kTcCols = 64;     // tile columns (N of the MMA)
-constexpr int kTcColBits = 6;
+constexpr int kMmaN = 64;                 // MMA N: columns per block
+constexpr int kMmaK = 128;                // MMA K (real rows, all blocks)
+constexpr int kTileAmps = 4096;           // complex amplitudes per tile
+constexpr int kTileBits = 12;
 constexpr int kLoadWarps = 8;
 constexpr int kEpiWarps = 4;
 constexpr int kLoadThreads = kLoadWarps * 32;
 constexpr int kEpiThreads = kEpiWarps * 32;
 constexpr int kTcThreads = kLoadThreads + 32 + kEpiThreads;  // loaders, MMA warp, epilogue
 constexpr int kMmaWarp = kLoadWarps;                          // warp 8
-constexpr int kEpiWarp0 = kLoadWarps + 1;                     // warps 9..12 (quadrants 1,2,3,0)
+constexpr int kEpiWarp0 = kLoadWarps + 1;                     // warps 9..12 (lane quadrants 1,2,3,0)
+constexpr int kBSlots = 3;
 constexpr int kTmemCols = 128;                                // two 64-column accumulators
+constexpr int kLoadDepth = 2;                                 // tiles in flight per loader
+constexpr int kVL = kTileAmps / 4 / kLoadThreads;             // float4 per component per loader
+constexpr int kVE = kTileAmps / 4 / kEpiThreads;              // float4 per component per epilogue thread
+constexpr uint32_t kABytes = 128u * kMmaK * 2u;               // one of Whi / Wlo
+constexpr uint32_t kBBytes = uint32_t(kMmaN) * kMmaK * 2u;    // one of Xhi / Xlo
 constexpr long long kWaitBudget = 1ll << 31;                  // clock64 cycles (~1 s)
+constexpr size_t kTcSmem = 1024 + 2 * kABytes + kBSlots * 2 * kBBytes + kTileAmps * 8 + 128 + 64 * 8 +
+                           3 * 64 * 2 + 256 * 2;
 
 struct TcParams {
-  uint32_t hibits[6];      // tile bits above the 6 column bits (ascending)
+  uint32_t hibits[6];      // tile bits above the 6 lowest state bits (ascending)
+  uint32_t ncb;            // column bits (12 - k)
   uint64_t hioff[64];      // address offset of the high tile bits
-  uint16_t dsthi[64];      // (row << 6 | col) contribution of the high tile bits
-  uint16_t dstlo[64];      // (row << 6 | col) contribution of the low 6 address bits
+  uint16_t dsthi[64];      // (row << ncb | col) contribution of the high tile bits
+  uint16_t dstlo[64];      // (row << ncb | col) contribution of the low 6 state bits
   uint16_t trow[64];       // address-order tile index of gate row s
-  uint16_t tcol[64];       // address-order tile index of column c
+  uint16_t tcol[256];      // address-order tile index of column c
   uint32_t bmode;          // 0: MN-major vector, 1: K-major vector, 2: scalar stores
 };
 
@@ -115,16 +130,13 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
   return true;
 }
 
-__device__ __forceinline__ void tmem_ld16(uint32_t addr, float (&v)[16]) {
-  uint32_t r[16];
+// 32 lanes x 16 fp32 columns, no wait (the caller issues tcgen05.wait::ld once for a batch).
+__device__ __forceinline__ void tmem_ld16(uint32_t addr, uint32_t (&r)[16]) {
   asm volatile(
       "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
       : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
         "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
       : "r"(addr));
-  asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
-#pragma unroll
-  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
 __device__ __forceinline__ void named_sync(uint32_t id, uint32_t nthreads) {
@@ -145,7 +157,7 @@ __device__ __forceinline__ uint2 pack4(const __nv_bfloat16 (&x)[4]) {
 
 // Byte offset in a K-major, 128-byte-swizzled operand with `rows` rows (8-row atoms of 1024 B; a
 // row of an atom holds 64 K-elements; 64-element K blocks follow each other every rows*128 B).
-__device__ __forceinline__ uint32_t kmaj_off(uint32_t row, uint32_t kk, uint32_t rows) {
+__host__ __device__ __forceinline__ uint32_t kmaj_off(uint32_t row, uint32_t kk, uint32_t rows) {
   return (kk >> 6) * (rows * 128u) + (row >> 3) * 1024u + (row & 7u) * 128u +
          ((((kk & 63u) >> 3) ^ (row & 7u)) << 4) + (kk & 7u) * 2u;
 }
@@ -156,63 +168,55 @@ __device__ __forceinline__ uint32_t mnmaj_off(uint32_t kk, uint32_t col) {
 // Output staging (fp32, address order) with a 16-byte XOR swizzle against bank conflicts.
 __device__ __forceinline__ uint32_t stage_idx(uint32_t t) { return t ^ (((t >> 7) & 7u) << 2); }
 
-template <int KQ> struct TcShape {
-  static constexpr int M2 = 1 << KQ;               // complex gate rows
-  static constexpr int KR = 2 * M2;                // real rows (MMA K)
-  static constexpr int KP = KR < 64 ? 64 : KR;     // padded K (one swizzle row = 64 elements)
-  static constexpr uint32_t A_BYTES = 128u * KP * 2u;
-  static constexpr uint32_t B_BYTES = 64u * KP * 2u;   // one of hi / lo
-  static constexpr int TILE = M2 * kTcCols;        // complex amplitudes per tile
-  static constexpr int VL = TILE / 4 / kLoadThreads;   // float4 per component per loader thread
-  static constexpr int R = KQ == 6 ? 2 : (KQ == 5 ? 4 : 8);  // tiles in flight per loader
-  static constexpr int VE = TILE / 4 / kEpiThreads;    // float4 per component per epilogue thread
-  static constexpr size_t SMEM = 1024 + 2 * A_BYTES + 2 * (2 * B_BYTES) + size_t(TILE) * 8 + 128 + 64 * 8 + 4 * 64 * 2;
-};
-
 template <int KQ>
 __global__ void __launch_bounds__(kTcThreads, 1) k_tc_dense(float* __restrict__ re, float* __restrict__ im,
                                                             uint64_t ntiles, const uint4* __restrict__ wpack,
                                                             TcParams p, int* err) {
-  using S = TcShape<KQ>;
+  constexpr int M2 = 1 << KQ;      // complex gate rows
+  constexpr int KR = 2 * M2;       // real rows of one block
+  constexpr int NCB = kTileBits - KQ;
+  constexpr uint32_t CMASK = (1u << NCB) - 1u;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint8_t* a_hi = smem;
-  uint8_t* a_lo = a_hi + S::A_BYTES;
-  uint8_t* bbuf = a_lo + S::A_BYTES;               // slot s: hi at bbuf + s*2*B, lo right after
-  float* stage = reinterpret_cast<float*>(bbuf + 4 * S::B_BYTES);  // re [TILE] then im [TILE]
-  uint64_t* bars = reinterpret_cast<uint64_t*>(stage + 2 * S::TILE);
-  uint64_t* bfull = bars;        // [2] loaders -> MMA
-  uint64_t* bfree = bars + 2;    // [2] MMA commit -> loaders
-  uint64_t* dfull = bars + 4;    // [2] MMA commit -> epilogue
-  uint64_t* dfree = bars + 6;    // [2] epilogue -> MMA
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 8);
+  uint8_t* a_lo = a_hi + kABytes;
+  uint8_t* bbuf = a_lo + kABytes;                  // slot s: hi at bbuf + s*2*B, lo right after
+  float* stage = reinterpret_cast<float*>(bbuf + kBSlots * 2 * kBBytes);  // re [TILE], im [TILE]
+  uint64_t* bars = reinterpret_cast<uint64_t*>(stage + 2 * kTileAmps);
+  uint64_t* bfull = bars;        // [3] loaders -> MMA
+  uint64_t* bfree = bars + 3;    // [3] MMA commit -> loaders
+  uint64_t* dfull = bars + 6;    // [2] MMA commit -> epilogue
+  uint64_t* dfree = bars + 8;    // [2] epilogue -> MMA
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 10);
   uint64_t* s_hioff = reinterpret_cast<uint64_t*>(bars + 16);
   uint16_t* s_dhi = reinterpret_cast<uint16_t*>(s_hioff + 64);
   uint16_t* s_dlo = s_dhi + 64;
   uint16_t* s_trow = s_dlo + 64;
-  uint16_t* s_tcol = s_trow + 64;
+  uint16_t* s_tcol = s_trow + 64;  // 256 entries
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   {
     uint4* dst = reinterpret_cast<uint4*>(a_hi);
-    for (uint32_t i = tid; i < 2 * S::A_BYTES / 16; i += kTcThreads) dst[i] = wpack[i];
+    for (uint32_t i = tid; i < 2 * kABytes / 16; i += kTcThreads) dst[i] = wpack[i];
   }
   for (int i = tid; i < 64; i += kTcThreads) {
     s_hioff[i] = p.hioff[i];
     s_dhi[i] = p.dsthi[i];
     s_dlo[i] = p.dstlo[i];
     s_trow[i] = p.trow[i];
-    s_tcol[i] = p.tcol[i];
   }
+  for (int i = tid; i < 256; i += kTcThreads) s_tcol[i] = p.tcol[i];
   if (warp == kMmaWarp) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
                  "r"(kTmemCols));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   if (tid == 0) {
-    for (int s = 0; s < 2; ++s) {
+    for (int s = 0; s < kBSlots; ++s) {
       mbar_init(&bfull[s], kLoadThreads);
       mbar_init(&bfree[s], 1);
+    }
+    for (int s = 0; s < 2; ++s) {
       mbar_init(&dfull[s], 1);
       mbar_init(&dfree[s], kEpiThreads);
     }
@@ -226,9 +230,9 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_dense(float* __restrict__ 
   const uint32_t b_mn = p.bmode == 0 ? 1u : 0u;
 
   auto tile_base = [&](uint64_t tile) {
-    uint64_t base = tile << kTcColBits;
+    uint64_t base = tile << 6;
 #pragma unroll
-    for (int j = 0; j < KQ; ++j) {
+    for (int j = 0; j < 6; ++j) {
       const uint32_t b = p.hibits[j];
       const uint64_t lo = base & ((1ull << b) - 1ull);
       base = ((base - lo) << 1) | lo;
@@ -239,46 +243,47 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_dense(float* __restrict__ 
 
   if (warp < kLoadWarps) {
     // ============================ loaders: global -> registers -> bf16 hi/lo B buffers
-    float4 rr[S::R][S::VL], ri[S::R][S::VL];
-    auto load = [&](uint64_t i, float4 (&xr)[S::VL], float4 (&xi)[S::VL]) {
+    float4 rr[kLoadDepth][kVL], ri[kLoadDepth][kVL];
+    auto load = [&](uint64_t i, float4 (&xr)[kVL], float4 (&xi)[kVL]) {
       const uint64_t base = tile_base(blockIdx.x + i * gridDim.x);
 #pragma unroll
-      for (int j = 0; j < S::VL; ++j) {
-        const int t = (tid + j * kLoadThreads) * 4, tlo = t & (kTcCols - 1), thi = t >> kTcColBits;
+      for (int j = 0; j < kVL; ++j) {
+        const int t = (tid + j * kLoadThreads) * 4, tlo = t & 63, thi = t >> 6;
         const uint64_t a = base + s_hioff[thi] + uint64_t(tlo);
         xr[j] = __ldcs(reinterpret_cast<const float4*>(re + a));
         xi[j] = __ldcs(reinterpret_cast<const float4*>(im + a));
       }
     };
 #pragma unroll
-    for (int r = 0; r < S::R; ++r)
+    for (int r = 0; r < kLoadDepth; ++r)
       if (uint64_t(r) < my_tiles) load(r, rr[r], ri[r]);
     bool ok = true;
-    for (uint64_t i0 = 0; i0 < my_tiles && ok; i0 += S::R) {
+    for (uint64_t i0 = 0; i0 < my_tiles && ok; i0 += kLoadDepth) {
 #pragma unroll
-      for (int r = 0; r < S::R; ++r) {
+      for (int r = 0; r < kLoadDepth; ++r) {
         const uint64_t i = i0 + r;
         if (i >= my_tiles || !ok) break;
-        const uint32_t slot = uint32_t(i & 1), par = uint32_t((i >> 1) & 1);
+        const uint32_t slot = uint32_t(i % kBSlots), par = uint32_t((i / kBSlots) & 1);
         if (!mbar_wait(&bfree[slot], par ^ 1u)) {
           atomicExch(err, 1);
           ok = false;
           break;
         }
-        uint8_t* b_hi = bbuf + slot * 2 * S::B_BYTES;
-        uint8_t* b_lo = b_hi + S::B_BYTES;
+        uint8_t* b_hi = bbuf + slot * 2 * kBBytes;
+        uint8_t* b_lo = b_hi + kBBytes;
 #pragma unroll
-        for (int j = 0; j < S::VL; ++j) {
-          const int t = (tid + j * kLoadThreads) * 4, tlo = t & (kTcCols - 1), thi = t >> kTcColBits;
+        for (int j = 0; j < kVL; ++j) {
+          const int t = (tid + j * kLoadThreads) * 4, tlo = t & 63, thi = t >> 6;
           const float vr[4] = {rr[r][j].x, rr[r][j].y, rr[r][j].z, rr[r][j].w};
           const float vi[4] = {ri[r][j].x, ri[r][j].y, ri[r][j].z, ri[r][j].w};
           if (p.bmode == 2) {
 #pragma unroll
             for (int e = 0; e < 4; ++e) {
               const uint32_t d = uint32_t(s_dlo[tlo + e]) + s_dhi[thi];
-              const uint32_t s = d >> 6, c = d & 63u;
-              const uint32_t o_re = b_mn ? mnmaj_off(s, c) : kmaj_off(c, s, 64);
-              const uint32_t o_im = b_mn ? mnmaj_off(s + S::M2, c) : kmaj_off(c, s + S::M2, 64);
+              const uint32_t s = d >> NCB, c = d & CMASK;
+              const uint32_t kb = (c >> 6) * KR, cl = c & 63u;
+              const uint32_t o_re = b_mn ? mnmaj_off(kb + s, cl) : kmaj_off(cl, kb + s, 64);
+              const uint32_t o_im = b_mn ? mnmaj_off(kb + M2 + s, cl) : kmaj_off(cl, kb + M2 + s, 64);
               __nv_bfloat16 h, l;
               split_bf16(vr[e], h, l);
               *reinterpret_cast<__nv_bfloat16*>(b_hi + o_re) = h;
@@ -290,9 +295,10 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_dense(float* __restrict__ 
           } else {
             // four consecutive columns of row s (MN-major) or four consecutive rows of column c
             const uint32_t d = uint32_t(s_dlo[tlo]) + s_dhi[thi];
-            const uint32_t s = d >> 6, c = d & 63u;
-            const uint32_t o_re = b_mn ? mnmaj_off(s, c) : kmaj_off(c, s, 64);
-            const uint32_t o_im = b_mn ? mnmaj_off(s + S::M2, c) : kmaj_off(c, s + S::M2, 64);
+            const uint32_t s = d >> NCB, c = d & CMASK;
+            const uint32_t kb = (c >> 6) * KR, cl = c & 63u;
+            const uint32_t o_re = b_mn ? mnmaj_off(kb + s, cl) : kmaj_off(cl, kb + s, 64);
+            const uint32_t o_im = b_mn ? mnmaj_off(kb + M2 + s, cl) : kmaj_off(cl, kb + M2 + s, 64);
             __nv_bfloat16 hr[4], lr[4], hm[4], lm[4];
 #pragma unroll
             for (int e = 0; e < 4; ++e) {
@@ -307,29 +313,30 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_dense(float* __restrict__ 
         }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         mbar_arrive(&bfull[slot]);
-        if (i + S::R < my_tiles) load(i + S::R, rr[r], ri[r]);
+        if (i + kLoadDepth < my_tiles) load(i + kLoadDepth, rr[r], ri[r]);
       }
     }
   } else if (warp == kMmaWarp) {
     // ============================ MMA issue: one lane
     if (lane == 0) {
-      const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | (b_mn << 16) | (uint32_t(kTcCols >> 3) << 17) |
+      const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | (b_mn << 16) | (uint32_t(kMmaN >> 3) << 17) |
                              (uint32_t(128 >> 4) << 24);
       const uint32_t a_hi_s = smem_u32(a_hi), a_lo_s = smem_u32(a_lo);
+      const uint32_t b_lbo = b_mn ? uint32_t(kMmaK) * 128u : 16u;
       for (uint64_t i = 0; i < my_tiles; ++i) {
-        const uint32_t slot = uint32_t(i & 1), par = uint32_t((i >> 1) & 1);
-        if (!mbar_wait(&bfull[slot], par) || !mbar_wait(&dfree[slot], par ^ 1u)) {
+        const uint32_t slot = uint32_t(i % kBSlots), par = uint32_t((i / kBSlots) & 1);
+        const uint32_t ds = uint32_t(i & 1), dpar = uint32_t((i >> 1) & 1);
+        if (!mbar_wait(&bfull[slot], par) || !mbar_wait(&dfree[ds], dpar ^ 1u)) {
           atomicExch(err, 1);
           break;
         }
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        const uint32_t b_hi_s = smem_u32(bbuf + slot * 2 * S::B_BYTES), b_lo_s = b_hi_s + S::B_BYTES;
-        const uint32_t d_tmem = tmem + slot * kTcCols;
+        const uint32_t b_hi_s = smem_u32(bbuf + slot * 2 * kBBytes), b_lo_s = b_hi_s + kBBytes;
+        const uint32_t d_tmem = tmem + ds * kMmaN;
 #pragma unroll 1
-        for (int s = 0; s < S::KR / 16; ++s) {
+        for (int s = 0; s < kMmaK / 16; ++s) {
           const uint32_t ak = (s >> 2) * (128u * 128u) + (s & 3) * 32u;
           const uint32_t bk = b_mn ? uint32_t(s) * 2048u : (s >> 2) * (64u * 128u) + (s & 3) * 32u;
-          const uint32_t b_lbo = b_mn ? uint32_t(S::KP) * 128u : 16u;
           const uint64_t dah = sw128_desc(a_hi_s + ak, 16u, 1024u), dal = sw128_desc(a_lo_s + ak, 16u, 1024u);
           const uint64_t dbh = sw128_desc(b_hi_s + bk, b_lbo, 1024u), dbl = sw128_desc(b_lo_s + bk, b_lbo, 1024u);
           mma_bf16(d_tmem, dal, dbh, idesc, s > 0 ? 1u : 0u);
@@ -337,60 +344,60 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_dense(float* __restrict__ 
           mma_bf16(d_tmem, dah, dbh, idesc, 1u);
         }
         mma_commit(&bfree[slot]);  // B buffer consumed
-        mma_commit(&dfull[slot]);  // accumulator ready
+        mma_commit(&dfull[ds]);    // accumulator ready
       }
     }
     __syncwarp();
   } else {
     // ============================ epilogue: TMEM -> staging -> global
-    const int ew = warp - kEpiWarp0;          // 0..3
-    const int quad = warp & 3;                // TMEM lane quadrant this warp may access
-    const int et = tid - kEpiWarp0 * 32;      // 0..127
+    const int quad = warp & 3;                      // TMEM lane quadrant this warp may access
+    const int et = tid - kEpiWarp0 * 32;            // 0..127
     const uint32_t m = uint32_t(quad * 32 + lane);  // accumulator row = TMEM lane
-    const bool has_row = int(m) < S::KR;
-    const uint32_t s = m & uint32_t(S::M2 - 1), part = m >> KQ;
-    (void)ew;
+    const uint32_t blk = m / KR, r = m % KR;
+    const uint32_t s = r & uint32_t(M2 - 1), part = r >> KQ;
+    float* st = stage + part * kTileAmps;
     for (uint64_t i = 0; i < my_tiles; ++i) {
-      const uint32_t slot = uint32_t(i & 1), par = uint32_t((i >> 1) & 1);
-      if (!mbar_wait(&dfull[slot], par)) {
+      const uint32_t ds = uint32_t(i & 1), dpar = uint32_t((i >> 1) & 1);
+      if (!mbar_wait(&dfull[ds], dpar)) {
         atomicExch(err, 1);
         break;
       }
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      named_sync(1, kEpiThreads);  // the previous tile's write-back has finished reading staging
-      if (quad * 32 < S::KR) {
-        float* st = stage + part * S::TILE;
-        const uint32_t tr = s_trow[s];
-#pragma unroll 1
-        for (int cb = 0; cb < kTcCols / 16; ++cb) {
-          float v[16];
-          tmem_ld16(tmem + (uint32_t(quad * 32) << 16) + slot * kTcCols + uint32_t(cb * 16), v);
-          if (has_row) {
-            if (p.bmode == 0) {
+      uint32_t v[4][16];
+      const uint32_t taddr = tmem + (uint32_t(quad * 32) << 16) + ds * kMmaN;
 #pragma unroll
-              for (int q = 0; q < 4; ++q) {
-                const uint32_t t = tr + s_tcol[cb * 16 + q * 4];
-                *reinterpret_cast<float4*>(st + stage_idx(t)) =
-                    make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
-              }
-            } else {
-#pragma unroll
-              for (int q = 0; q < 16; ++q) st[stage_idx(tr + s_tcol[cb * 16 + q])] = v[q];
-            }
-          }
-        }
-      }
+      for (int cb = 0; cb < 4; ++cb) tmem_ld16(taddr + uint32_t(cb * 16), v[cb]);
+      asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
       asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-      mbar_arrive(&dfree[slot]);
+      mbar_arrive(&dfree[ds]);     // accumulator may be overwritten now
+      named_sync(1, kEpiThreads);  // the previous tile's write-back has finished reading staging
+      const uint32_t tr = s_trow[s];
+      const uint16_t* tc = s_tcol + blk * 64;
+      if (p.bmode == 0) {
+#pragma unroll
+        for (int cb = 0; cb < 4; ++cb)
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            const uint32_t t = tr + tc[cb * 16 + q * 4];
+            *reinterpret_cast<float4*>(st + stage_idx(t)) =
+                make_float4(__uint_as_float(v[cb][4 * q]), __uint_as_float(v[cb][4 * q + 1]),
+                            __uint_as_float(v[cb][4 * q + 2]), __uint_as_float(v[cb][4 * q + 3]));
+          }
+      } else {
+#pragma unroll
+        for (int cb = 0; cb < 4; ++cb)
+#pragma unroll
+          for (int q = 0; q < 16; ++q) st[stage_idx(tr + tc[cb * 16 + q])] = __uint_as_float(v[cb][q]);
+      }
       named_sync(1, kEpiThreads);  // staging complete
       const uint64_t base = tile_base(blockIdx.x + i * gridDim.x);
 #pragma unroll
-      for (int j = 0; j < S::VE; ++j) {
-        const int t = (et + j * kEpiThreads) * 4, tlo = t & (kTcCols - 1), thi = t >> kTcColBits;
+      for (int j = 0; j < kVE; ++j) {
+        const int t = (et + j * kEpiThreads) * 4, tlo = t & 63, thi = t >> 6;
         const uint64_t a = base + s_hioff[thi] + uint64_t(tlo);
         const uint32_t si = stage_idx(uint32_t(t));
         __stcs(reinterpret_cast<float4*>(re + a), *reinterpret_cast<const float4*>(stage + si));
-        __stcs(reinterpret_cast<float4*>(im + a), *reinterpret_cast<const float4*>(stage + S::TILE + si));
+        __stcs(reinterpret_cast<float4*>(im + a), *reinterpret_cast<const float4*>(stage + kTileAmps + si));
       }
     }
   }
@@ -416,48 +423,42 @@ float bf16_to_float(uint16_t h) {
   std::memcpy(&f, &u, 4);
   return f;
 }
-uint32_t kmaj_off_host(uint32_t row, uint32_t kk, uint32_t rows) {
-  return (kk >> 6) * (rows * 128u) + (row >> 3) * 1024u + (row & 7u) * 128u +
-         ((((kk & 63u) >> 3) ^ (row & 7u)) << 4) + (kk & 7u) * 2u;
-}
 
 }  // namespace
 
 bool tc_dense_supported(const Sweep& s, uint32_t n) {
-  return (s.kind == SK_DENSE || s.kind == SK_DENSE_TC) && s.m >= 4 && s.m <= 6 && n >= s.m + kTcColBits + 2 &&
-         n >= 12;
+  return (s.kind == SK_DENSE || s.kind == SK_DENSE_TC) && s.m >= 4 && s.m <= 6 && n >= uint32_t(kTileBits);
 }
 
-size_t tc_matrix_bytes(const Sweep& s) {
-  const size_t KR = size_t(2) << s.m, KP = std::max<size_t>(64, KR);
-  return 2 * 128 * KP * 2;
-}
+size_t tc_matrix_bytes(const Sweep&) { return 2 * size_t(kABytes); }
 
-// W = [[Ur, -Ui], [Ui, Ur]] split into bf16 hi/lo, K-major, 128-byte swizzle, 128 rows.
+// A = blockdiag(W, ..., W) (128 / KR copies), W = [[Ur, -Ui], [Ui, Ur]], split into bf16 hi/lo,
+// K-major, 128-byte swizzle, 128 x 128.
 void tc_pack_matrix(const Sweep& s, void* dst) {
-  const uint32_t M2 = 1u << s.m, KR = 2 * M2, KP = std::max<uint32_t>(64, KR);
-  const size_t a_bytes = size_t(128) * KP * 2;
+  const uint32_t M2 = 1u << s.m, KR = 2 * M2, nblk = 128 / KR;
   uint8_t* hi = static_cast<uint8_t*>(dst);
-  uint8_t* lo = hi + a_bytes;
-  std::memset(dst, 0, 2 * a_bytes);
-  for (uint32_t r = 0; r < KR; ++r)
-    for (uint32_t k = 0; k < KR; ++k) {
-      const cd u = s.mat[size_t(r % M2) * M2 + (k % M2)];
-      double w;
-      if (r < M2) w = k < M2 ? u.real() : -u.imag();
-      else w = k < M2 ? u.imag() : u.real();
-      const uint16_t h = bf16_bits_rn(float(w));
-      const uint16_t l = bf16_bits_rn(float(w - double(bf16_to_float(h))));
-      const uint32_t o = kmaj_off_host(r, k, 128);
-      std::memcpy(hi + o, &h, 2);
-      std::memcpy(lo + o, &l, 2);
-    }
+  uint8_t* lo = hi + kABytes;
+  std::memset(dst, 0, 2 * size_t(kABytes));
+  for (uint32_t b = 0; b < nblk; ++b)
+    for (uint32_t r = 0; r < KR; ++r)
+      for (uint32_t k = 0; k < KR; ++k) {
+        const cd u = s.mat[size_t(r % M2) * M2 + (k % M2)];
+        double w;
+        if (r < M2) w = k < M2 ? u.real() : -u.imag();
+        else w = k < M2 ? u.imag() : u.real();
+        const uint16_t h = bf16_bits_rn(float(w));
+        const uint16_t l = bf16_bits_rn(float(w - double(bf16_to_float(h))));
+        const uint32_t o = kmaj_off(b * KR + r, b * KR + k, 128);
+        std::memcpy(hi + o, &h, 2);
+        std::memcpy(lo + o, &l, 2);
+      }
 }
 
 template <int KQ>
 static void launch_tc_k(const LaunchEnv& env, float* re, float* im, uint32_t n, const Sweep& s, const void* dev_mat) {
-  constexpr int M2 = 1 << KQ;
+  constexpr int M2 = 1 << KQ, NCB = kTileBits - KQ;
   TcParams p{};
+  p.ncb = NCB;
   int gate_rank[64], col_rank[64];
   for (int b = 0; b < 64; ++b) gate_rank[b] = col_rank[b] = -1;
   for (int j = 0; j < KQ; ++j) gate_rank[s.q[j]] = j;
@@ -465,20 +466,21 @@ static void launch_tc_k(const LaunchEnv& env, float* re, float* im, uint32_t n, 
   int ncol = 0;
   for (uint32_t b = 0; b < n; ++b) {
     if (gate_rank[b] >= 0) tbits.push_back(b);
-    else if (ncol < kTcColBits) {
+    else if (ncol < NCB) {
       col_rank[b] = ncol++;
       tbits.push_back(b);
     }
   }
-  for (int j = 0; j < kTcColBits; ++j) QSVB_REQUIRE(tbits[j] == uint32_t(j), "tc tile: low bits not contiguous");
+  QSVB_REQUIRE(tbits.size() == size_t(kTileBits), "tc tile: state too small");
+  for (int j = 0; j < 6; ++j) QSVB_REQUIRE(tbits[j] == uint32_t(j), "tc tile: low bits not contiguous");
   auto contrib = [&](uint32_t b) -> uint32_t {
-    return gate_rank[b] >= 0 ? (uint32_t(1) << gate_rank[b]) << kTcColBits : (uint32_t(1) << col_rank[b]);
+    return gate_rank[b] >= 0 ? (uint32_t(1) << gate_rank[b]) << NCB : (uint32_t(1) << col_rank[b]);
   };
-  for (int j = 0; j < KQ; ++j) p.hibits[j] = tbits[kTcColBits + j];
-  for (int h = 0; h < M2; ++h) {
+  for (int j = 0; j < 6; ++j) p.hibits[j] = tbits[6 + j];
+  for (int h = 0; h < 64; ++h) {
     uint64_t off = 0;
     uint32_t d = 0;
-    for (int j = 0; j < KQ; ++j)
+    for (int j = 0; j < 6; ++j)
       if ((h >> j) & 1) {
         off |= 1ull << p.hibits[j];
         d += contrib(p.hibits[j]);
@@ -486,39 +488,38 @@ static void launch_tc_k(const LaunchEnv& env, float* re, float* im, uint32_t n, 
     p.hioff[h] = off;
     p.dsthi[h] = uint16_t(d);
   }
-  for (int l = 0; l < kTcCols; ++l) {
+  for (int l = 0; l < 64; ++l) {
     uint32_t d = 0;
-    for (int b = 0; b < kTcColBits; ++b)
+    for (int b = 0; b < 6; ++b)
       if ((l >> b) & 1) d += contrib(uint32_t(b));
     p.dstlo[l] = uint16_t(d);
   }
   // address-order tile index of each gate row / column: tile position = rank among tile bits
+  auto rank_of = [&](uint32_t b) { return uint32_t(std::find(tbits.begin(), tbits.end(), b) - tbits.begin()); };
   for (int sidx = 0; sidx < M2; ++sidx) {
     uint32_t t = 0;
     for (int j = 0; j < KQ; ++j)
-      if ((sidx >> j) & 1) t |= 1u << uint32_t(std::find(tbits.begin(), tbits.end(), s.q[j]) - tbits.begin());
+      if ((sidx >> j) & 1) t |= 1u << rank_of(s.q[j]);
     p.trow[sidx] = uint16_t(t);
   }
-  for (int c = 0; c < kTcCols; ++c) {
+  for (int c = 0; c < (1 << NCB); ++c) {
     uint32_t t = 0;
     for (uint32_t b = 0; b < n; ++b)
-      if (col_rank[b] >= 0 && ((c >> col_rank[b]) & 1))
-        t |= 1u << uint32_t(std::find(tbits.begin(), tbits.end(), b) - tbits.begin());
+      if (col_rank[b] >= 0 && ((c >> col_rank[b]) & 1)) t |= 1u << rank_of(b);
     p.tcol[c] = uint16_t(t);
   }
   const bool low_cols = gate_rank[0] < 0 && gate_rank[1] < 0;
   const bool low_rows = gate_rank[0] == 0 && gate_rank[1] == 1;
   p.bmode = low_cols ? 0u : (low_rows ? 1u : 2u);
 
-  const uint64_t ntiles = 1ull << (n - KQ - kTcColBits);
-  const size_t smem = TcShape<KQ>::SMEM;
-  QSVB_CK(cudaFuncSetAttribute(k_tc_dense<KQ>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+  const uint64_t ntiles = 1ull << (n - kTileBits);
+  QSVB_CK(cudaFuncSetAttribute(k_tc_dense<KQ>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kTcSmem)));
   QSVB_CK(cudaFuncSetAttribute(k_tc_dense<KQ>, cudaFuncAttributePreferredSharedMemoryCarveout,
                                int(cudaSharedmemCarveoutMaxShared)));
   // one persistent CTA per SM (the tensor-memory allocation assumes it)
   const unsigned grid = unsigned(std::max<uint64_t>(1, std::min<uint64_t>(ntiles, uint64_t(env.num_sms))));
-  k_tc_dense<KQ><<<grid, kTcThreads, smem, env.stream>>>(re, im, ntiles, static_cast<const uint4*>(dev_mat), p,
-                                                         env.err_flag);
+  k_tc_dense<KQ><<<grid, kTcThreads, kTcSmem, env.stream>>>(re, im, ntiles, static_cast<const uint4*>(dev_mat), p,
+                                                            env.err_flag);
   QSVB_CK(cudaGetLastError());
 }
 
