@@ -305,6 +305,87 @@ __global__ void __launch_bounds__(kThreads) k_phase(R* __restrict__ re, R* __res
   }
 }
 
+// Phase polynomial in Ising form for states of >= 12 qubits. Any product of <= 2-qubit diagonal
+// phases is exp(i theta(x)) with theta = C + sum_q h_q z_q + sum_(a<b) J_ab z_a z_b, z_q = 1 - 2 x_q.
+// A CTA walks chunks of 4096 consecutive amplitudes. The edge terms inside the low 12 bits are
+// tabulated once per CTA (32 KB); per chunk, the high bits are constant, so the high-high terms fold
+// into one scalar and the high-low edges into the linear coefficients of the low bits, kept as two
+// 64-entry tables. Each amplitude then costs three shared loads, three adds and one FP64 sincos.
+constexpr int kIsingMaxEdges = 160;
+constexpr int kIsingChunkBits = 12;
+struct IsingP {
+  double c0;
+  double h[64];
+  double J[kIsingMaxEdges];
+  uint8_t ea[kIsingMaxEdges], eb[kIsingMaxEdges];  // ea < eb
+  uint32_t nedges;
+};
+
+__device__ __forceinline__ double zsign(uint64_t x, uint32_t q) { return 1.0 - 2.0 * double((x >> q) & 1ull); }
+
+template <class R>
+__global__ void __launch_bounds__(kThreads) k_ising(R* __restrict__ re, R* __restrict__ im, uint64_t nchunks,
+                                                    IsingP p) {
+  constexpr int CB = kIsingChunkBits, CH = 1 << CB, N = VecT<R>::N;
+  __shared__ double tll[CH];
+  __shared__ double l1[64], l2[64], hp[CB];
+  __shared__ double thh;
+  const int tid = threadIdx.x;
+  for (int l = tid; l < CH; l += kThreads) {
+    double s = 0.0;
+    for (uint32_t e = 0; e < p.nedges; ++e)
+      if (p.eb[e] < CB) s += p.J[e] * zsign(uint64_t(l), p.ea[e]) * zsign(uint64_t(l), p.eb[e]);
+    tll[l] = s;
+  }
+  for (uint64_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
+    const uint64_t base = ch << CB;
+    __syncthreads();  // the previous chunk is done with l1 / l2 / thh (and tll is built)
+    if (tid < CB) {
+      double v = p.h[tid];
+      for (uint32_t e = 0; e < p.nedges; ++e)
+        if (p.ea[e] == uint32_t(tid) && p.eb[e] >= CB) v += p.J[e] * zsign(base, p.eb[e]);
+      hp[tid] = v;
+    } else if (tid == 32) {
+      double v = p.c0;
+      for (uint32_t q = CB; q < 64; ++q)
+        if (p.h[q] != 0.0) v += p.h[q] * zsign(base, q);
+      for (uint32_t e = 0; e < p.nedges; ++e)
+        if (p.ea[e] >= CB) v += p.J[e] * zsign(base, p.ea[e]) * zsign(base, p.eb[e]);
+      thh = v;
+    }
+    __syncthreads();
+    if (tid < 64) {
+      double v = 0.0;
+      for (int q = 0; q < 6; ++q) v += hp[q] * zsign(uint64_t(tid), q);
+      l1[tid] = v;
+    } else if (tid < 128) {
+      double v = 0.0;
+      for (int q = 0; q < 6; ++q) v += hp[6 + q] * zsign(uint64_t(tid - 64), q);
+      l2[tid - 64] = v;
+    }
+    __syncthreads();
+    const double t0 = thh;
+    for (int v = tid; v < CH / N; v += kThreads) {
+      const uint32_t l = uint32_t(v * N);
+      R xr[N], xi[N];
+      vld(re + base + l, xr);
+      vld(im + base + l, xi);
+#pragma unroll
+      for (int e = 0; e < N; ++e) {
+        const uint32_t x = l + e;
+        const double th = t0 + tll[x] + l1[x & 63u] + l2[x >> 6];
+        double sn, cs;
+        sincos(th, &sn, &cs);
+        const double a = double(xr[e]), c = double(xi[e]);
+        xr[e] = R(cs * a - sn * c);
+        xi[e] = R(cs * c + sn * a);
+      }
+      vst(re + base + l, xr);
+      vst(im + base + l, xi);
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------------------------
 // Dense k-qubit sweep on CUDA cores (qsv kernels.cu:91-120 gathers one 2^m block per thread into
 // local arrays; here a CTA gathers a tile of 2^K rows x NC columns into shared memory, where the
@@ -833,6 +914,43 @@ template <class R>
 void launch_phase(const LaunchEnv& env, R* re, R* im, uint32_t n, const Sweep& s, const void* dev_terms) {
   const uint64_t dim = 1ull << n;
   const uint32_t nt = uint32_t(s.terms.size());
+  if (n >= uint32_t(kIsingChunkBits)) {
+    // Walsh transform of every term: theta = c0 + c1 z0 (+ c2 z1 + c3 z0 z1), index = b0 + 2 b1
+    IsingP p{};
+    std::vector<std::pair<uint32_t, uint32_t>> keys;
+    std::vector<double> js;
+    for (const PhaseTerm& t : s.terms) {
+      const double* a = t.ang;
+      if (t.m == 1) {
+        p.c0 += 0.5 * (a[0] + a[1]);
+        p.h[t.q[0]] += 0.5 * (a[0] - a[1]);
+        continue;
+      }
+      p.c0 += 0.25 * (a[0] + a[1] + a[2] + a[3]);
+      p.h[t.q[0]] += 0.25 * (a[0] - a[1] + a[2] - a[3]);
+      p.h[t.q[1]] += 0.25 * (a[0] + a[1] - a[2] - a[3]);
+      const double j = 0.25 * (a[0] - a[1] - a[2] + a[3]);
+      const auto key = std::make_pair(std::min(t.q[0], t.q[1]), std::max(t.q[0], t.q[1]));
+      const auto it = std::find(keys.begin(), keys.end(), key);
+      if (it == keys.end()) {
+        keys.push_back(key);
+        js.push_back(j);
+      } else {
+        js[size_t(it - keys.begin())] += j;
+      }
+    }
+    QSVB_REQUIRE(keys.size() <= size_t(kIsingMaxEdges), "phase polynomial has too many distinct pairs");
+    p.nedges = uint32_t(keys.size());
+    for (size_t e = 0; e < keys.size(); ++e) {
+      p.ea[e] = uint8_t(keys[e].first);
+      p.eb[e] = uint8_t(keys[e].second);
+      p.J[e] = js[e];
+    }
+    const uint64_t nchunks = dim >> kIsingChunkBits;
+    k_ising<R><<<grid_for(nchunks, 1, env.num_sms, 4), kThreads, 0, env.stream>>>(re, im, nchunks, p);
+    check_launch();
+    return;
+  }
   const size_t smem = nt * sizeof(PhaseTermDev);
   QSVB_REQUIRE(smem <= 200 * 1024, "phase polynomial too large");
   QSVB_CK(cudaFuncSetAttribute(k_phase<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));

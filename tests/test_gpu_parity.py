@@ -291,3 +291,41 @@ def test_errors_are_status_codes(be):
     # the context stays usable after every rejected call
     be.init_basis(st, 3)
     assert abs(be.amplitude(st, 3) - 1.0) < 1e-12
+
+
+# --------------------------------------------------------------- phase-polynomial (QAOA cost layer)
+@pytest.mark.parametrize("n", [8, 12, 14])
+def test_qaoa_phase_sweeps_match_oracle(be, n):
+    from rustatevec_b200.circuits import qaoa_maxcut
+    c = qaoa_maxcut(n, 3, 11 + n)
+    st = be.alloc(n)
+    be.init_basis(st, 0)
+    stats = be.run(st, c, opts(PLAN_LEARNED, 4))
+    assert stats["by_kind"].get("phase", 0) >= 1, stats
+    got = be.download(st).as_complex()
+    assert max_abs_diff(ref_state(c), got) < TOL[be.precision] * 10, stats
+
+
+def test_phase_sweep_general_diagonals(be):
+    # mixed 1- and 2-qubit diagonal terms, repeated pairs, and a low/high split at bit 12
+    n = 14
+    rng = np.random.default_rng(5)
+    c = Circuit(n)
+    for q in range(n):
+        c.h(q)
+    for _ in range(40):
+        a, b = (int(x) for x in rng.choice(n, size=2, replace=False))
+        kind = rng.integers(4)
+        if kind == 0:
+            c.rzz(a, b, float(rng.uniform(0, 6.3)))
+        elif kind == 1:
+            c.cphase(a, b, float(rng.uniform(0, 6.3)))
+        elif kind == 2:
+            c.rz(a, float(rng.uniform(0, 6.3)))
+        else:
+            c.cz(a, b)
+    st = be.alloc(n)
+    be.init_basis(st, 0)
+    stats = be.run(st, c, opts(PLAN_LEARNED, 3))
+    got = be.download(st).as_complex()
+    assert max_abs_diff(ref_state(c), got) < TOL[be.precision] * 10, stats
