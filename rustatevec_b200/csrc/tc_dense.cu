@@ -13,16 +13,18 @@
 // columns, the columns being the 12 - k lowest non-gate state bits, so every global access is a
 // contiguous run of >= 64 amplitudes) and all 128 accumulator lanes carry results.
 //
-// One persistent CTA per SM runs a warp-specialized pipeline:
-//   loader warps (8): keep 2 tiles of loads in flight in registers, split each tile into bf16
-//     hi/lo and store it into one of three B buffers (128-byte swizzle; MN-major when state bits
-//     0-1 are tile columns, K-major when they are the gate's two lowest qubits);
-//   MMA warp (1, one lane): 24 tcgen05.mma per tile into one of two TMEM accumulators
-//     (128 lanes x 64 fp32 columns); tcgen05.commit frees the B buffer and hands the accumulator
-//     to the epilogue;
-//   epilogue warps (4, one per TMEM lane quadrant): tcgen05.ld the accumulator, stage it in
-//     address order (16-byte XOR swizzle), release the accumulator, then write the tile back with
-//     coalesced 16-byte streaming stores to the addresses it was read from.
+// One persistent CTA per SM runs a warp-specialized pipeline over its tiles:
+//   producer warp (1 lane): TMA bulk copies (cp.async.bulk, one per contiguous run, no
+//     multicast) of the tile's re/im runs into one of three fp32 staging slots, completing on
+//     that slot's mbarrier;
+//   converter warps (8): split the staged tile into bf16 hi/lo and store it into one of two B
+//     buffers (128-byte swizzle; MN-major when state bits 0-1 are tile columns, K-major when
+//     they are the gate's two lowest qubits);
+//   MMA warp (1 lane): 24 tcgen05.mma per tile into one of two TMEM accumulators (128 lanes x
+//     64 fp32 columns); tcgen05.commit frees the B buffer and hands the accumulator on;
+//   epilogue warps (4, one per TMEM lane quadrant): tcgen05.ld the accumulator, write the result
+//     over the tile's own staging slot (address order, 16-byte XOR swizzle), release the
+//     accumulator, write the tile back with coalesced 16-byte streaming stores, release the slot.
 // A (Whi, Wlo; K-major, 128-byte swizzle) is packed on the host in the exact shared-memory byte
 // layout and copied in once per CTA. Every mbarrier wait is bounded: a wait that runs out sets the
 // context error flag and that role stops; the host reports QSVB_E_TIMEOUT.
@@ -44,27 +46,30 @@ constexpr int kMmaN = 64;                 // MMA N: columns per block
 constexpr int kMmaK = 128;                // MMA K (real rows, all blocks)
 constexpr int kTileAmps = 4096;           // complex amplitudes per tile
 constexpr int kTileBits = 12;
-constexpr int kLoadWarps = 8;
+constexpr int kCvtWarps = 8;
 constexpr int kEpiWarps = 4;
-constexpr int kLoadThreads = kLoadWarps * 32;
+constexpr int kCvtThreads = kCvtWarps * 32;
 constexpr int kEpiThreads = kEpiWarps * 32;
-constexpr int kTcThreads = kLoadThreads + 32 + kEpiThreads;  // loaders, MMA warp, epilogue
-constexpr int kMmaWarp = kLoadWarps;                          // warp 8
-constexpr int kEpiWarp0 = kLoadWarps + 1;                     // warps 9..12 (lane quadrants 1,2,3,0)
-constexpr int kBSlots = 3;
+constexpr int kProdWarp = kCvtWarps;                          // warp 8
+constexpr int kMmaWarp = kCvtWarps + 1;                       // warp 9
+constexpr int kEpiWarp0 = kCvtWarps + 2;                      // warps 10..13 (lane quadrants 2,3,0,1)
+constexpr int kTcThreads = (kCvtWarps + 2 + kEpiWarps) * 32;
+constexpr int kBSlots = 2;
+constexpr int kIoSlots = 3;
 constexpr int kTmemCols = 128;                                // two 64-column accumulators
-constexpr int kLoadDepth = 2;                                 // tiles in flight per loader
-constexpr int kVL = kTileAmps / 4 / kLoadThreads;             // float4 per component per loader
+constexpr int kVC = kTileAmps / 4 / kCvtThreads;              // float4 per component per converter
 constexpr int kVE = kTileAmps / 4 / kEpiThreads;              // float4 per component per epilogue thread
 constexpr uint32_t kABytes = 128u * kMmaK * 2u;               // one of Whi / Wlo
 constexpr uint32_t kBBytes = uint32_t(kMmaN) * kMmaK * 2u;    // one of Xhi / Xlo
+constexpr uint32_t kIoBytes = kTileAmps * 8u;                 // re [4096] + im [4096] fp32
 constexpr long long kWaitBudget = 1ll << 31;                  // clock64 cycles (~1 s)
-constexpr size_t kTcSmem = 1024 + 2 * kABytes + kBSlots * 2 * kBBytes + kTileAmps * 8 + 128 + 64 * 8 +
-                           3 * 64 * 2 + 256 * 2;
+constexpr size_t kTcSmem = 1024 + 2 * size_t(kABytes) + kBSlots * 2 * size_t(kBBytes) + kIoSlots * size_t(kIoBytes) +
+                           128 + 64 * 8 + 3 * 64 * 2 + 256 * 2;
 
 struct TcParams {
   uint32_t hibits[6];      // tile bits above the 6 lowest state bits (ascending)
   uint32_t ncb;            // column bits (12 - k)
+  uint32_t runbits;        // log2 of the contiguous run length of a tile (>= 6)
   uint64_t hioff[64];      // address offset of the high tile bits
   uint16_t dsthi[64];      // (row << ncb | col) contribution of the high tile bits
   uint16_t dstlo[64];      // (row << ncb | col) contribution of the low 6 state bits
@@ -168,6 +173,19 @@ __device__ __forceinline__ uint32_t mnmaj_off(uint32_t kk, uint32_t col) {
 // Output staging (fp32, address order) with a 16-byte XOR swizzle against bank conflicts.
 __device__ __forceinline__ uint32_t stage_idx(uint32_t t) { return t ^ (((t >> 7) & 7u) << 2); }
 
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+
+// One bulk copy global -> this CTA's shared memory, completing on `bar` (no multicast).
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+
 template <int KQ>
 __global__ void __launch_bounds__(kTcThreads, 1) k_tc_dense(float* __restrict__ re, float* __restrict__ im,
                                                             uint64_t ntiles, const uint4* __restrict__ wpack,
@@ -181,13 +199,15 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_dense(float* __restrict__ 
   uint8_t* a_hi = smem;
   uint8_t* a_lo = a_hi + kABytes;
   uint8_t* bbuf = a_lo + kABytes;                  // slot s: hi at bbuf + s*2*B, lo right after
-  float* stage = reinterpret_cast<float*>(bbuf + kBSlots * 2 * kBBytes);  // re [TILE], im [TILE]
-  uint64_t* bars = reinterpret_cast<uint64_t*>(stage + 2 * kTileAmps);
-  uint64_t* bfull = bars;        // [3] loaders -> MMA
-  uint64_t* bfree = bars + 3;    // [3] MMA commit -> loaders
-  uint64_t* dfull = bars + 6;    // [2] MMA commit -> epilogue
-  uint64_t* dfree = bars + 8;    // [2] epilogue -> MMA
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 10);
+  float* io = reinterpret_cast<float*>(bbuf + kBSlots * 2 * kBBytes);  // slot s: re [4096], im [4096]
+  uint64_t* bars = reinterpret_cast<uint64_t*>(io + kIoSlots * 2 * kTileAmps);
+  uint64_t* iofull = bars;       // [3] TMA complete_tx -> converters
+  uint64_t* ioempty = bars + 3;  // [3] epilogue -> producer
+  uint64_t* bfull = bars + 6;    // [2] converters -> MMA
+  uint64_t* bfree = bars + 8;    // [2] MMA commit -> converters
+  uint64_t* dfull = bars + 10;   // [2] MMA commit -> epilogue
+  uint64_t* dfree = bars + 12;   // [2] epilogue -> MMA
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 14);
   uint64_t* s_hioff = reinterpret_cast<uint64_t*>(bars + 16);
   uint16_t* s_dhi = reinterpret_cast<uint16_t*>(s_hioff + 64);
   uint16_t* s_dlo = s_dhi + 64;
@@ -212,11 +232,13 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_dense(float* __restrict__ 
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   if (tid == 0) {
-    for (int s = 0; s < kBSlots; ++s) {
-      mbar_init(&bfull[s], kLoadThreads);
-      mbar_init(&bfree[s], 1);
+    for (int s = 0; s < kIoSlots; ++s) {
+      mbar_init(&iofull[s], 1);
+      mbar_init(&ioempty[s], kEpiThreads);
     }
     for (int s = 0; s < 2; ++s) {
+      mbar_init(&bfull[s], kCvtThreads);
+      mbar_init(&bfree[s], 1);
       mbar_init(&dfull[s], 1);
       mbar_init(&dfree[s], kEpiThreads);
     }
@@ -241,80 +263,86 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_dense(float* __restrict__ 
   };
   const uint64_t my_tiles = uint64_t(blockIdx.x) < ntiles ? (ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
 
-  if (warp < kLoadWarps) {
-    // ============================ loaders: global -> registers -> bf16 hi/lo B buffers
-    float4 rr[kLoadDepth][kVL], ri[kLoadDepth][kVL];
-    auto load = [&](uint64_t i, float4 (&xr)[kVL], float4 (&xi)[kVL]) {
-      const uint64_t base = tile_base(blockIdx.x + i * gridDim.x);
-#pragma unroll
-      for (int j = 0; j < kVL; ++j) {
-        const int t = (tid + j * kLoadThreads) * 4, tlo = t & 63, thi = t >> 6;
-        const uint64_t a = base + s_hioff[thi] + uint64_t(tlo);
-        xr[j] = __ldcs(reinterpret_cast<const float4*>(re + a));
-        xi[j] = __ldcs(reinterpret_cast<const float4*>(im + a));
+  if (warp == kProdWarp) {
+    // ============================ producer: TMA bulk copies of the tile's contiguous runs
+    const uint32_t rb = p.runbits, nruns = uint32_t(kTileAmps) >> rb, run_bytes = 4u << rb;
+    for (uint64_t i = 0; i < my_tiles; ++i) {
+      const uint32_t slot = uint32_t(i % kIoSlots), par = uint32_t((i / kIoSlots) & 1);
+      bool ok = true;
+      if (lane == 0) {
+        ok = mbar_wait(&ioempty[slot], par ^ 1u);
+        if (ok) mbar_arrive_expect_tx(&iofull[slot], kIoBytes);
+        else atomicExch(err, 1);
       }
-    };
+      ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
+      if (!ok) break;
+      const uint64_t base = tile_base(blockIdx.x + i * gridDim.x);
+      float* dre = io + slot * 2 * kTileAmps;
+      float* dim_ = dre + kTileAmps;
+      for (uint32_t j = lane; j < nruns; j += 32) {
+        const uint32_t t0 = j << rb;
+        const uint64_t a = base + s_hioff[t0 >> 6];
+        bulk_g2s(dre + t0, re + a, run_bytes, &iofull[slot]);
+        bulk_g2s(dim_ + t0, im + a, run_bytes, &iofull[slot]);
+      }
+    }
+  } else if (warp < kCvtWarps) {
+    // ============================ converters: staged fp32 -> bf16 hi/lo B buffers
+    for (uint64_t i = 0; i < my_tiles; ++i) {
+      const uint32_t slot = uint32_t(i % kIoSlots), par = uint32_t((i / kIoSlots) & 1);
+      const uint32_t bs = uint32_t(i & 1), bpar = uint32_t((i >> 1) & 1);
+      if (!mbar_wait(&iofull[slot], par) || !mbar_wait(&bfree[bs], bpar ^ 1u)) {
+        atomicExch(err, 1);
+        break;
+      }
+      const float* sre = io + slot * 2 * kTileAmps;
+      const float* sim = sre + kTileAmps;
+      uint8_t* b_hi = bbuf + bs * 2 * kBBytes;
+      uint8_t* b_lo = b_hi + kBBytes;
 #pragma unroll
-    for (int r = 0; r < kLoadDepth; ++r)
-      if (uint64_t(r) < my_tiles) load(r, rr[r], ri[r]);
-    bool ok = true;
-    for (uint64_t i0 = 0; i0 < my_tiles && ok; i0 += kLoadDepth) {
+      for (int j = 0; j < kVC; ++j) {
+        const int t = (tid + j * kCvtThreads) * 4, tlo = t & 63, thi = t >> 6;
+        const float4 xr = *reinterpret_cast<const float4*>(sre + t);
+        const float4 xi = *reinterpret_cast<const float4*>(sim + t);
+        const float vr[4] = {xr.x, xr.y, xr.z, xr.w};
+        const float vi[4] = {xi.x, xi.y, xi.z, xi.w};
+        if (p.bmode == 2) {
 #pragma unroll
-      for (int r = 0; r < kLoadDepth; ++r) {
-        const uint64_t i = i0 + r;
-        if (i >= my_tiles || !ok) break;
-        const uint32_t slot = uint32_t(i % kBSlots), par = uint32_t((i / kBSlots) & 1);
-        if (!mbar_wait(&bfree[slot], par ^ 1u)) {
-          atomicExch(err, 1);
-          ok = false;
-          break;
-        }
-        uint8_t* b_hi = bbuf + slot * 2 * kBBytes;
-        uint8_t* b_lo = b_hi + kBBytes;
-#pragma unroll
-        for (int j = 0; j < kVL; ++j) {
-          const int t = (tid + j * kLoadThreads) * 4, tlo = t & 63, thi = t >> 6;
-          const float vr[4] = {rr[r][j].x, rr[r][j].y, rr[r][j].z, rr[r][j].w};
-          const float vi[4] = {ri[r][j].x, ri[r][j].y, ri[r][j].z, ri[r][j].w};
-          if (p.bmode == 2) {
-#pragma unroll
-            for (int e = 0; e < 4; ++e) {
-              const uint32_t d = uint32_t(s_dlo[tlo + e]) + s_dhi[thi];
-              const uint32_t s = d >> NCB, c = d & CMASK;
-              const uint32_t kb = (c >> 6) * KR, cl = c & 63u;
-              const uint32_t o_re = b_mn ? mnmaj_off(kb + s, cl) : kmaj_off(cl, kb + s, 64);
-              const uint32_t o_im = b_mn ? mnmaj_off(kb + M2 + s, cl) : kmaj_off(cl, kb + M2 + s, 64);
-              __nv_bfloat16 h, l;
-              split_bf16(vr[e], h, l);
-              *reinterpret_cast<__nv_bfloat16*>(b_hi + o_re) = h;
-              *reinterpret_cast<__nv_bfloat16*>(b_lo + o_re) = l;
-              split_bf16(vi[e], h, l);
-              *reinterpret_cast<__nv_bfloat16*>(b_hi + o_im) = h;
-              *reinterpret_cast<__nv_bfloat16*>(b_lo + o_im) = l;
-            }
-          } else {
-            // four consecutive columns of row s (MN-major) or four consecutive rows of column c
-            const uint32_t d = uint32_t(s_dlo[tlo]) + s_dhi[thi];
+          for (int e = 0; e < 4; ++e) {
+            const uint32_t d = uint32_t(s_dlo[tlo + e]) + s_dhi[thi];
             const uint32_t s = d >> NCB, c = d & CMASK;
             const uint32_t kb = (c >> 6) * KR, cl = c & 63u;
             const uint32_t o_re = b_mn ? mnmaj_off(kb + s, cl) : kmaj_off(cl, kb + s, 64);
             const uint32_t o_im = b_mn ? mnmaj_off(kb + M2 + s, cl) : kmaj_off(cl, kb + M2 + s, 64);
-            __nv_bfloat16 hr[4], lr[4], hm[4], lm[4];
-#pragma unroll
-            for (int e = 0; e < 4; ++e) {
-              split_bf16(vr[e], hr[e], lr[e]);
-              split_bf16(vi[e], hm[e], lm[e]);
-            }
-            *reinterpret_cast<uint2*>(b_hi + o_re) = pack4(hr);
-            *reinterpret_cast<uint2*>(b_lo + o_re) = pack4(lr);
-            *reinterpret_cast<uint2*>(b_hi + o_im) = pack4(hm);
-            *reinterpret_cast<uint2*>(b_lo + o_im) = pack4(lm);
+            __nv_bfloat16 h, l;
+            split_bf16(vr[e], h, l);
+            *reinterpret_cast<__nv_bfloat16*>(b_hi + o_re) = h;
+            *reinterpret_cast<__nv_bfloat16*>(b_lo + o_re) = l;
+            split_bf16(vi[e], h, l);
+            *reinterpret_cast<__nv_bfloat16*>(b_hi + o_im) = h;
+            *reinterpret_cast<__nv_bfloat16*>(b_lo + o_im) = l;
           }
+        } else {
+          // four consecutive columns of row s (MN-major) or four consecutive rows of column c
+          const uint32_t d = uint32_t(s_dlo[tlo]) + s_dhi[thi];
+          const uint32_t s = d >> NCB, c = d & CMASK;
+          const uint32_t kb = (c >> 6) * KR, cl = c & 63u;
+          const uint32_t o_re = b_mn ? mnmaj_off(kb + s, cl) : kmaj_off(cl, kb + s, 64);
+          const uint32_t o_im = b_mn ? mnmaj_off(kb + M2 + s, cl) : kmaj_off(cl, kb + M2 + s, 64);
+          __nv_bfloat16 hr[4], lr[4], hm[4], lm[4];
+#pragma unroll
+          for (int e = 0; e < 4; ++e) {
+            split_bf16(vr[e], hr[e], lr[e]);
+            split_bf16(vi[e], hm[e], lm[e]);
+          }
+          *reinterpret_cast<uint2*>(b_hi + o_re) = pack4(hr);
+          *reinterpret_cast<uint2*>(b_lo + o_re) = pack4(lr);
+          *reinterpret_cast<uint2*>(b_hi + o_im) = pack4(hm);
+          *reinterpret_cast<uint2*>(b_lo + o_im) = pack4(lm);
         }
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        mbar_arrive(&bfull[slot]);
-        if (i + kLoadDepth < my_tiles) load(i + kLoadDepth, rr[r], ri[r]);
       }
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      mbar_arrive(&bfull[bs]);
     }
   } else if (warp == kMmaWarp) {
     // ============================ MMA issue: one lane
@@ -324,15 +352,14 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_dense(float* __restrict__ 
       const uint32_t a_hi_s = smem_u32(a_hi), a_lo_s = smem_u32(a_lo);
       const uint32_t b_lbo = b_mn ? uint32_t(kMmaK) * 128u : 16u;
       for (uint64_t i = 0; i < my_tiles; ++i) {
-        const uint32_t slot = uint32_t(i % kBSlots), par = uint32_t((i / kBSlots) & 1);
-        const uint32_t ds = uint32_t(i & 1), dpar = uint32_t((i >> 1) & 1);
-        if (!mbar_wait(&bfull[slot], par) || !mbar_wait(&dfree[ds], dpar ^ 1u)) {
+        const uint32_t bs = uint32_t(i & 1), par = uint32_t((i >> 1) & 1);
+        if (!mbar_wait(&bfull[bs], par) || !mbar_wait(&dfree[bs], par ^ 1u)) {
           atomicExch(err, 1);
           break;
         }
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        const uint32_t b_hi_s = smem_u32(bbuf + slot * 2 * kBBytes), b_lo_s = b_hi_s + kBBytes;
-        const uint32_t d_tmem = tmem + ds * kMmaN;
+        const uint32_t b_hi_s = smem_u32(bbuf + bs * 2 * kBBytes), b_lo_s = b_hi_s + kBBytes;
+        const uint32_t d_tmem = tmem + bs * kMmaN;
 #pragma unroll 1
         for (int s = 0; s < kMmaK / 16; ++s) {
           const uint32_t ak = (s >> 2) * (128u * 128u) + (s & 3) * 32u;
@@ -343,20 +370,20 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_dense(float* __restrict__ 
           mma_bf16(d_tmem, dah, dbl, idesc, 1u);
           mma_bf16(d_tmem, dah, dbh, idesc, 1u);
         }
-        mma_commit(&bfree[slot]);  // B buffer consumed
-        mma_commit(&dfull[ds]);    // accumulator ready
+        mma_commit(&bfree[bs]);  // B buffer consumed
+        mma_commit(&dfull[bs]);  // accumulator ready
       }
     }
     __syncwarp();
   } else {
-    // ============================ epilogue: TMEM -> staging -> global
+    // ============================ epilogue: TMEM -> the tile's staging slot -> global
     const int quad = warp & 3;                      // TMEM lane quadrant this warp may access
     const int et = tid - kEpiWarp0 * 32;            // 0..127
     const uint32_t m = uint32_t(quad * 32 + lane);  // accumulator row = TMEM lane
     const uint32_t blk = m / KR, r = m % KR;
     const uint32_t s = r & uint32_t(M2 - 1), part = r >> KQ;
-    float* st = stage + part * kTileAmps;
     for (uint64_t i = 0; i < my_tiles; ++i) {
+      const uint32_t slot = uint32_t(i % kIoSlots);
       const uint32_t ds = uint32_t(i & 1), dpar = uint32_t((i >> 1) & 1);
       if (!mbar_wait(&dfull[ds], dpar)) {
         atomicExch(err, 1);
@@ -369,8 +396,9 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_dense(float* __restrict__ 
       for (int cb = 0; cb < 4; ++cb) tmem_ld16(taddr + uint32_t(cb * 16), v[cb]);
       asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
       asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-      mbar_arrive(&dfree[ds]);     // accumulator may be overwritten now
-      named_sync(1, kEpiThreads);  // the previous tile's write-back has finished reading staging
+      mbar_arrive(&dfree[ds]);  // accumulator may be overwritten now
+      // the converters finished reading this slot before the MMAs that produced v were issued
+      float* st = io + slot * 2 * kTileAmps + part * kTileAmps;
       const uint32_t tr = s_trow[s];
       const uint16_t* tc = s_tcol + blk * 64;
       if (p.bmode == 0) {
@@ -389,16 +417,20 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_dense(float* __restrict__ 
 #pragma unroll
           for (int q = 0; q < 16; ++q) st[stage_idx(tr + tc[cb * 16 + q])] = __uint_as_float(v[cb][q]);
       }
-      named_sync(1, kEpiThreads);  // staging complete
+      named_sync(1, kEpiThreads);  // the whole result is staged
+      const float* sre = io + slot * 2 * kTileAmps;
       const uint64_t base = tile_base(blockIdx.x + i * gridDim.x);
 #pragma unroll
       for (int j = 0; j < kVE; ++j) {
         const int t = (et + j * kEpiThreads) * 4, tlo = t & 63, thi = t >> 6;
         const uint64_t a = base + s_hioff[thi] + uint64_t(tlo);
         const uint32_t si = stage_idx(uint32_t(t));
-        __stcs(reinterpret_cast<float4*>(re + a), *reinterpret_cast<const float4*>(stage + si));
-        __stcs(reinterpret_cast<float4*>(im + a), *reinterpret_cast<const float4*>(stage + kTileAmps + si));
+        __stcs(reinterpret_cast<float4*>(re + a), *reinterpret_cast<const float4*>(sre + si));
+        __stcs(reinterpret_cast<float4*>(im + a), *reinterpret_cast<const float4*>(sre + kTileAmps + si));
       }
+      // this thread's reads of the slot are done; the producer may refill it once all 128 arrive
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      mbar_arrive(&ioempty[slot]);
     }
   }
   __syncwarp();  // roles may leave their loops at different iterations after a timeout
@@ -508,6 +540,9 @@ static void launch_tc_k(const LaunchEnv& env, float* re, float* im, uint32_t n, 
       if (col_rank[b] >= 0 && ((c >> col_rank[b]) & 1)) t |= 1u << rank_of(b);
     p.tcol[c] = uint16_t(t);
   }
+  uint32_t rb = 0;
+  while (rb < uint32_t(kTileBits) && tbits[rb] == rb) ++rb;
+  p.runbits = rb;
   const bool low_cols = gate_rank[0] < 0 && gate_rank[1] < 0;
   const bool low_rows = gate_rank[0] == 0 && gate_rank[1] == 1;
   p.bmode = low_cols ? 0u : (low_rows ? 1u : 2u);
