@@ -29,11 +29,15 @@
 // layout and copied in once per CTA. Every mbarrier wait is bounded: a wait that runs out sets the
 // context error flag and that role stops; the host reports QSVB_E_TIMEOUT.
 
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 
 #include "qsvb_internal.h"
@@ -55,16 +59,17 @@ constexpr int kMmaWarp = kCvtWarps + 1;                       // warp 9
 constexpr int kEpiWarp0 = kCvtWarps + 2;                      // warps 10..13 (lane quadrants 2,3,0,1)
 constexpr int kTcThreads = (kCvtWarps + 2 + kEpiWarps) * 32;
 constexpr int kBSlots = 2;
-constexpr int kIoSlots = 3;
-constexpr int kTmemCols = 128;                                // two 64-column accumulators
+constexpr int kIoSlots = 4;
+constexpr int kTmemCols = 256;                                // two 64-column accumulators + Whi + Wlo
+constexpr uint32_t kTmemAHi = 128, kTmemALo = 192;           // A operand columns (64 each)
 constexpr int kVC = kTileAmps / 4 / kCvtThreads;              // float4 per component per converter
 constexpr int kVE = kTileAmps / 4 / kEpiThreads;              // float4 per component per epilogue thread
-constexpr uint32_t kABytes = 128u * kMmaK * 2u;               // one of Whi / Wlo
+constexpr uint32_t kABytes = 128u * kMmaK * 2u;               // one of Whi / Wlo (global image)
 constexpr uint32_t kBBytes = uint32_t(kMmaN) * kMmaK * 2u;    // one of Xhi / Xlo
 constexpr uint32_t kIoBytes = kTileAmps * 8u;                 // re [4096] + im [4096] fp32
 constexpr long long kWaitBudget = 1ll << 31;                  // clock64 cycles (~1 s)
-constexpr size_t kTcSmem = 1024 + 2 * size_t(kABytes) + kBSlots * 2 * size_t(kBBytes) + kIoSlots * size_t(kIoBytes) +
-                           128 + 64 * 8 + 3 * 64 * 2 + 256 * 2;
+constexpr size_t kTcSmem = 1024 + kBSlots * 2 * size_t(kBBytes) + kIoSlots * size_t(kIoBytes) +
+                           144 + 64 * 8 + 3 * 64 * 2 + 256 * 2;
 
 struct TcParams {
   uint32_t hibits[6];      // tile bits above the 6 lowest state bits (ascending)
@@ -76,6 +81,11 @@ struct TcParams {
   uint16_t trow[64];       // address-order tile index of gate row s
   uint16_t tcol[256];      // address-order tile index of column c
   uint32_t bmode;          // 0: MN-major vector, 1: K-major vector, 2: scalar stores
+  uint32_t tcl[16];        // tcol[q] for q < 16 (uniform; read straight from the parameter bank)
+  uint32_t tm_rank;        // > 0: the producer uses one tensor-map TMA per component per tile
+  uint32_t tm_start[5];    // first state bit of each tensor dimension (runs of tile / non-tile bits)
+  uint32_t tm_len[5];      // bits in that run
+  uint32_t tm_tile[5];     // 1 when the run holds tile bits (coordinate 0, box = whole run)
 };
 
 // ----------------------------------------------------------------------------- PTX helpers
@@ -99,6 +109,16 @@ __device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint64_t a, uint64_t b
       "setp.ne.b32 p, %4, 0;\n\t"
       "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d_tmem),
       "l"(a), "l"(b), "r"(idesc), "r"(acc));
+}
+
+// A from tensor memory (M rows in lanes, K packed two bf16 per 32-bit column), B from shared.
+__device__ __forceinline__ void mma_bf16_ts(uint32_t d_tmem, uint32_t a_tmem, uint64_t b, uint32_t idesc,
+                                            uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, p;\n\t}\n" ::"r"(d_tmem),
+      "r"(a_tmem), "l"(b), "r"(idesc), "r"(acc));
 }
 
 __device__ __forceinline__ void mma_commit(uint64_t* bar) {
@@ -135,6 +155,14 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
   return true;
 }
 
+// Same, adding the cycles spent waiting to `acc` (stall profiling).
+__device__ __forceinline__ bool mbar_wait_t(uint64_t* bar, uint32_t parity, long long& acc) {
+  const long long t0 = clock64();
+  const bool ok = mbar_wait(bar, parity);
+  acc += clock64() - t0;
+  return ok;
+}
+
 // 32 lanes x 16 fp32 columns, no wait (the caller issues tcgen05.wait::ld once for a batch).
 __device__ __forceinline__ void tmem_ld16(uint32_t addr, uint32_t (&r)[16]) {
   asm volatile(
@@ -142,6 +170,22 @@ __device__ __forceinline__ void tmem_ld16(uint32_t addr, uint32_t (&r)[16]) {
       : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
         "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
       : "r"(addr));
+}
+
+// 32 lanes x 64 32-bit columns from registers (one lane per thread of the warp).
+__device__ __forceinline__ void tmem_st64(uint32_t addr, const uint32_t (&r)[64]) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x64.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,"
+      "%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,%32,%33,%34,%35,%36,%37,%38,%39,%40,%41,%42,"
+      "%43,%44,%45,%46,%47,%48,%49,%50,%51,%52,%53,%54,%55,%56,%57,%58,%59,%60,%61,%62,%63,%64};\n" ::"r"(addr),
+      "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]), "r"(r[8]), "r"(r[9]),
+      "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]), "r"(r[15]), "r"(r[16]), "r"(r[17]), "r"(r[18]),
+      "r"(r[19]), "r"(r[20]), "r"(r[21]), "r"(r[22]), "r"(r[23]), "r"(r[24]), "r"(r[25]), "r"(r[26]), "r"(r[27]),
+      "r"(r[28]), "r"(r[29]), "r"(r[30]), "r"(r[31]), "r"(r[32]), "r"(r[33]), "r"(r[34]), "r"(r[35]), "r"(r[36]),
+      "r"(r[37]), "r"(r[38]), "r"(r[39]), "r"(r[40]), "r"(r[41]), "r"(r[42]), "r"(r[43]), "r"(r[44]), "r"(r[45]),
+      "r"(r[46]), "r"(r[47]), "r"(r[48]), "r"(r[49]), "r"(r[50]), "r"(r[51]), "r"(r[52]), "r"(r[53]), "r"(r[54]),
+      "r"(r[55]), "r"(r[56]), "r"(r[57]), "r"(r[58]), "r"(r[59]), "r"(r[60]), "r"(r[61]), "r"(r[62]), "r"(r[63])
+      : "memory");
 }
 
 __device__ __forceinline__ void named_sync(uint32_t id, uint32_t nthreads) {
@@ -178,6 +222,35 @@ __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t by
                : "memory");
 }
 
+// One tiled tensor-map copy global -> this CTA's shared memory (no multicast), rank 1..5.
+__device__ __forceinline__ void tma_tensor_g2s(void* dst, const CUtensorMap* map, const int (&c)[5], uint32_t rank,
+                                               uint64_t* bar) {
+  const uint64_t m = reinterpret_cast<uint64_t>(map);
+  const uint32_t d = smem_u32(dst), b = smem_u32(bar);
+  switch (rank) {
+    case 1:
+      asm volatile("cp.async.bulk.tensor.1d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2}], [%3];"
+                   ::"r"(d), "l"(m), "r"(c[0]), "r"(b) : "memory");
+      break;
+    case 2:
+      asm volatile("cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+                   ::"r"(d), "l"(m), "r"(c[0]), "r"(c[1]), "r"(b) : "memory");
+      break;
+    case 3:
+      asm volatile("cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
+                   ::"r"(d), "l"(m), "r"(c[0]), "r"(c[1]), "r"(c[2]), "r"(b) : "memory");
+      break;
+    case 4:
+      asm volatile("cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], [%6];"
+                   ::"r"(d), "l"(m), "r"(c[0]), "r"(c[1]), "r"(c[2]), "r"(c[3]), "r"(b) : "memory");
+      break;
+    default:
+      asm volatile("cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5, %6}], [%7];"
+                   ::"r"(d), "l"(m), "r"(c[0]), "r"(c[1]), "r"(c[2]), "r"(c[3]), "r"(c[4]), "r"(b) : "memory");
+      break;
+  }
+}
+
 // One bulk copy global -> this CTA's shared memory, completing on `bar` (no multicast).
 __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
   asm volatile(
@@ -189,36 +262,34 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
 template <int KQ>
 __global__ void __launch_bounds__(kTcThreads, 1) k_tc_dense(float* __restrict__ re, float* __restrict__ im,
                                                             uint64_t ntiles, const uint4* __restrict__ wpack,
-                                                            TcParams p, int* err) {
+                                                            TcParams p, int* err, long long* prof,
+                                                            const __grid_constant__ CUtensorMap tm_re,
+                                                            const __grid_constant__ CUtensorMap tm_im) {
   constexpr int M2 = 1 << KQ;      // complex gate rows
   constexpr int KR = 2 * M2;       // real rows of one block
   constexpr int NCB = kTileBits - KQ;
   constexpr uint32_t CMASK = (1u << NCB) - 1u;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  uint8_t* a_hi = smem;
-  uint8_t* a_lo = a_hi + kABytes;
-  uint8_t* bbuf = a_lo + kABytes;                  // slot s: hi at bbuf + s*2*B, lo right after
+  uint8_t* bbuf = smem;                            // slot s: hi at bbuf + s*2*B, lo right after
   float* io = reinterpret_cast<float*>(bbuf + kBSlots * 2 * kBBytes);  // slot s: re [4096], im [4096]
   uint64_t* bars = reinterpret_cast<uint64_t*>(io + kIoSlots * 2 * kTileAmps);
-  uint64_t* iofull = bars;       // [3] TMA complete_tx -> converters
-  uint64_t* ioempty = bars + 3;  // [3] epilogue -> producer
-  uint64_t* bfull = bars + 6;    // [2] converters -> MMA
-  uint64_t* bfree = bars + 8;    // [2] MMA commit -> converters
-  uint64_t* dfull = bars + 10;   // [2] MMA commit -> epilogue
-  uint64_t* dfree = bars + 12;   // [2] epilogue -> MMA
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 14);
-  uint64_t* s_hioff = reinterpret_cast<uint64_t*>(bars + 16);
+  uint64_t* iofull = bars;       // [4] TMA complete_tx -> converters
+  uint64_t* ioempty = bars + 4;  // [4] epilogue -> producer
+  uint64_t* bfull = bars + 8;    // [2] converters -> MMA
+  uint64_t* bfree = bars + 10;   // [2] MMA commit -> converters
+  uint64_t* dfull = bars + 12;   // [2] MMA commit -> epilogue
+  uint64_t* dfree = bars + 14;   // [2] epilogue -> MMA
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 16);
+  uint64_t* s_hioff = reinterpret_cast<uint64_t*>(bars + 18);
   uint16_t* s_dhi = reinterpret_cast<uint16_t*>(s_hioff + 64);
   uint16_t* s_dlo = s_dhi + 64;
   uint16_t* s_trow = s_dlo + 64;
   uint16_t* s_tcol = s_trow + 64;  // 256 entries
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  {
-    uint4* dst = reinterpret_cast<uint4*>(a_hi);
-    for (uint32_t i = tid; i < 2 * kABytes / 16; i += kTcThreads) dst[i] = wpack[i];
-  }
+  const long long t_start = clock64();
+  long long w0 = 0, w1 = 0, w2 = 0, w3 = 0, w4 = 0;  // per-role stall counters (stall profiling only)
   for (int i = tid; i < 64; i += kTcThreads) {
     s_hioff[i] = p.hioff[i];
     s_dhi[i] = p.dsthi[i];
@@ -250,6 +321,29 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_dense(float* __restrict__ 
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = *tmem_slot;
   const uint32_t b_mn = p.bmode == 0 ? 1u : 0u;
+  if (warp >= kEpiWarp0) {
+    // A (Whi, Wlo) into tensor memory: the thread owning TMEM lane m writes row m of each, 64
+    // 32-bit columns of packed bf16 pairs (element 2j in the low half).
+    const uint32_t quad = uint32_t(warp & 3), m = quad * 32 + uint32_t(lane);
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      uint32_t r[64];
+      const uint4* src = wpack + (size_t(h) * 128 + m) * 16;
+#pragma unroll
+      for (int q = 0; q < 16; ++q) {
+        const uint4 u = src[q];
+        r[4 * q] = u.x;
+        r[4 * q + 1] = u.y;
+        r[4 * q + 2] = u.z;
+        r[4 * q + 3] = u.w;
+      }
+      tmem_st64(tmem + ((quad * 32) << 16) + (h == 0 ? kTmemAHi : kTmemALo), r);
+    }
+    asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 
   auto tile_base = [&](uint64_t tile) {
     uint64_t base = tile << 6;
@@ -270,7 +364,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_dense(float* __restrict__ 
       const uint32_t slot = uint32_t(i % kIoSlots), par = uint32_t((i / kIoSlots) & 1);
       bool ok = true;
       if (lane == 0) {
-        ok = mbar_wait(&ioempty[slot], par ^ 1u);
+        ok = mbar_wait_t(&ioempty[slot], par ^ 1u, w0);
         if (ok) mbar_arrive_expect_tx(&iofull[slot], kIoBytes);
         else atomicExch(err, 1);
       }
@@ -279,6 +373,17 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_dense(float* __restrict__ 
       const uint64_t base = tile_base(blockIdx.x + i * gridDim.x);
       float* dre = io + slot * 2 * kTileAmps;
       float* dim_ = dre + kTileAmps;
+      if (p.tm_rank > 0) {
+        if (lane == 0) {
+          int c[5];
+#pragma unroll
+          for (uint32_t d = 0; d < 5; ++d)
+            c[d] = (d < p.tm_rank && !p.tm_tile[d]) ? int((base >> p.tm_start[d]) & ((1ull << p.tm_len[d]) - 1ull)) : 0;
+          tma_tensor_g2s(dre, &tm_re, c, p.tm_rank, &iofull[slot]);
+          tma_tensor_g2s(dim_, &tm_im, c, p.tm_rank, &iofull[slot]);
+        }
+        continue;
+      }
       for (uint32_t j = lane; j < nruns; j += 32) {
         const uint32_t t0 = j << rb;
         const uint64_t a = base + s_hioff[t0 >> 6];
@@ -291,7 +396,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_dense(float* __restrict__ 
     for (uint64_t i = 0; i < my_tiles; ++i) {
       const uint32_t slot = uint32_t(i % kIoSlots), par = uint32_t((i / kIoSlots) & 1);
       const uint32_t bs = uint32_t(i & 1), bpar = uint32_t((i >> 1) & 1);
-      if (!mbar_wait(&iofull[slot], par) || !mbar_wait(&bfree[bs], bpar ^ 1u)) {
+      if (!mbar_wait_t(&iofull[slot], par, w0) || !mbar_wait_t(&bfree[bs], bpar ^ 1u, w1)) {
         atomicExch(err, 1);
         break;
       }
@@ -299,11 +404,20 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_dense(float* __restrict__ 
       const float* sim = sre + kTileAmps;
       uint8_t* b_hi = bbuf + bs * 2 * kBBytes;
       uint8_t* b_lo = b_hi + kBBytes;
+      // all shared-memory loads first (the B stores below could alias them for the compiler)
+      float4 xra[kVC], xia[kVC];
+      uint32_t dda[kVC];
+#pragma unroll
+      for (int j = 0; j < kVC; ++j) {
+        const int t = (tid + j * kCvtThreads) * 4;
+        xra[j] = *reinterpret_cast<const float4*>(sre + t);
+        xia[j] = *reinterpret_cast<const float4*>(sim + t);
+        dda[j] = uint32_t(s_dlo[t & 63]) + s_dhi[t >> 6];
+      }
 #pragma unroll
       for (int j = 0; j < kVC; ++j) {
         const int t = (tid + j * kCvtThreads) * 4, tlo = t & 63, thi = t >> 6;
-        const float4 xr = *reinterpret_cast<const float4*>(sre + t);
-        const float4 xi = *reinterpret_cast<const float4*>(sim + t);
+        const float4 xr = xra[j], xi = xia[j];
         const float vr[4] = {xr.x, xr.y, xr.z, xr.w};
         const float vi[4] = {xi.x, xi.y, xi.z, xi.w};
         if (p.bmode == 2) {
@@ -324,7 +438,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_dense(float* __restrict__ 
           }
         } else {
           // four consecutive columns of row s (MN-major) or four consecutive rows of column c
-          const uint32_t d = uint32_t(s_dlo[tlo]) + s_dhi[thi];
+          const uint32_t d = dda[j];
           const uint32_t s = d >> NCB, c = d & CMASK;
           const uint32_t kb = (c >> 6) * KR, cl = c & 63u;
           const uint32_t o_re = b_mn ? mnmaj_off(kb + s, cl) : kmaj_off(cl, kb + s, 64);
@@ -349,11 +463,10 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_dense(float* __restrict__ 
     if (lane == 0) {
       const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | (b_mn << 16) | (uint32_t(kMmaN >> 3) << 17) |
                              (uint32_t(128 >> 4) << 24);
-      const uint32_t a_hi_s = smem_u32(a_hi), a_lo_s = smem_u32(a_lo);
       const uint32_t b_lbo = b_mn ? uint32_t(kMmaK) * 128u : 16u;
       for (uint64_t i = 0; i < my_tiles; ++i) {
         const uint32_t bs = uint32_t(i & 1), par = uint32_t((i >> 1) & 1);
-        if (!mbar_wait(&bfull[bs], par) || !mbar_wait(&dfree[bs], par ^ 1u)) {
+        if (!mbar_wait_t(&bfull[bs], par, w0) || !mbar_wait_t(&dfree[bs], par ^ 1u, w1)) {
           atomicExch(err, 1);
           break;
         }
@@ -362,13 +475,12 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_dense(float* __restrict__ 
         const uint32_t d_tmem = tmem + bs * kMmaN;
 #pragma unroll 1
         for (int s = 0; s < kMmaK / 16; ++s) {
-          const uint32_t ak = (s >> 2) * (128u * 128u) + (s & 3) * 32u;
           const uint32_t bk = b_mn ? uint32_t(s) * 2048u : (s >> 2) * (64u * 128u) + (s & 3) * 32u;
-          const uint64_t dah = sw128_desc(a_hi_s + ak, 16u, 1024u), dal = sw128_desc(a_lo_s + ak, 16u, 1024u);
+          const uint32_t tah = tmem + kTmemAHi + uint32_t(s) * 8u, tal = tmem + kTmemALo + uint32_t(s) * 8u;
           const uint64_t dbh = sw128_desc(b_hi_s + bk, b_lbo, 1024u), dbl = sw128_desc(b_lo_s + bk, b_lbo, 1024u);
-          mma_bf16(d_tmem, dal, dbh, idesc, s > 0 ? 1u : 0u);
-          mma_bf16(d_tmem, dah, dbl, idesc, 1u);
-          mma_bf16(d_tmem, dah, dbh, idesc, 1u);
+          mma_bf16_ts(d_tmem, tal, dbh, idesc, s > 0 ? 1u : 0u);
+          mma_bf16_ts(d_tmem, tah, dbl, idesc, 1u);
+          mma_bf16_ts(d_tmem, tah, dbh, idesc, 1u);
         }
         mma_commit(&bfree[bs]);  // B buffer consumed
         mma_commit(&dfull[bs]);  // accumulator ready
@@ -382,14 +494,21 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_dense(float* __restrict__ 
     const uint32_t m = uint32_t(quad * 32 + lane);  // accumulator row = TMEM lane
     const uint32_t blk = m / KR, r = m % KR;
     const uint32_t s = r & uint32_t(M2 - 1), part = r >> KQ;
+    // address-order index of (row s, column blk*64 + cb*16 + q) = tr + tch[cb] + tcl[q]: the column
+    // map is a bit deposit, so it splits additively into the low 4 column bits and the rest
+    const uint32_t tr = s_trow[s];
+    uint32_t tch[4];
+#pragma unroll
+    for (int cb = 0; cb < 4; ++cb) tch[cb] = s_tcol[blk * 64 + cb * 16];
     for (uint64_t i = 0; i < my_tiles; ++i) {
       const uint32_t slot = uint32_t(i % kIoSlots);
       const uint32_t ds = uint32_t(i & 1), dpar = uint32_t((i >> 1) & 1);
-      if (!mbar_wait(&dfull[ds], dpar)) {
+      if (!mbar_wait_t(&dfull[ds], dpar, w0)) {
         atomicExch(err, 1);
         break;
       }
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const long long ta = clock64();
       uint32_t v[4][16];
       const uint32_t taddr = tmem + (uint32_t(quad * 32) << 16) + ds * kMmaN;
 #pragma unroll
@@ -397,16 +516,16 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_dense(float* __restrict__ 
       asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
       asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
       mbar_arrive(&dfree[ds]);  // accumulator may be overwritten now
+      const long long tb = clock64();
+      w2 += tb - ta;
       // the converters finished reading this slot before the MMAs that produced v were issued
       float* st = io + slot * 2 * kTileAmps + part * kTileAmps;
-      const uint32_t tr = s_trow[s];
-      const uint16_t* tc = s_tcol + blk * 64;
       if (p.bmode == 0) {
 #pragma unroll
         for (int cb = 0; cb < 4; ++cb)
 #pragma unroll
           for (int q = 0; q < 4; ++q) {
-            const uint32_t t = tr + tc[cb * 16 + q * 4];
+            const uint32_t t = tr + tch[cb] + p.tcl[q * 4];
             *reinterpret_cast<float4*>(st + stage_idx(t)) =
                 make_float4(__uint_as_float(v[cb][4 * q]), __uint_as_float(v[cb][4 * q + 1]),
                             __uint_as_float(v[cb][4 * q + 2]), __uint_as_float(v[cb][4 * q + 3]));
@@ -415,9 +534,13 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_dense(float* __restrict__ 
 #pragma unroll
         for (int cb = 0; cb < 4; ++cb)
 #pragma unroll
-          for (int q = 0; q < 16; ++q) st[stage_idx(tr + tc[cb * 16 + q])] = __uint_as_float(v[cb][q]);
+          for (int q = 0; q < 16; ++q) st[stage_idx(tr + tch[cb] + p.tcl[q])] = __uint_as_float(v[cb][q]);
       }
+      const long long tc0 = clock64();
+      w3 += tc0 - tb;
       named_sync(1, kEpiThreads);  // the whole result is staged
+      const long long ts = clock64();
+      w4 += ts - tc0;
       const float* sre = io + slot * 2 * kTileAmps;
       const uint64_t base = tile_base(blockIdx.x + i * gridDim.x);
 #pragma unroll
@@ -431,6 +554,27 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_dense(float* __restrict__ 
       // this thread's reads of the slot are done; the producer may refill it once all 128 arrive
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       mbar_arrive(&ioempty[slot]);
+      w1 += clock64() - ts;
+    }
+  }
+  if (prof != nullptr) {  // [producer, converter x2, MMA x2, epilogue x5, total] per CTA
+    long long* pc = prof + 12 * blockIdx.x;
+    if (warp == kProdWarp && lane == 0) pc[0] = w0;
+    if (tid == 0) {
+      pc[1] = w0;
+      pc[2] = w1;
+    }
+    if (warp == kMmaWarp && lane == 0) {
+      pc[3] = w0;
+      pc[4] = w1;
+    }
+    if (tid == kEpiWarp0 * 32) {
+      pc[5] = w0;
+      pc[6] = w1;
+      pc[7] = clock64() - t_start;
+      pc[8] = w2;
+      pc[9] = w3;
+      pc[10] = w4;
     }
   }
   __syncwarp();  // roles may leave their loops at different iterations after a timeout
@@ -464,12 +608,13 @@ bool tc_dense_supported(const Sweep& s, uint32_t n) {
 
 size_t tc_matrix_bytes(const Sweep&) { return 2 * size_t(kABytes); }
 
-// A = blockdiag(W, ..., W) (128 / KR copies), W = [[Ur, -Ui], [Ui, Ur]], split into bf16 hi/lo,
-// K-major, 128-byte swizzle, 128 x 128.
+// A = blockdiag(W, ..., W) (128 / KR copies), W = [[Ur, -Ui], [Ui, Ur]], split into bf16 hi/lo.
+// Image for tensor memory: hi then lo, each 128 rows x 64 32-bit words, word j of row m holding
+// elements (2j, 2j+1) of that row (2j in the low half).
 void tc_pack_matrix(const Sweep& s, void* dst) {
   const uint32_t M2 = 1u << s.m, KR = 2 * M2, nblk = 128 / KR;
-  uint8_t* hi = static_cast<uint8_t*>(dst);
-  uint8_t* lo = hi + kABytes;
+  uint16_t* hi = static_cast<uint16_t*>(dst);
+  uint16_t* lo = hi + 128 * 128;
   std::memset(dst, 0, 2 * size_t(kABytes));
   for (uint32_t b = 0; b < nblk; ++b)
     for (uint32_t r = 0; r < KR; ++r)
@@ -480,9 +625,9 @@ void tc_pack_matrix(const Sweep& s, void* dst) {
         else w = k < M2 ? u.imag() : u.real();
         const uint16_t h = bf16_bits_rn(float(w));
         const uint16_t l = bf16_bits_rn(float(w - double(bf16_to_float(h))));
-        const uint32_t o = kmaj_off(b * KR + r, b * KR + k, 128);
-        std::memcpy(hi + o, &h, 2);
-        std::memcpy(lo + o, &l, 2);
+        const size_t o = size_t(b * KR + r) * 128 + (b * KR + k);
+        hi[o] = h;
+        lo[o] = l;
       }
 }
 
@@ -539,10 +684,60 @@ static void launch_tc_k(const LaunchEnv& env, float* re, float* im, uint32_t n, 
     for (uint32_t b = 0; b < n; ++b)
       if (col_rank[b] >= 0 && ((c >> col_rank[b]) & 1)) t |= 1u << rank_of(b);
     p.tcol[c] = uint16_t(t);
+    if (c < 16) p.tcl[c] = t;
   }
   uint32_t rb = 0;
   while (rb < uint32_t(kTileBits) && tbits[rb] == rb) ++rb;
   p.runbits = rb;
+  // Short runs: describe the state as a tensor whose dimensions are the maximal runs of tile /
+  // non-tile bits, so one tiled TMA per component fetches the whole tile in address order.
+  CUtensorMap maps[2];
+  std::memset(maps, 0, sizeof(maps));
+  if (rb <= 8) {
+    std::vector<std::pair<uint32_t, uint32_t>> runs;  // (start, len)
+    std::vector<bool> is_tile;
+    for (uint32_t b = 0; b < n;) {
+      const bool t = gate_rank[b] >= 0 || col_rank[b] >= 0;
+      uint32_t e = b;
+      while (e < n && (gate_rank[e] >= 0 || col_rank[e] >= 0) == t) ++e;
+      runs.push_back({b, e - b});
+      is_tile.push_back(t);
+      b = e;
+    }
+    bool ok = runs.size() <= 5;
+    for (size_t d = 0; d < runs.size() && ok; ++d)
+      if (is_tile[d] && runs[d].second > 8) ok = false;  // box dimensions are at most 256
+    if (ok) {
+      static PFN_cuTensorMapEncodeTiled_v12000 encode = [] {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+          fn = nullptr;
+        return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+      }();
+      if (encode) {
+        cuuint64_t dims[5], strides[4];
+        cuuint32_t box[5], estr[5];
+        for (size_t d = 0; d < runs.size(); ++d) {
+          dims[d] = cuuint64_t(1) << runs[d].second;
+          box[d] = is_tile[d] ? cuuint32_t(1) << runs[d].second : 1;
+          estr[d] = 1;
+          if (d > 0) strides[d - 1] = (cuuint64_t(1) << runs[d].first) * sizeof(float);
+          p.tm_start[d] = runs[d].first;
+          p.tm_len[d] = runs[d].second;
+          p.tm_tile[d] = is_tile[d] ? 1u : 0u;
+        }
+        float* bases[2] = {re, im};
+        bool enc_ok = true;
+        for (int c = 0; c < 2 && enc_ok; ++c)
+          enc_ok = encode(&maps[c], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, cuuint32_t(runs.size()), bases[c], dims, strides,
+                          box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+        if (enc_ok) p.tm_rank = uint32_t(runs.size());
+      }
+    }
+  }
   const bool low_cols = gate_rank[0] < 0 && gate_rank[1] < 0;
   const bool low_rows = gate_rank[0] == 0 && gate_rank[1] == 1;
   p.bmode = low_cols ? 0u : (low_rows ? 1u : 2u);
@@ -553,9 +748,30 @@ static void launch_tc_k(const LaunchEnv& env, float* re, float* im, uint32_t n, 
                                int(cudaSharedmemCarveoutMaxShared)));
   // one persistent CTA per SM (the tensor-memory allocation assumes it)
   const unsigned grid = unsigned(std::max<uint64_t>(1, std::min<uint64_t>(ntiles, uint64_t(env.num_sms))));
+  // QSVB_TC_PROFILE=1: per-role stall cycles, averaged over CTAs, printed to stderr (synchronous)
+  static const bool profile = std::getenv("QSVB_TC_PROFILE") != nullptr;
+  long long* prof = nullptr;
+  if (profile) QSVB_CK(cudaMalloc(&prof, sizeof(long long) * 12 * grid));
+  if (prof) QSVB_CK(cudaMemsetAsync(prof, 0, sizeof(long long) * 12 * grid, env.stream));
   k_tc_dense<KQ><<<grid, kTcThreads, kTcSmem, env.stream>>>(re, im, ntiles, static_cast<const uint4*>(dev_mat), p,
-                                                            env.err_flag);
+                                                            env.err_flag, prof, maps[0], maps[1]);
   QSVB_CK(cudaGetLastError());
+  if (prof) {
+    std::vector<long long> h(12 * size_t(grid));
+    QSVB_CK(cudaMemcpyAsync(h.data(), prof, h.size() * sizeof(long long), cudaMemcpyDeviceToHost, env.stream));
+    QSVB_CK(cudaStreamSynchronize(env.stream));
+    cudaFree(prof);
+    double avg[12] = {0};
+    for (unsigned b = 0; b < grid; ++b)
+      for (int k = 0; k < 12; ++k) avg[k] += double(h[12 * b + k]) / grid;
+    std::fprintf(stderr,
+                 "{\"tc_profile\": {\"k\": %d, \"bmode\": %u, \"tiles_per_cta\": %.1f, \"cycles\": %.0f, "
+                 "\"prod_wait_empty\": %.0f, \"cvt_wait_full\": %.0f, \"cvt_wait_bfree\": %.0f, "
+                 "\"mma_wait_bfull\": %.0f, \"mma_wait_dfree\": %.0f, \"epi_wait_dfull\": %.0f, "
+                 "\"epi_store\": %.0f, \"epi_tmem\": %.0f, \"epi_stage\": %.0f, \"epi_sync\": %.0f}}\n",
+                 KQ, p.bmode, double(ntiles) / grid, avg[7], avg[0], avg[1], avg[2], avg[3], avg[4], avg[5], avg[6],
+                 avg[8], avg[9], avg[10]);
+  }
 }
 
 void launch_tc_dense(const LaunchEnv& env, float* re, float* im, uint32_t n, const Sweep& s, const void* dev_mat) {
