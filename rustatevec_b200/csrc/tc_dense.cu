@@ -83,9 +83,8 @@ struct TcParams {
   uint32_t bmode;          // 0: MN-major vector, 1: K-major vector, 2: scalar stores
   uint32_t tcl[16];        // tcol[q] for q < 16 (uniform; read straight from the parameter bank)
   uint32_t tm_rank;        // > 0: the producer uses one tensor-map TMA per component per tile
-  uint32_t tm_start[5];    // first state bit of each tensor dimension (runs of tile / non-tile bits)
-  uint32_t tm_len[5];      // bits in that run
-  uint32_t tm_tile[5];     // 1 when the run holds tile bits (coordinate 0, box = whole run)
+  uint32_t tm_start[5];    // first state bit of each tensor dimension
+  uint32_t tm_len[5];      // bits of that dimension (a run of tile bits plus the run of non-tile bits above it)
 };
 
 // ----------------------------------------------------------------------------- PTX helpers
@@ -378,7 +377,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_dense(float* __restrict__ 
           int c[5];
 #pragma unroll
           for (uint32_t d = 0; d < 5; ++d)
-            c[d] = (d < p.tm_rank && !p.tm_tile[d]) ? int((base >> p.tm_start[d]) & ((1ull << p.tm_len[d]) - 1ull)) : 0;
+            c[d] = d < p.tm_rank ? int((base >> p.tm_start[d]) & ((1ull << p.tm_len[d]) - 1ull)) : 0;
           tma_tensor_g2s(dre, &tm_re, c, p.tm_rank, &iofull[slot]);
           tma_tensor_g2s(dim_, &tm_im, c, p.tm_rank, &iofull[slot]);
         }
@@ -689,24 +688,29 @@ static void launch_tc_k(const LaunchEnv& env, float* re, float* im, uint32_t n, 
   uint32_t rb = 0;
   while (rb < uint32_t(kTileBits) && tbits[rb] == rb) ++rb;
   p.runbits = rb;
-  // Short runs: describe the state as a tensor whose dimensions are the maximal runs of tile /
-  // non-tile bits, so one tiled TMA per component fetches the whole tile in address order.
+  // Short runs: view the state as a tensor with one dimension per run of tile bits, each extended
+  // by the run of non-tile bits above it. The box covers the tile part of every dimension and the
+  // tile's coordinates are the base's bits (its tile bits are zero), so one tiled TMA per
+  // component fetches the whole tile in address order.
   CUtensorMap maps[2];
   std::memset(maps, 0, sizeof(maps));
   if (rb <= 8) {
-    std::vector<std::pair<uint32_t, uint32_t>> runs;  // (start, len)
-    std::vector<bool> is_tile;
+    struct Dim {
+      uint32_t start, tile_len, len;
+    };
+    std::vector<Dim> dims;
+    auto in_tile = [&](uint32_t b) { return gate_rank[b] >= 0 || col_rank[b] >= 0; };
     for (uint32_t b = 0; b < n;) {
-      const bool t = gate_rank[b] >= 0 || col_rank[b] >= 0;
       uint32_t e = b;
-      while (e < n && (gate_rank[e] >= 0 || col_rank[e] >= 0) == t) ++e;
-      runs.push_back({b, e - b});
-      is_tile.push_back(t);
-      b = e;
+      while (e < n && in_tile(e)) ++e;   // tile run [b, e)
+      uint32_t f = e;
+      while (f < n && !in_tile(f)) ++f;  // non-tile run above it [e, f)
+      dims.push_back({b, e - b, f - b});
+      b = f;
     }
-    bool ok = runs.size() <= 5;
-    for (size_t d = 0; d < runs.size() && ok; ++d)
-      if (is_tile[d] && runs[d].second > 8) ok = false;  // box dimensions are at most 256
+    bool ok = dims.size() <= 5;
+    for (const Dim& d : dims) ok = ok && d.tile_len <= 8 && d.len <= 31;  // box <= 256, extent < 2^32
+    for (size_t d = 1; d < dims.size(); ++d) ok = ok && dims[d].start >= 2;  // 16-byte strides
     if (ok) {
       static PFN_cuTensorMapEncodeTiled_v12000 encode = [] {
         void* fn = nullptr;
@@ -717,24 +721,23 @@ static void launch_tc_k(const LaunchEnv& env, float* re, float* im, uint32_t n, 
         return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
       }();
       if (encode) {
-        cuuint64_t dims[5], strides[4];
+        cuuint64_t gdim[5], strides[4];
         cuuint32_t box[5], estr[5];
-        for (size_t d = 0; d < runs.size(); ++d) {
-          dims[d] = cuuint64_t(1) << runs[d].second;
-          box[d] = is_tile[d] ? cuuint32_t(1) << runs[d].second : 1;
+        for (size_t d = 0; d < dims.size(); ++d) {
+          gdim[d] = cuuint64_t(1) << dims[d].len;
+          box[d] = cuuint32_t(1) << dims[d].tile_len;
           estr[d] = 1;
-          if (d > 0) strides[d - 1] = (cuuint64_t(1) << runs[d].first) * sizeof(float);
-          p.tm_start[d] = runs[d].first;
-          p.tm_len[d] = runs[d].second;
-          p.tm_tile[d] = is_tile[d] ? 1u : 0u;
+          if (d > 0) strides[d - 1] = (cuuint64_t(1) << dims[d].start) * sizeof(float);
+          p.tm_start[d] = dims[d].start;
+          p.tm_len[d] = dims[d].len;
         }
         float* bases[2] = {re, im};
         bool enc_ok = true;
         for (int c = 0; c < 2 && enc_ok; ++c)
-          enc_ok = encode(&maps[c], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, cuuint32_t(runs.size()), bases[c], dims, strides,
+          enc_ok = encode(&maps[c], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, cuuint32_t(dims.size()), bases[c], gdim, strides,
                           box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                           CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
-        if (enc_ok) p.tm_rank = uint32_t(runs.size());
+        if (enc_ok) p.tm_rank = uint32_t(dims.size());
       }
     }
   }

@@ -76,6 +76,29 @@ def test_single_tc_sweep(be, k, qset, n):
     assert infidelity(want, got) < 1e-8
 
 
+@pytest.mark.parametrize("qs", [
+    [5, 6, 11, 12, 13, 14],      # two tile runs -> 2-D tensor-map TMA
+    [3, 8, 9, 13, 14, 18],       # four tile runs -> 4-D tensor map
+    [5, 6, 11, 12, 17, 18],      # brickwork window shape
+    [7, 9, 11, 13, 15, 17],      # seven tile runs -> bulk-copy fallback
+    [0, 2, 9, 10, 16, 19],       # bit 0 in the gate, bit 1 a column (scalar B stores)
+    [2, 3, 4, 5],                # k = 4, one contiguous tile
+    [1, 6, 7, 12, 19],           # k = 5, bit 1 in the gate
+])
+def test_tc_tile_shapes_n20(be, qs):
+    n = 20
+    k = len(qs)
+    psi = random_state(n, sum(qs))
+    c = Circuit(n)
+    c.push(G.DenseGate(k, haar(k, 99 + sum(qs))), qs)
+    got, kinds = run_tc(be, c, psi)
+    assert kinds.get("dense_tc", 0) == 1, kinds
+    re, im = oracle.run(c, oracle.CPU_PARALLEL, oracle.F64, state=(psi.real.copy(), psi.imag.copy()))
+    want = re + 1j * im
+    assert max_abs_diff(want, got) < 1e-5
+    assert infidelity(want, got) < 1e-8
+
+
 @pytest.mark.parametrize("planner", [PLAN_WINDOW, PLAN_LEARNED])
 def test_tc_circuits_match_oracle(be, planner):
     for seed in range(6):
