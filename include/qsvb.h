@@ -175,6 +175,17 @@ int qsvb_norm_sqr(qsvb_ctx* ctx, const qsvb_state* st, double* out);
 /* <a|b> in FP64 (no trait counterpart). a and b may differ in precision (complex64 vs complex128),
  * which is how a complex64 run is scored against its FP64 twin. */
 int qsvb_inner_product(qsvb_ctx* ctx, const qsvb_state* a, const qsvb_state* b, double out[2]);
+/* <Z_mask> like qsvb_expectation_z, for callers that cannot allocate device memory: it takes the
+ * caller's own device SoA buffers (re[2^n], im[2^n] in the precision `dtype`), a CUDA stream
+ * (NULL = default stream) and a host `out`, needs no context, and calls no cudaMalloc / cudaFree.
+ * Its reduction scratch is a fixed 16.4 KB __device__ array inside the library (held on every GPU
+ * that loads it until exit; partial sums of at most 1024 CTAs; n_qubits up to 34, larger or
+ * malformed requests return QSVB_E_INVALID). All calls share that array, so calls whose kernels
+ * overlap on the GPU race; the first call on a device sets the array up and must come before any
+ * stream capture. No counterpart in the reference: it exists for hosts that run under a fixed
+ * device-memory budget or own every device allocation themselves. Waits for its result. */
+int qsvb_expectation_z_noalloc(const void* d_re, const void* d_im, uint32_t n_qubits, int dtype, uint64_t mask,
+                               void* stream, double* out);
 /* |<a|b>|^2 in FP64 (no trait counterpart). */
 int qsvb_fidelity(qsvb_ctx* ctx, const qsvb_state* a, const qsvb_state* b, double* out);
 

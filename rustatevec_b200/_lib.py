@@ -112,6 +112,7 @@ SIGNATURES = {
     "qsvb_norm_sqr": (_i, [_vp, _vp, _dp]),
     "qsvb_inner_product": (_i, [_vp, _vp, _vp, _dp]),
     "qsvb_fidelity": (_i, [_vp, _vp, _vp, _dp]),
+    "qsvb_expectation_z_noalloc": (_i, [_vp, _vp, _u32, _i, _u64, _vp, _dp]),
     "qsvb_execute_batch": (_i, [_vp, C.POINTER(CircuitS), _sz, _i, _dp, _dp, C.POINTER(_u64),
                                 C.POINTER(PlanStats)]),
 }

@@ -16,6 +16,7 @@
 namespace qsvb {
 
 static thread_local std::string g_last_error;
+void set_last_error(const std::string& msg) { g_last_error = msg; }
 
 [[noreturn]] void throw_cuda(cudaError_t e, const char* what, const char* file, int line) {
   const int code = e == cudaErrorMemoryAllocation ? QSVB_E_OOM : QSVB_E_CUDA;

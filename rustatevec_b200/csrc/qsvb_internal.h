@@ -21,6 +21,7 @@ struct Error : std::runtime_error {
   Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
 };
 [[noreturn]] void throw_cuda(cudaError_t e, const char* what, const char* file, int line);
+void set_last_error(const std::string& msg);  // the message qsvb_last_error() returns on this thread
 #define QSVB_CK(x)                                                        \
   do {                                                                    \
     cudaError_t _qe = (x);                                                \
