@@ -169,8 +169,10 @@ def run_gpu(args):
     from rustatevec_b200 import _lib as L
     from rustatevec_b200.circuits import brickwork
 
+    from rustatevec_b200 import tuning
     world, rank, local = dist_setup()
     torch.cuda.set_device(local)
+    model_doc = tuning.load()  # the learned cost model trained on this pool's B200s (None: roofline model)
     be = B200Backend(local, precision="f32")
     stream = torch.cuda.ExternalStream(be.stream(), device=torch.device("cuda", local))
     circuit = brickwork(N_QUBITS, DEPTH, SEED)
@@ -295,6 +297,7 @@ def run_gpu(args):
                        "l2": "state is 8 GiB (> 126 MB L2): no flush needed",
                        "parallelism": "replicas" if world > 1 else "single GPU"},
             "infidelity_vs_fp64": float(1.0 - fid),
+            "cost_model": (model_doc or {}).get("meta", "none (roofline model)"),
             "methods_seconds": {k: round(v["seconds"], 5) for k, v in results.items()},
             "methods_sweeps": {k: v["sweeps"] for k, v in results.items()},
             "best_plain_gpu": {"method": best_plain[0], "seconds": best_plain[1],

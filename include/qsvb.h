@@ -189,6 +189,30 @@ int qsvb_expectation_z_noalloc(const void* d_re, const void* d_im, uint32_t n_qu
 /* |<a|b>|^2 in FP64 (no trait counterpart). */
 int qsvb_fidelity(qsvb_ctx* ctx, const qsvb_state* a, const qsvb_state* b, double* out);
 
+/* ---------------------------------------------------------------- autotuner and learned cost model
+ * (no trait counterpart: they replace the fixed max-k rule of fusion.rs:26-36 with a planner that
+ * picks fusion width, strategy and kernel engine from predicted sweep times). */
+/* Times candidate sweeps (every kind, k = 1..6, CUDA-core and tensor-core engines, several qubit
+ * placements) on an n-qubit state (12 <= n <= 32): features[i*16..] is the cost-model input of
+ * candidate i, seconds[i] its mean device time over `reps` launches, kinds[i] its sweep kind.
+ * Call with features == NULL to get the candidate count in *count. */
+int qsvb_autotune(qsvb_ctx* ctx, uint32_t n_qubits, int dtype, int reps, uint64_t seed, float* features,
+                  double* seconds, uint32_t* kinds, size_t cap, size_t* count);
+/* Trains the MLP cost model (16 -> hidden -> hidden -> 1, ReLU, predicts log2 seconds) on the
+ * GPU with full-batch Adam and installs it for the learned planner. */
+int qsvb_costmodel_train(qsvb_ctx* ctx, const float* features, const float* log2_seconds, size_t n,
+                         uint32_t hidden, uint32_t epochs, float lr, uint64_t seed, float* final_loss);
+/* One forward + backward pass on the GPU for given flat parameters (see mlp.cu for the layout) on
+ * already-normalised inputs: mean-squared-error loss and its gradient (gradient checks). */
+int qsvb_costmodel_forward_backward(qsvb_ctx* ctx, const float* params, uint32_t hidden, const float* x,
+                                    const float* target, size_t n, float* loss, float* grad);
+/* Installed model as a flat float image (call with out == NULL for its length); set installs an
+ * image (NULL / 0 uninstalls: the planner falls back to its roofline model). */
+int qsvb_costmodel_get(float* out, size_t cap, size_t* needed);
+int qsvb_costmodel_set(const float* image, size_t len);
+/* Host forward of the installed model: log2 seconds for each 16-float feature row. */
+int qsvb_costmodel_predict(const float* features, size_t n, float* out_log2_seconds);
+
 /* ---------------------------------------------------------------- batched circuits */
 /* Many small independent circuits (each n <= 20) in one persistent kernel. For circuit i the
  * engine writes <Z_0> to z0_out[i] and, when probs_out != NULL, its 2^n_i FP64 probabilities

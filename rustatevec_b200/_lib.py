@@ -113,6 +113,14 @@ SIGNATURES = {
     "qsvb_inner_product": (_i, [_vp, _vp, _vp, _dp]),
     "qsvb_fidelity": (_i, [_vp, _vp, _vp, _dp]),
     "qsvb_expectation_z_noalloc": (_i, [_vp, _vp, _u32, _i, _u64, _vp, _dp]),
+    "qsvb_autotune": (_i, [_vp, _u32, _i, _i, _u64, C.c_void_p, C.c_void_p, C.c_void_p, _sz, C.POINTER(_sz)]),
+    "qsvb_costmodel_train": (_i, [_vp, C.c_void_p, C.c_void_p, _sz, _u32, _u32, C.c_float, _u64,
+                                  C.POINTER(C.c_float)]),
+    "qsvb_costmodel_forward_backward": (_i, [_vp, C.c_void_p, _u32, C.c_void_p, C.c_void_p, _sz,
+                                             C.POINTER(C.c_float), C.c_void_p]),
+    "qsvb_costmodel_get": (_i, [C.c_void_p, _sz, C.POINTER(_sz)]),
+    "qsvb_costmodel_set": (_i, [C.c_void_p, _sz]),
+    "qsvb_costmodel_predict": (_i, [C.c_void_p, _sz, C.c_void_p]),
     "qsvb_execute_batch": (_i, [_vp, C.POINTER(CircuitS), _sz, _i, _dp, _dp, C.POINTER(_u64),
                                 C.POINTER(PlanStats)]),
 }

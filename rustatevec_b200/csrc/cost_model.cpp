@@ -42,11 +42,28 @@ void sweep_features(const Sweep& s, uint32_t n, int dtype, float* f) {
   for (uint32_t j = 0; j < s.m; ++j) hi = std::max<int>(hi, int(s.q[j]));
   if (s.kind == SK_1Q || s.kind == SK_CTRL) hi = std::max<int>(hi, int(s.target));
   f[11] = float(std::min(lo, 40));
-  f[12] = float(hi);
   f[13] = float(s.terms.size()) / 16.0f;
-  uint32_t nlow = 0;
-  for (uint32_t j = 0; j < s.m; ++j) nlow += s.q[j] < 7;
-  f[14] = float(nlow);
+  if (s.kind == SK_DENSE || s.kind == SK_DENSE_TC) {
+    // the dense kernels' tile: gate bits + the (12 - k) lowest other bits; its memory pattern is
+    // set by how many runs of consecutive state bits it spans and by which bits are the lowest two
+    bool gate[64] = {false}, tile[64] = {false};
+    for (uint32_t j = 0; j < s.m; ++j) gate[s.q[j]] = tile[s.q[j]] = true;
+    uint32_t ncol = 0;
+    for (uint32_t b = 0; b < n && ncol < 12 - s.m; ++b)
+      if (!gate[b]) {
+        tile[b] = true;
+        ++ncol;
+      }
+    uint32_t runs = 0;
+    for (uint32_t b = 0; b < n; ++b) runs += tile[b] && (b == 0 || !tile[b - 1]);
+    f[12] = float(runs);
+    f[14] = (!gate[0] && !gate[1]) ? 0.0f : (gate[0] && gate[1] ? 1.0f : 2.0f);
+  } else {
+    f[12] = float(hi);
+    uint32_t nlow = 0;
+    for (uint32_t j = 0; j < s.m; ++j) nlow += s.q[j] < 7;
+    f[14] = float(nlow);
+  }
   f[15] = float(std::log2(analytic_sweep_seconds(s, n, dtype)));
 }
 
@@ -110,11 +127,19 @@ double predict_plan_seconds(const std::vector<Sweep>& sw, uint32_t n, int dtype)
 }
 
 void select_engines(std::vector<Sweep>& sw, uint32_t n, const qsvb_plan_opts& o, int dtype) {
+  const bool learned = g_model.hidden > 0 && o.planner == QSVB_PLAN_LEARNED;
   for (Sweep& s : sw) {
     if (s.kind != SK_DENSE) continue;
-    const bool want_tc = dtype == QSVB_C64 && ((o.engine == QSVB_ENGINE_TENSOR_CORE && s.m >= 4) ||
-                                               (o.engine == QSVB_ENGINE_AUTO && s.m >= 5));
-    if (want_tc && tc_dense_supported(s, n)) s.kind = SK_DENSE_TC;
+    if (dtype != QSVB_C64 || !tc_dense_supported(s, n) || o.engine == QSVB_ENGINE_CUDA_CORE) continue;
+    if (o.engine == QSVB_ENGINE_TENSOR_CORE) {
+      s.kind = SK_DENSE_TC;
+    } else if (learned) {  // auto + trained model: the cheaper engine by prediction
+      Sweep t = s;
+      t.kind = SK_DENSE_TC;
+      if (predict_sweep_seconds(t, n, dtype) < predict_sweep_seconds(s, n, dtype)) s.kind = SK_DENSE_TC;
+    } else if (s.m >= 5) {  // auto without a model: tensor cores once CUDA cores turn compute-bound
+      s.kind = SK_DENSE_TC;
+    }
   }
 }
 
