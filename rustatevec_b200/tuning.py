@@ -38,6 +38,44 @@ def autotune(backend, n_qubits: int, reps: int = 3, seed: int = 0) -> dict:
             "n_qubits": np.full(m, n_qubits), "precision": [backend.precision] * m}
 
 
+def plan_records(backend, n_qubits: int, reps: int = 2, seed: int = 0) -> dict:
+    """Per-sweep device times of the candidate plans the planner weighs (qsv greedy fuse and window
+    fusion at k = 2..6, CUDA-core and tensor-core engines) for representative circuits, so the model
+    is trained on the sweeps real plans contain."""
+    from .backend import Plan
+    from .circuits import brickwork, qaoa_maxcut, qft, random_circuit
+    circuits = [random_circuit(n_qubits, 20 * n_qubits, seed + 1), brickwork(n_qubits, 6, seed + 2),
+                qft(n_qubits), qaoa_maxcut(n_qubits, 1, seed + 3)]
+    engines = [L.ENGINE_CUDA_CORE] + ([L.ENGINE_TENSOR_CORE] if backend.dtype == L.C64 else [])
+    feats, secs, kinds = [], [], []
+    st = backend.alloc(n_qubits)
+    try:
+        backend.init_basis(st, 0)
+        seen = set()
+        for circ in circuits:
+            for planner in (L.PLAN_GREEDY, L.PLAN_WINDOW):
+                for k in (2, 4, 6):
+                    for eng in engines:
+                        p = Plan(backend, circ, L.make_opts(planner, k, eng, use_graph=False))
+                        info = p.sweeps()
+                        t = p.profile(st, reps)
+                        for s, sec in zip(info, t):
+                            key = tuple(s["features"])
+                            if key in seen:
+                                continue
+                            seen.add(key)
+                            feats.append(s["features"])
+                            secs.append(sec)
+                            kinds.append(L.SWEEP_KINDS.index(s["kind"]))
+                        p.free()
+    finally:
+        st.free()
+    m = len(secs)
+    return {"features": np.asarray(feats, np.float32).reshape(m, NUM_FEATURES), "seconds": np.asarray(secs),
+            "kinds": np.asarray(kinds, np.uint32), "n_qubits": np.full(m, n_qubits),
+            "precision": [backend.precision] * m}
+
+
 def collect(device: int = 0, sizes=(22, 25, 28, 30), precisions=("f32", "f64"), reps: int = 3) -> dict:
     from .backend import B200Backend
     parts = []
@@ -48,6 +86,7 @@ def collect(device: int = 0, sizes=(22, 25, 28, 30), precisions=("f32", "f64"), 
                 if prec == "f64" and n > 30:
                     continue
                 parts.append(autotune(be, n, reps, seed=n))
+                parts.append(plan_records(be, n, reps=2, seed=n))
         finally:
             be.close()
     return {k: (np.concatenate([p[k] for p in parts]) if k != "precision" else sum((p[k] for p in parts), []))

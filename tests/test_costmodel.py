@@ -122,7 +122,9 @@ def test_learned_planner_gains_over_the_untrained_method(be32):
     import torch
     from rustatevec_b200 import Plan, PLAN_GREEDY, PLAN_LEARNED, ENGINE_AUTO
     from rustatevec_b200.circuits import brickwork, random_circuit
-    rec = tuning.autotune(be32, 24, reps=3, seed=24)
+    a = tuning.autotune(be32, 24, reps=3, seed=24)
+    b = tuning.plan_records(be32, 24, reps=2, seed=24)
+    rec = {k: np.concatenate([a[k], b[k]]) if k != "precision" else a[k] + b[k] for k in a}
     loss = tuning.train(be32, rec, hidden=64, epochs=3000)
     pred = tuning.predict(rec["features"])
     truth = np.log2(rec["seconds"])
