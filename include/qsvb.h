@@ -214,13 +214,40 @@ int qsvb_costmodel_set(const float* image, size_t len);
 int qsvb_costmodel_predict(const float* features, size_t n, float* out_log2_seconds);
 
 /* ---------------------------------------------------------------- batched circuits */
-/* Many small independent circuits (each n <= 20) in one persistent kernel. For circuit i the
- * engine writes <Z_0> to z0_out[i] and, when probs_out != NULL, its 2^n_i FP64 probabilities
- * at probs_out + probs_offset[i] (host memory; offsets supplied by the caller). Each circuit
- * starts from |0..0>. No trait counterpart. */
+/* Many small independent circuits (each n <= 30, gates of 1 or 2 qubits) in one persistent
+ * kernel. For circuit i the engine writes <Z_0> to z0_out[i] (when z0_out != NULL) and, when
+ * probs_out != NULL, its 2^n_i FP64 probabilities at probs_out + probs_offset[i] (host memory),
+ * or packed in circuit order when probs_offset == NULL. Each circuit starts from |0..0>.
+ * stats (optional): n_sweeps = passes over shared-memory tiles, n_sweeps_by_kind[0] = register
+ * phases, algorithmic_bytes = HBM bytes of those passes plus the probabilities, flops = gate
+ * arithmetic, predicted_seconds = measured device seconds of the batched kernels. Replaces a host
+ * loop of Backend::execute over the circuits (crates/qsv-core/src/backend/mod.rs:66-73) followed
+ * by expectation_z (crates/qsv-core/src/sample.rs:177-200). */
 int qsvb_execute_batch(qsvb_ctx* ctx, const qsvb_circuit* circuits, size_t n_circuits, int dtype,
                        double* z0_out, double* probs_out, const uint64_t* probs_offset,
                        qsvb_plan_stats* stats);
+/* A reusable batch: the plan (passes over HBM, register phases, work queue), its device buffers
+ * and one CUDA graph with the per-run device work, built once; each run replays the graph and
+ * copies <Z_0> (and, when asked, the probabilities) to the host. local_qubits as in
+ * qsvb_execute_batch_ex. No trait counterpart. */
+typedef struct qsvb_batch qsvb_batch;
+int qsvb_batch_create(qsvb_ctx* ctx, const qsvb_circuit* circuits, size_t n_circuits, int dtype,
+                      uint32_t local_qubits, qsvb_batch** out);
+int qsvb_batch_run(qsvb_ctx* ctx, qsvb_batch* batch, double* z0_out, double* probs_out,
+                   const uint64_t* probs_offset, qsvb_plan_stats* stats);
+int qsvb_batch_free(qsvb_ctx* ctx, qsvb_batch* batch);
+/* Times each local-qubit count from 9 up to the limit on this batch; writes the fastest to *best
+ * and, when seconds != NULL, the device seconds of each candidate (ascending count, at most cap;
+ * *count = number of candidates). */
+int qsvb_batch_autotune(qsvb_ctx* ctx, const qsvb_circuit* circuits, size_t n_circuits, int dtype,
+                        uint32_t* best, double* seconds, size_t cap, size_t* count);
+/* Same as qsvb_execute_batch, with the number of local qubits per shared-memory tile chosen by
+ * the caller (7..14 for complex64, 7..13 for complex128; 0 = the engine's choice). Circuits with
+ * at most that many qubits run whole in one thread block; larger ones take several passes over
+ * HBM. */
+int qsvb_execute_batch_ex(qsvb_ctx* ctx, const qsvb_circuit* circuits, size_t n_circuits, int dtype,
+                          uint32_t local_qubits, double* z0_out, double* probs_out,
+                          const uint64_t* probs_offset, qsvb_plan_stats* stats);
 
 #ifdef __cplusplus
 }

@@ -123,6 +123,12 @@ SIGNATURES = {
     "qsvb_costmodel_predict": (_i, [C.c_void_p, _sz, C.c_void_p]),
     "qsvb_execute_batch": (_i, [_vp, C.POINTER(CircuitS), _sz, _i, _dp, _dp, C.POINTER(_u64),
                                 C.POINTER(PlanStats)]),
+    "qsvb_batch_create": (_i, [_vp, C.POINTER(CircuitS), _sz, _i, _u32, C.POINTER(_vp)]),
+    "qsvb_batch_run": (_i, [_vp, _vp, _dp, _dp, C.POINTER(_u64), C.POINTER(PlanStats)]),
+    "qsvb_batch_free": (_i, [_vp, _vp]),
+    "qsvb_batch_autotune": (_i, [_vp, C.POINTER(CircuitS), _sz, _i, C.POINTER(_u32), _dp, _sz, C.POINTER(_sz)]),
+    "qsvb_execute_batch_ex": (_i, [_vp, C.POINTER(CircuitS), _sz, _i, _u32, _dp, _dp, C.POINTER(_u64),
+                                   C.POINTER(PlanStats)]),
 }
 
 _lib = None
@@ -173,6 +179,45 @@ class PackedCircuit:
 
     def ref(self):
         return C.byref(self.struct)
+
+
+_GATE_DT = np.dtype({"names": ["n", "q", "mat"], "formats": ["<u4", ("<u4", MAX_GATE_QUBITS), "<u8"],
+                     "offsets": [0, 4, 32], "itemsize": 40})
+_CIRC_DT = np.dtype({"names": ["n", "ngates", "gates"], "formats": ["<u4", "<u8", "<u8"],
+                     "offsets": [0, 8, 16], "itemsize": 24})
+
+
+class PackedBatch:
+    """Many circuits packed into one ``qsvb_circuit`` array (numpy-built, no per-gate Python
+    ctypes work); keeps every buffer alive."""
+
+    def __init__(self, circuits):
+        assert C.sizeof(Gate) == _GATE_DT.itemsize and C.sizeof(CircuitS) == _CIRC_DT.itemsize
+        flats = [c.flatten() for c in circuits]
+        arity = np.concatenate([f[0] for f in flats]) if flats else np.zeros(0, np.uint32)
+        self.mats = np.ascontiguousarray(np.concatenate([f[2] for f in flats]) if flats else np.zeros(1))
+        ng = len(arity)
+        self.gates = np.zeros(max(ng, 1), dtype=_GATE_DT)
+        self.gates["n"][:ng] = arity
+        a64 = arity.astype(np.int64)
+        qoff = np.concatenate([[0], np.cumsum(a64)])
+        allq = np.concatenate([f[1] for f in flats]) if flats else np.zeros(0, np.uint32)
+        for j in range(int(a64.max()) if ng else 0):
+            sel = a64 > j
+            self.gates["q"][:ng][sel, j] = allq[qoff[:-1][sel] + j]
+        moff = np.concatenate([[0], np.cumsum(2 * (1 << (2 * a64)))])[:-1]
+        self.gates["mat"][:ng] = self.mats.ctypes.data + 8 * moff
+        counts = np.array([len(f[0]) for f in flats], dtype=np.int64)
+        goff = np.concatenate([[0], np.cumsum(counts)])[:-1]
+        self.circs = np.zeros(max(len(flats), 1), dtype=_CIRC_DT)
+        self.circs["n"][:len(flats)] = [c.n_qubits() for c in circuits]
+        self.circs["ngates"][:len(flats)] = counts
+        self.circs["gates"][:len(flats)] = self.gates.ctypes.data + _GATE_DT.itemsize * goff
+        self.count = len(flats)
+        self.n_qubits = np.array([c.n_qubits() for c in circuits], dtype=np.int64)
+
+    def ptr(self):
+        return C.cast(self.circs.ctypes.data, C.POINTER(CircuitS))
 
 
 def make_opts(planner=PLAN_GREEDY, max_fused_qubits=4, engine=ENGINE_AUTO, use_graph=True) -> PlanOpts:

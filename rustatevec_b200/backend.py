@@ -192,6 +192,30 @@ class B200Backend:
         self.run(state, circuit)
         return state
 
+    def execute_batch(self, circuits, probabilities: bool = True, local_qubits: int = 0):
+        """Run many small circuits (each from |0..0>) in one persistent kernel: the batched form of
+        ``execute`` followed by ``expectation_z(probs, 1)`` (sample.rs:177-200) per circuit.
+
+        Returns ``(z0, probs, stats)``: ``z0`` f64[count]; ``probs`` one FP64 array of 2^n_i per
+        circuit (views into one packed buffer) or None; ``stats`` the batch statistics with
+        ``predicted_seconds`` = measured device seconds."""
+        pb = circuits if isinstance(circuits, L.PackedBatch) else L.PackedBatch(circuits)
+        z0 = np.zeros(pb.count, dtype=np.float64)
+        probs = None
+        pptr = None
+        if probabilities:
+            sizes = np.left_shift(1, pb.n_qubits)
+            probs_flat = np.empty(int(sizes.sum()), dtype=np.float64)
+            pptr = probs_flat.ctypes.data_as(C.POINTER(C.c_double))
+        st = L.PlanStats()
+        L.check(L.lib().qsvb_execute_batch_ex(self.ctx, pb.ptr(), pb.count, self.dtype, local_qubits,
+                                              z0.ctypes.data_as(C.POINTER(C.c_double)), pptr, None,
+                                              C.byref(st)))
+        if probabilities:
+            edges = np.concatenate([[0], np.cumsum(sizes)])
+            probs = [probs_flat[edges[i]:edges[i + 1]] for i in range(pb.count)]
+        return z0, probs, st.to_dict()
+
     def stream(self) -> int:
         """The engine's cudaStream_t as an integer (for torch.cuda.ExternalStream)."""
         out = C.c_void_p()

@@ -632,7 +632,55 @@ int qsvb_execute_batch(qsvb_ctx* c, const qsvb_circuit* circuits, size_t n_circu
   return guarded([&] {
     check_ctx(c);
     DeviceGuard dg(c->device);
-    run_batch(c, circuits, n_circuits, dtype, z0_out, probs_out, probs_offset, stats);
+    run_batch(c, circuits, n_circuits, dtype, 0, z0_out, probs_out, probs_offset, stats);
+  });
+}
+
+int qsvb_batch_create(qsvb_ctx* c, const qsvb_circuit* circuits, size_t n_circuits, int dtype, uint32_t local_qubits,
+                      qsvb_batch** out) {
+  return guarded([&] {
+    check_ctx(c);
+    QSVB_REQUIRE(out != nullptr, "null output");
+    *out = nullptr;
+    DeviceGuard dg(c->device);
+    *out = qsvb::batch_create(c, circuits, n_circuits, dtype, local_qubits);
+  });
+}
+
+int qsvb_batch_run(qsvb_ctx* c, qsvb_batch* b, double* z0_out, double* probs_out, const uint64_t* probs_offset,
+                   qsvb_plan_stats* stats) {
+  return guarded([&] {
+    check_ctx(c);
+    DeviceGuard dg(c->device);
+    qsvb::batch_run(c, b, z0_out, probs_out, probs_offset, stats);
+  });
+}
+
+int qsvb_batch_free(qsvb_ctx* c, qsvb_batch* b) {
+  return guarded([&] {
+    check_ctx(c);
+    DeviceGuard dg(c->device);
+    free_batch(b);
+  });
+}
+
+int qsvb_batch_autotune(qsvb_ctx* c, const qsvb_circuit* circuits, size_t n_circuits, int dtype, uint32_t* best,
+                        double* seconds, size_t cap, size_t* count) {
+  return guarded([&] {
+    check_ctx(c);
+    QSVB_REQUIRE(best != nullptr, "null output");
+    DeviceGuard dg(c->device);
+    *best = qsvb::batch_autotune(c, circuits, n_circuits, dtype, seconds, cap, count);
+  });
+}
+
+int qsvb_execute_batch_ex(qsvb_ctx* c, const qsvb_circuit* circuits, size_t n_circuits, int dtype,
+                          uint32_t local_qubits, double* z0_out, double* probs_out, const uint64_t* probs_offset,
+                          qsvb_plan_stats* stats) {
+  return guarded([&] {
+    check_ctx(c);
+    DeviceGuard dg(c->device);
+    run_batch(c, circuits, n_circuits, dtype, local_qubits, z0_out, probs_out, probs_offset, stats);
   });
 }
 

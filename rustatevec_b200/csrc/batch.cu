@@ -1,7 +1,1001 @@
-// Batched execution of many small independent circuits (placeholder until the persistent runner
-// lands): rejects the request so callers see a clear status.
+// Batched execution of many small independent circuits in one persistent kernel.
+//
+// Host plan. Each circuit is split into passes over HBM: a pass owns a set S of at most L local
+// qubits (always including state bits 0-4, so global accesses are runs of >= 32 contiguous
+// amplitudes) and takes the gates that act inside S and commute past every gate left for later
+// passes (gates on disjoint qubits). A circuit with n <= L is a single pass whose whole state lives
+// in one thread block's shared memory: |0..0> is built there and only the FP64 probabilities and
+// <Z_0> leave the SM. Larger circuits keep their state in HBM; a pass is 2^(n-|S|) disjoint tiles of
+// 2^|S| amplitudes (the non-local bits fixed), each loaded into shared memory, updated and written
+// back (the first pass starts from |0..0> without reading, the last writes probabilities instead of
+// the state).
+//
+// Inside a pass the gates are split the same way once more into register phases: a phase owns RB
+// local positions (5 for complex64, 4 for complex128); a thread holds a group of 2^RB amplitudes
+// that share the other local bits in registers, applies all of the phase's gates there, and writes
+// them back (256 threads, up to 512 groups per phase). Shared memory is touched once per phase
+// instead of once per gate. The shared-memory index is XOR-swizzled (a linear map on the index
+// bits) and each phase picks which non-register positions become warp lanes so that a warp's 32
+// accesses fall in distinct banks.
+//
+// Work items are (pass, tile) pairs in one queue ordered level by level (pass 0 of every circuit,
+// then pass 1, ...), costliest circuits first within a level, so every item's dependencies are
+// earlier in the queue and were taken by a running block. A persistent grid takes items with an
+// atomic counter; a tile of pass p spins, with a clock64 budget, until all tiles of pass p-1 of its
+// circuit are done. A spin that runs out sets the context's error flag and later waits give up at
+// once (the host reports QSVB_E_TIMEOUT). <Z_0> partial sums go to one slot per last-pass tile and
+// are summed per circuit in a fixed order afterwards, so results are deterministic. The per-run
+// device work (counter resets, the persistent kernel, the <Z_0> sums) is one CUDA graph per batch.
+
+#include <cuda/atomic>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <memory>
+#include <numeric>
+#include <string>
+#include <vector>
+
 #include "qsvb_internal.h"
 
-void run_batch(qsvb_ctx*, const qsvb_circuit*, size_t, int, double*, double*, const uint64_t*, qsvb_plan_stats*) {
-  throw qsvb::Error(QSVB_E_UNSUPPORTED, "batched execution is not available in this build");
+namespace qsvb {
+namespace {
+
+constexpr int kBatchThreads = 256;
+constexpr int kMaxLocal = 14;
+constexpr int kMaxHi = 512;                   // 2^(kMaxLocal - 5): entries of the address / swizzle tables
+constexpr long long kSpinBudget = 1ll << 32;  // clock64 cycles (about 2 s)
+
+enum BatchOp : uint32_t { OP_PHASE = 0, OP_1Q = 1, OP_D1 = 2, OP_CX = 3, OP_2Q = 4, OP_D2 = 5 };
+
+struct Instr {
+  uint32_t op;
+  uint32_t a, b;  // register bits (1Q/D1: a; CX: a = control, b = target; 2Q/D2: a < b, matrix bit 0 <-> a)
+  uint32_t coef;  // complex index into the coefficient array (OP_PHASE: phase index)
+};
+
+struct PhaseDev {
+  uint32_t rphys[5];  // swizzled shared-memory offset of each register bit's unit vector
+  uint8_t tpos[12];   // group bit i -> local position (bits 0..4 are the warp lanes)
+  uint32_t r, nt;     // register bits used, group bits (2^nt groups of 2^r amplitudes)
+  uint32_t ninstr;    // gate instructions that follow the phase instruction
+};
+
+struct PassDev {
+  uint32_t circuit, nlocal, first, last;
+  uint32_t prog_off, prog_len, ntiles, prev;  // prev: previous pass of the same circuit (or ~0u)
+  uint32_t nnon;
+  uint8_t nonlocal[32];  // non-local state bits, ascending
+  uint8_t local[16];     // local position -> state bit, ascending
+  uint64_t state_off;    // amplitude offset of the circuit's state
+  uint64_t prob_off;     // offset of the circuit's probabilities
+  uint64_t zslot;        // first <Z_0> partial slot (last pass)
+};
+
+struct Item {
+  uint32_t pass;
+  uint32_t tile;
+};
+
+// Swizzle: shared-memory slot = x ^ (XOR over set bits p >= W of x of col(p)), a linear bijection
+// that only changes the low W bits (W = 5 for 4-byte words, 4 for 8-byte words: the bits that pick
+// the bank for a warp, or for each half-warp with 8-byte words).
+__host__ __device__ inline uint32_t swz_col(int p, int W) {
+  if (p < W) return 0u;
+  if (p < 2 * W) return 1u << (p - W);
+  return (1u << (W - 1)) | (1u << ((p - 2 * W) % (W - 1)));
 }
+
+// One amplitude component global -> shared without a register round trip (many in flight).
+template <class R>
+__device__ __forceinline__ void cp_async_elem(R* dst, const R* src) {
+  const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(dst));
+  if constexpr (sizeof(R) == 4)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(src) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src) : "memory");
+}
+
+template <class R>
+__device__ __forceinline__ void cmac(R& yr, R& yi, R ar, R ai, R xr, R xi) {
+  yr = fma(ar, xr, yr);
+  yr = fma(-ai, xi, yr);
+  yi = fma(ar, xi, yi);
+  yi = fma(ai, xr, yi);
+}
+
+// ---- gates on register bits (compile-time bit positions, so the amplitudes stay in registers)
+template <int J, class R, int RB>
+__device__ __forceinline__ void g1q(R* vr, R* vi, const R* __restrict__ c) {
+  if constexpr (J < RB) {
+    const R a0 = c[0], a1 = c[1], b0 = c[2], b1 = c[3], c0 = c[4], c1 = c[5], d0 = c[6], d1 = c[7];
+#pragma unroll
+    for (int s = 0; s < (1 << RB); ++s) {
+      if (s & (1 << J)) continue;
+      const int t = s | (1 << J);
+      const R xr0 = vr[s], xi0 = vi[s], xr1 = vr[t], xi1 = vi[t];
+      R yr0 = 0, yi0 = 0, yr1 = 0, yi1 = 0;
+      cmac(yr0, yi0, a0, a1, xr0, xi0);
+      cmac(yr0, yi0, b0, b1, xr1, xi1);
+      cmac(yr1, yi1, c0, c1, xr0, xi0);
+      cmac(yr1, yi1, d0, d1, xr1, xi1);
+      vr[s] = yr0;
+      vi[s] = yi0;
+      vr[t] = yr1;
+      vi[t] = yi1;
+    }
+  }
+}
+
+template <int J, class R, int RB>
+__device__ __forceinline__ void gd1(R* vr, R* vi, const R* __restrict__ c) {
+  if constexpr (J < RB) {
+    const R p0r = c[0], p0i = c[1], p1r = c[2], p1i = c[3];
+#pragma unroll
+    for (int s = 0; s < (1 << RB); ++s) {
+      const R pr = (s & (1 << J)) ? p1r : p0r, pi = (s & (1 << J)) ? p1i : p0i;
+      const R xr = vr[s], xi = vi[s];
+      vr[s] = fma(pr, xr, -pi * xi);
+      vi[s] = fma(pr, xi, pi * xr);
+    }
+  }
+}
+
+template <int J, int K, class R, int RB>
+__device__ __forceinline__ void gcx(R* vr, R* vi) {
+  if constexpr (J < RB && K < RB && J != K) {
+#pragma unroll
+    for (int s = 0; s < (1 << RB); ++s) {
+      if (!(s & (1 << J)) || (s & (1 << K))) continue;
+      const int t = s | (1 << K);
+      const R tr = vr[s], ti = vi[s];
+      vr[s] = vr[t];
+      vi[s] = vi[t];
+      vr[t] = tr;
+      vi[t] = ti;
+    }
+  }
+}
+
+template <int J, int K, class R, int RB>
+__device__ __forceinline__ void g2q(R* vr, R* vi, const R* __restrict__ c) {
+  if constexpr (J < K && K < RB) {
+#pragma unroll
+    for (int s = 0; s < (1 << RB); ++s) {
+      if (s & ((1 << J) | (1 << K))) continue;
+      const int idx[4] = {s, s | (1 << J), s | (1 << K), s | (1 << J) | (1 << K)};
+      R xr[4], xi[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        xr[q] = vr[idx[q]];
+        xi[q] = vi[idx[q]];
+      }
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        R yr = 0, yi = 0;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) cmac(yr, yi, c[2 * (4 * r + q)], c[2 * (4 * r + q) + 1], xr[q], xi[q]);
+        vr[idx[r]] = yr;
+        vi[idx[r]] = yi;
+      }
+    }
+  }
+}
+
+template <int J, int K, class R, int RB>
+__device__ __forceinline__ void gd2(R* vr, R* vi, const R* __restrict__ c) {
+  if constexpr (J < K && K < RB) {
+#pragma unroll
+    for (int s = 0; s < (1 << RB); ++s) {
+      const int d = ((s >> J) & 1) | (((s >> K) & 1) << 1);
+      const R pr = c[2 * d], pi = c[2 * d + 1];
+      const R xr = vr[s], xi = vi[s];
+      vr[s] = fma(pr, xr, -pi * xi);
+      vi[s] = fma(pr, xi, pi * xr);
+    }
+  }
+}
+
+#define QSVB_PAIR_CASES(F, ...)                       \
+  case 0 * 8 + 1: F<0, 1, R, RB>(__VA_ARGS__); break; \
+  case 0 * 8 + 2: F<0, 2, R, RB>(__VA_ARGS__); break; \
+  case 0 * 8 + 3: F<0, 3, R, RB>(__VA_ARGS__); break; \
+  case 0 * 8 + 4: F<0, 4, R, RB>(__VA_ARGS__); break; \
+  case 1 * 8 + 2: F<1, 2, R, RB>(__VA_ARGS__); break; \
+  case 1 * 8 + 3: F<1, 3, R, RB>(__VA_ARGS__); break; \
+  case 1 * 8 + 4: F<1, 4, R, RB>(__VA_ARGS__); break; \
+  case 2 * 8 + 3: F<2, 3, R, RB>(__VA_ARGS__); break; \
+  case 2 * 8 + 4: F<2, 4, R, RB>(__VA_ARGS__); break; \
+  case 3 * 8 + 4: F<3, 4, R, RB>(__VA_ARGS__); break;
+
+template <class R, int RB>
+__device__ __forceinline__ void apply_instr(const Instr& in, R* vr, R* vi, const R* __restrict__ coef) {
+  const R* c = coef + 2 * size_t(in.coef);
+  switch (in.op) {
+    case OP_1Q:
+      switch (in.a) {
+        case 0: g1q<0, R, RB>(vr, vi, c); break;
+        case 1: g1q<1, R, RB>(vr, vi, c); break;
+        case 2: g1q<2, R, RB>(vr, vi, c); break;
+        case 3: g1q<3, R, RB>(vr, vi, c); break;
+        case 4: g1q<4, R, RB>(vr, vi, c); break;
+      }
+      break;
+    case OP_D1:
+      switch (in.a) {
+        case 0: gd1<0, R, RB>(vr, vi, c); break;
+        case 1: gd1<1, R, RB>(vr, vi, c); break;
+        case 2: gd1<2, R, RB>(vr, vi, c); break;
+        case 3: gd1<3, R, RB>(vr, vi, c); break;
+        case 4: gd1<4, R, RB>(vr, vi, c); break;
+      }
+      break;
+    case OP_CX: {
+      const uint32_t lo = min(in.a, in.b), hi = max(in.a, in.b);
+      const bool fwd = in.a < in.b;  // the control is the lower register bit
+      switch (lo * 8 + hi) {
+#define QSVB_CX_CASE(J, K)             \
+  case J * 8 + K:                      \
+    if (fwd) gcx<J, K, R, RB>(vr, vi); \
+    else gcx<K, J, R, RB>(vr, vi);     \
+    break;
+        QSVB_CX_CASE(0, 1)
+        QSVB_CX_CASE(0, 2)
+        QSVB_CX_CASE(0, 3)
+        QSVB_CX_CASE(0, 4)
+        QSVB_CX_CASE(1, 2)
+        QSVB_CX_CASE(1, 3)
+        QSVB_CX_CASE(1, 4)
+        QSVB_CX_CASE(2, 3)
+        QSVB_CX_CASE(2, 4)
+        QSVB_CX_CASE(3, 4)
+#undef QSVB_CX_CASE
+      }
+      break;
+    }
+    case OP_2Q:
+      switch (in.a * 8 + in.b) { QSVB_PAIR_CASES(g2q, vr, vi, c) }
+      break;
+    case OP_D2:
+      switch (in.a * 8 + in.b) { QSVB_PAIR_CASES(gd2, vr, vi, c) }
+      break;
+  }
+}
+
+template <class R, int RB, int W>
+__global__ void __launch_bounds__(kBatchThreads, 1)
+    k_batch(const Item* __restrict__ items, uint32_t nitems, const PassDev* __restrict__ passes,
+            const PhaseDev* __restrict__ phases, const Instr* __restrict__ prog, const R* __restrict__ coef,
+            R* __restrict__ sre, R* __restrict__ sim, double* __restrict__ probs, double* __restrict__ zpart,
+            uint32_t* __restrict__ done, uint32_t* __restrict__ queue, int* __restrict__ err, uint32_t lbits,
+            long long* __restrict__ prof) {
+  extern __shared__ __align__(16) uint8_t smem_raw[];
+  R* xr = reinterpret_cast<R*>(smem_raw);
+  R* xi = xr + (size_t(1) << lbits);  // every pass has nlocal <= lbits
+  __shared__ uint64_t s_gaddr[kMaxHi];
+  __shared__ uint16_t s_swz[kMaxHi];
+  __shared__ uint32_t s_item;
+  __shared__ double s_red[kBatchThreads / 32];
+  __shared__ int s_ok;
+  const int tid = threadIdx.x;
+  constexpr int NV = 1 << RB;
+  // swizzle table over the index bits above W
+  for (uint32_t h = tid; h < (1u << (lbits - W)); h += kBatchThreads) {
+    uint32_t v = 0;
+    for (int i = 0; i < int(lbits) - W; ++i)
+      if ((h >> i) & 1u) v ^= swz_col(W + i, W);
+    s_swz[h] = uint16_t(v);
+  }
+  long long t_wait = 0, t_fill = 0, t_gates = 0, t_out = 0, n_items = 0, t_mark = prof ? clock64() : 0;
+  while (true) {
+    if (tid == 0) s_item = atomicAdd(queue, 1u);
+    __syncthreads();
+    const uint32_t it = s_item;
+    if (it >= nitems) break;
+    const Item item = items[it];
+    const PassDev& P = passes[item.pass];
+    const uint32_t L = P.nlocal, T = 1u << L;
+    if (tid == 0) {
+      int ok = *reinterpret_cast<volatile int*>(err) == 0;
+      if (ok && P.prev != ~0u) {
+        cuda::atomic_ref<uint32_t, cuda::thread_scope_device> d(done[P.prev]);
+        const uint32_t need = passes[P.prev].ntiles;
+        if (d.load(cuda::memory_order_acquire) < need) {
+          const long long t0 = clock64();
+          while (d.load(cuda::memory_order_acquire) < need) {
+            if (clock64() - t0 > kSpinBudget) {
+              ok = 0;
+              atomicExch(err, 1);
+              break;
+            }
+            if (*reinterpret_cast<volatile int*>(err)) {  // an earlier wait gave up: abandon fast
+              ok = 0;
+              break;
+            }
+            __nanosleep(256);
+          }
+        }
+      }
+      s_ok = ok;
+    }
+    // global offset of each value of the local index bits above bit 4 (local positions 0..4 are
+    // state bits 0..4, contiguous in memory)
+    const uint32_t nhi = L > 5 ? L - 5 : 0;
+    {
+      uint64_t base = 0;
+      for (uint32_t j = 0; j < P.nnon; ++j) base |= uint64_t((item.tile >> j) & 1u) << P.nonlocal[j];
+      for (uint32_t h = tid; h < (1u << nhi); h += kBatchThreads) {
+        uint64_t a = base;
+        for (uint32_t j = 0; j < nhi; ++j) a |= uint64_t((h >> j) & 1u) << P.local[5 + j];
+        s_gaddr[h] = a;
+      }
+    }
+    __syncthreads();
+    if (prof) t_wait += clock64() - t_mark, t_mark = clock64(), ++n_items;
+    if (!s_ok) continue;
+    const uint32_t lowmask = L >= 5 ? 31u : (T - 1u);
+    R* gre = sre + P.state_off;
+    R* gim = sim + P.state_off;
+    if (P.first) {
+      for (uint32_t x = tid; x < T; x += kBatchThreads) {
+        xr[x] = R(0);
+        xi[x] = R(0);
+      }
+      __syncthreads();
+      if (tid == 0 && item.tile == 0) xr[0] = R(1);  // the swizzle maps 0 to 0
+    } else {
+      for (uint32_t x = tid; x < T; x += kBatchThreads) {
+        const uint64_t a = s_gaddr[x >> 5] | (x & lowmask);
+        const uint32_t y = x ^ s_swz[x >> W];
+        cp_async_elem(xr + y, gre + a);
+        cp_async_elem(xi + y, gim + a);
+      }
+      asm volatile("cp.async.wait_all;" ::: "memory");
+    }
+    __syncthreads();
+    if (prof) t_fill += clock64() - t_mark, t_mark = clock64();
+    // register phases: each group of 2^r amplitudes (fixed non-register bits) is loaded into one
+    // thread's registers, takes all of the phase's gates there, and is written back
+    uint32_t k = 0;
+    while (k < P.prog_len) {
+      const PhaseDev& D = phases[prog[P.prog_off + k].coef];
+      const uint32_t r = D.r, nt = D.nt;
+      const uint32_t kbeg = P.prog_off + k + 1, kend = kbeg + D.ninstr;
+      uint32_t rp[RB];
+#pragma unroll
+      for (int j = 0; j < RB; ++j) rp[j] = D.rphys[j];
+      for (uint32_t grp = tid; grp < (1u << nt); grp += kBatchThreads) {
+        uint32_t x0 = 0;
+        for (uint32_t i = 0; i < nt; ++i) x0 |= ((grp >> i) & 1u) << D.tpos[i];
+        const uint32_t p0 = x0 ^ s_swz[x0 >> W];
+        R vr[NV], vi[NV];
+#pragma unroll
+        for (int s = 0; s < NV; ++s) {
+          if (uint32_t(s) >> r) continue;
+          uint32_t off = p0;
+#pragma unroll
+          for (int j = 0; j < RB; ++j)
+            if (s & (1 << j)) off ^= rp[j];
+          vr[s] = xr[off];
+          vi[s] = xi[off];
+        }
+        for (uint32_t kk = kbeg; kk < kend; ++kk) apply_instr<R, RB>(prog[kk], vr, vi, coef);
+#pragma unroll
+        for (int s = 0; s < NV; ++s) {
+          if (uint32_t(s) >> r) continue;
+          uint32_t off = p0;
+#pragma unroll
+          for (int j = 0; j < RB; ++j)
+            if (s & (1 << j)) off ^= rp[j];
+          xr[off] = vr[s];
+          xi[off] = vi[s];
+        }
+      }
+      k = kend - P.prog_off;
+      __syncthreads();
+    }
+    if (prof) t_gates += clock64() - t_mark, t_mark = clock64();
+    if (P.last) {
+      // FP64 probabilities and the <Z_0> partial (state bit 0 is local position 0)
+      double z = 0.0;
+      double* pout = probs + P.prob_off;
+      for (uint32_t x = tid; x < T; x += kBatchThreads) {
+        const uint32_t y = x ^ s_swz[x >> W];
+        const double p = double(xr[y]) * double(xr[y]) + double(xi[y]) * double(xi[y]);
+        __stcs(pout + (s_gaddr[x >> 5] | (x & lowmask)), p);
+        z += (x & 1u) ? -p : p;
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) z += __shfl_xor_sync(0xffffffffu, z, o);
+      if ((tid & 31) == 0) s_red[tid >> 5] = z;
+      __syncthreads();
+      if (tid == 0) {
+        double s = 0.0;
+        for (int w = 0; w < kBatchThreads / 32; ++w) s += s_red[w];
+        zpart[P.zslot + item.tile] = s;
+      }
+    } else {
+      for (uint32_t x = tid; x < T; x += kBatchThreads) {
+        const uint64_t a = s_gaddr[x >> 5] | (x & lowmask);
+        const uint32_t y = x ^ s_swz[x >> W];
+        __stcg(gre + a, xr[y]);
+        __stcg(gim + a, xi[y]);
+      }
+    }
+    __syncthreads();
+    if (tid == 0) {
+      __threadfence();
+      cuda::atomic_ref<uint32_t, cuda::thread_scope_device> d(done[item.pass]);
+      d.fetch_add(1u, cuda::memory_order_release);
+    }
+    if (prof) t_out += clock64() - t_mark, t_mark = clock64();
+  }
+  if (prof && tid == 0) {
+    long long* o = prof + 5 * blockIdx.x;
+    o[0] = t_wait;
+    o[1] = t_fill;
+    o[2] = t_gates;
+    o[3] = t_out;
+    o[4] = n_items;
+  }
+}
+
+__global__ void k_batch_z0(const double* __restrict__ zpart, const uint64_t* __restrict__ zoff,
+                           const uint32_t* __restrict__ zcnt, uint32_t ncirc, double* __restrict__ z0) {
+  const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncirc) return;
+  double s = 0.0;
+  for (uint32_t t = 0; t < zcnt[c]; ++t) s += zpart[zoff[c] + t];
+  z0[c] = s;
+}
+
+// ------------------------------------------------------------------------------------ host plan
+struct HostGate {
+  uint32_t m;
+  uint32_t q[2];
+  std::vector<cd> a;
+};
+
+enum LKind : uint32_t { LK_1Q = OP_1Q, LK_D1 = OP_D1, LK_CX = OP_CX, LK_2Q = OP_2Q, LK_D2 = OP_D2 };
+
+struct LGate {  // a gate on local positions
+  uint32_t kind;
+  uint32_t p[2];
+  const HostGate* g;
+};
+
+std::vector<HostGate> fuse_single_qubit_runs(const qsvb_circuit& c) {
+  // consecutive gates on the same single qubit are composed (exactly, in FP64); the rest stays
+  std::vector<HostGate> out;
+  std::vector<int> open1q(c.n_qubits, -1);  // index in `out` of the open 1q gate on each qubit
+  for (size_t i = 0; i < c.n_gates; ++i) {
+    const qsvb_gate& g = c.gates[i];
+    QSVB_REQUIRE(g.n_qubits <= 2, "batched circuits take 1- and 2-qubit gates (gate " + std::to_string(i) + ")");
+    HostGate h;
+    h.m = g.n_qubits;
+    h.q[0] = g.qubits[0];
+    h.q[1] = h.m == 2 ? g.qubits[1] : 0u;
+    const size_t d = size_t(1) << h.m;
+    h.a.resize(d * d);
+    for (size_t k = 0; k < d * d; ++k) h.a[k] = cd(g.matrix[2 * k], g.matrix[2 * k + 1]);
+    if (h.m == 1 && open1q[h.q[0]] >= 0) {
+      HostGate& o = out[size_t(open1q[h.q[0]])];
+      std::vector<cd> r(4);
+      for (int x = 0; x < 2; ++x)
+        for (int y = 0; y < 2; ++y) r[x * 2 + y] = h.a[x * 2 + 0] * o.a[0 * 2 + y] + h.a[x * 2 + 1] * o.a[1 * 2 + y];
+      o.a = r;
+      continue;
+    }
+    for (uint32_t j = 0; j < h.m; ++j) open1q[h.q[j]] = -1;
+    out.push_back(std::move(h));
+    if (out.back().m == 1) open1q[out.back().q[0]] = int(out.size() - 1);
+  }
+  return out;
+}
+
+uint32_t gate_kind(const HostGate& g) {
+  const size_t d = size_t(1) << g.m;
+  bool diag = true;
+  for (size_t r = 0; r < d; ++r)
+    for (size_t c = 0; c < d; ++c)
+      if (r != c && g.a[r * d + c] != cd(0, 0)) diag = false;
+  if (g.m == 1) return diag ? LK_D1 : LK_1Q;
+  if (diag) return LK_D2;
+  static const double cx[16] = {1, 0, 0, 0, 0, 0, 0, 1, 0, 0, 1, 0, 0, 1, 0, 0};
+  bool is_cx = true;
+  for (int k = 0; k < 16; ++k) is_cx = is_cx && g.a[size_t(k)] == cd(cx[k], 0);
+  return is_cx ? LK_CX : LK_2Q;
+}
+
+}  // namespace
+
+struct BatchPlan {
+  int dtype = 0;
+  uint32_t local_bits = 14, rb = 5, swz_w = 5;
+  uint32_t ncirc = 0;
+  std::vector<PassDev> passes;
+  std::vector<PhaseDev> phases;
+  std::vector<Instr> prog;
+  std::vector<double> coef;  // complex entries as (re, im) pairs in FP64
+  std::vector<Item> items;
+  std::vector<uint64_t> prob_off, zoff;
+  std::vector<uint32_t> zcnt, nq;
+  uint64_t state_amps = 0, prob_total = 0, zslots = 0;
+  qsvb_plan_stats stats{};
+};
+
+namespace {
+
+void push_coef(BatchPlan& bp, const cd& v) {
+  bp.coef.push_back(v.real());
+  bp.coef.push_back(v.imag());
+}
+
+// Splits a pass's gates into register phases and appends them to the plan's program.
+void emit_phases(BatchPlan& bp, const std::vector<LGate>& G, uint32_t nlocal) {
+  const uint32_t rb = std::min(bp.rb, nlocal);
+  const uint32_t W = bp.swz_w;
+  const uint32_t all = (1u << nlocal) - 1u;
+  std::vector<char> done(G.size(), 0);
+  size_t first = 0;
+  std::vector<size_t> taken;
+  while (true) {
+    while (first < G.size() && done[first]) ++first;
+    if (first == G.size()) break;
+    uint32_t Rm = 0, blocked = 0;
+    taken.clear();
+    for (size_t i = first; i < G.size(); ++i) {
+      if (done[i]) continue;
+      const LGate& g = G[i];
+      const uint32_t m = (1u << g.p[0]) | (g.kind >= LK_CX ? (1u << g.p[1]) : 0u);
+      if ((m & blocked) == 0 && uint32_t(__builtin_popcount(Rm | m)) <= rb) {
+        Rm |= m;
+        done[i] = 1;
+        taken.push_back(i);
+      } else {
+        blocked |= m;
+      }
+      const bool full = uint32_t(__builtin_popcount(Rm)) == rb;
+      if (blocked == all || (full && (Rm & ~blocked) == 0)) break;
+    }
+    for (uint32_t p = 0; p < nlocal && uint32_t(__builtin_popcount(Rm)) < rb; ++p) Rm |= 1u << p;
+    // register bits: the phase's local positions in ascending order
+    int regbit[32];
+    uint32_t nr = 0;
+    PhaseDev D{};
+    for (uint32_t p = 0; p < nlocal; ++p) {
+      regbit[p] = -1;
+      if ((Rm >> p) & 1u) {
+        regbit[p] = int(nr);
+        D.rphys[nr++] = (1u << p) ^ swz_col(int(p), int(W));
+      }
+    }
+    D.r = nr;
+    // lanes: non-register positions whose bank bits span the W bank-selecting bits
+    std::vector<uint32_t> nonr, lanes;
+    for (uint32_t p = 0; p < nlocal; ++p)
+      if (!((Rm >> p) & 1u)) nonr.push_back(p);
+    const size_t nlanes = std::min<size_t>(5, nonr.size());
+    uint32_t basis[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // GF(2) elimination keyed by leading bit
+    std::vector<char> used(nonr.size(), 0);
+    for (size_t i = 0; i < nonr.size() && lanes.size() < nlanes; ++i) {
+      const uint32_t p = nonr[i];
+      uint32_t v = ((1u << p) ^ swz_col(int(p), int(W))) & ((1u << W) - 1u);
+      for (int b = int(W) - 1; b >= 0 && v; --b) {
+        if (!((v >> b) & 1u)) continue;
+        if (basis[b]) {
+          v ^= basis[b];
+        } else {
+          basis[b] = v;
+          break;
+        }
+      }
+      if (v) {
+        lanes.push_back(p);
+        used[i] = 1;
+      }
+    }
+    for (size_t i = 0; i < nonr.size() && lanes.size() < nlanes; ++i)
+      if (!used[i]) {
+        lanes.push_back(nonr[i]);
+        used[i] = 1;
+      }
+    for (size_t i = 0; i < nonr.size(); ++i)
+      if (!used[i]) lanes.push_back(nonr[i]);
+    D.nt = uint32_t(nonr.size());
+    for (size_t i = 0; i < lanes.size(); ++i) D.tpos[i] = uint8_t(lanes[i]);
+    D.ninstr = uint32_t(taken.size());
+    bp.prog.push_back(Instr{OP_PHASE, 0, 0, uint32_t(bp.phases.size())});
+    bp.phases.push_back(D);
+    for (size_t i : taken) {
+      const LGate& g = G[i];
+      Instr in{g.kind, uint32_t(regbit[g.p[0]]), 0, uint32_t(bp.coef.size() / 2)};
+      const std::vector<cd>& a = g.g->a;
+      switch (g.kind) {
+        case LK_1Q:
+          for (int k = 0; k < 4; ++k) push_coef(bp, a[size_t(k)]);
+          break;
+        case LK_D1:
+          push_coef(bp, a[0]);
+          push_coef(bp, a[3]);
+          break;
+        case LK_CX:
+          in.b = uint32_t(regbit[g.p[1]]);
+          break;
+        default: {  // LK_2Q / LK_D2: the kernel wants matrix bit 0 on the lower register bit
+          const uint32_t ra = uint32_t(regbit[g.p[0]]), rbit = uint32_t(regbit[g.p[1]]);
+          const bool swap = ra > rbit;
+          in.a = std::min(ra, rbit);
+          in.b = std::max(ra, rbit);
+          auto perm = [&](int s) { return swap ? (((s & 1) << 1) | ((s >> 1) & 1)) : s; };
+          if (g.kind == LK_2Q) {
+            for (int r = 0; r < 4; ++r)
+              for (int c = 0; c < 4; ++c) push_coef(bp, a[size_t(perm(r) * 4 + perm(c))]);
+          } else {
+            for (int r = 0; r < 4; ++r) push_coef(bp, a[size_t(perm(r) * 4 + perm(r))]);
+          }
+          break;
+        }
+      }
+      bp.prog.push_back(in);
+    }
+  }
+}
+
+}  // namespace
+
+std::unique_ptr<BatchPlan> build_batch(const qsvb_circuit* circuits, size_t ncirc, int dtype, uint32_t local_bits) {
+  QSVB_REQUIRE(circuits != nullptr && ncirc > 0, "empty batch");
+  QSVB_REQUIRE(ncirc <= (1u << 20), "at most 2^20 circuits per batch");
+  QSVB_REQUIRE(dtype == QSVB_C64 || dtype == QSVB_C128, "dtype must be QSVB_C64 or QSVB_C128");
+  QSVB_REQUIRE(local_bits >= 7 && local_bits <= uint32_t(kMaxLocal), "local qubits must be 7..14");
+  auto bp = std::make_unique<BatchPlan>();
+  bp->dtype = dtype;
+  bp->local_bits = local_bits;
+  bp->rb = dtype == QSVB_C128 ? 4u : 5u;
+  bp->swz_w = dtype == QSVB_C128 ? 4u : 5u;
+  bp->ncirc = uint32_t(ncirc);
+  std::vector<std::vector<uint32_t>> circuit_passes(ncirc);
+  std::vector<double> cost(ncirc);
+  const double eb = dtype == QSVB_C128 ? 16.0 : 8.0;
+  double bytes = 0, flops = 0;
+  for (size_t ci = 0; ci < ncirc; ++ci) {
+    const qsvb_circuit& c = circuits[ci];
+    validate_circuit(&c);
+    QSVB_REQUIRE(c.n_qubits <= 30, "batched circuits have at most 30 qubits");
+    const uint32_t n = c.n_qubits;
+    bp->nq.push_back(n);
+    const std::vector<HostGate> gates = fuse_single_qubit_runs(c);
+    std::vector<uint32_t> kinds(gates.size());
+    for (size_t i = 0; i < gates.size(); ++i) kinds[i] = gate_kind(gates[i]);
+    const uint32_t L = std::min(n, local_bits);
+    const bool single = n <= local_bits;
+    const double amps = std::ldexp(1.0, int(n));
+    std::vector<char> done(gates.size(), 0);
+    size_t first_open = 0;
+    uint64_t state_off = 0;
+    if (!single) {
+      state_off = bp->state_amps;
+      bp->state_amps += uint64_t(1) << n;
+    }
+    bp->prob_off.push_back(bp->prob_total);
+    bp->prob_total += uint64_t(1) << n;
+    do {
+      while (first_open < gates.size() && done[first_open]) ++first_open;
+      // local set: all qubits, or bits 0..4 plus the qubits of the first pending gates
+      uint64_t S = 0;
+      if (single) {
+        S = (1ull << n) - 1ull;
+      } else {
+        S = (1ull << 5) - 1ull;
+        for (size_t i = first_open; i < gates.size() && uint32_t(__builtin_popcountll(S)) < L; ++i) {
+          if (done[i]) continue;
+          uint64_t m = 0;
+          for (uint32_t j = 0; j < gates[i].m; ++j) m |= 1ull << gates[i].q[j];
+          if (uint32_t(__builtin_popcountll(S | m)) <= L) S |= m;
+        }
+        for (uint32_t b = 5; b < n && uint32_t(__builtin_popcountll(S)) < L; ++b) S |= 1ull << b;
+      }
+      PassDev P{};
+      P.circuit = uint32_t(ci);
+      P.nlocal = uint32_t(__builtin_popcountll(S));
+      uint32_t nl = 0, nn = 0;
+      int pos[64];
+      for (uint32_t b = 0; b < n; ++b) {
+        if ((S >> b) & 1) {
+          pos[b] = int(nl);
+          P.local[nl++] = uint8_t(b);
+        } else {
+          pos[b] = -1;
+          P.nonlocal[nn++] = uint8_t(b);
+        }
+      }
+      P.nnon = nn;
+      P.ntiles = 1u << nn;
+      P.state_off = state_off;
+      P.prob_off = bp->prob_off.back();
+      std::vector<LGate> G;
+      uint64_t blocked = 0;
+      for (size_t i = first_open; i < gates.size(); ++i) {
+        if (done[i]) continue;
+        uint64_t m = 0;
+        for (uint32_t j = 0; j < gates[i].m; ++j) m |= 1ull << gates[i].q[j];
+        if ((m & ~S) == 0 && (m & blocked) == 0) {
+          done[i] = 1;
+          const LGate g{kinds[i],
+                        {uint32_t(pos[gates[i].q[0]]), gates[i].m == 2 ? uint32_t(pos[gates[i].q[1]]) : 0u},
+                        &gates[i]};
+          G.push_back(g);
+          flops += amps * (g.kind == LK_1Q ? 16.0 : g.kind == LK_2Q ? 32.0 : g.kind == LK_CX ? 0.0 : 6.0);
+        } else {
+          blocked |= m;
+        }
+      }
+      P.prog_off = uint32_t(bp->prog.size());
+      emit_phases(*bp, G, P.nlocal);
+      P.prog_len = uint32_t(bp->prog.size()) - P.prog_off;
+      P.first = circuit_passes[ci].empty() ? 1u : 0u;
+      P.prev = circuit_passes[ci].empty() ? ~0u : circuit_passes[ci].back();
+      circuit_passes[ci].push_back(uint32_t(bp->passes.size()));
+      bp->passes.push_back(P);
+    } while (std::find(done.begin(), done.end(), char(0)) != done.end());
+    // the last pass writes probabilities and <Z_0> partials
+    PassDev& last = bp->passes[circuit_passes[ci].back()];
+    last.last = 1;
+    last.zslot = bp->zslots;
+    bp->zoff.push_back(bp->zslots);
+    bp->zcnt.push_back(last.ntiles);
+    bp->zslots += last.ntiles;
+    const size_t np = circuit_passes[ci].size();
+    bytes += amps * 8.0 + double(np - 1) * 2.0 * amps * eb;
+    cost[ci] = double(np) * amps + double(gates.size()) * amps / 16.0;
+  }
+  // work items: level by level, costliest circuits first within a level
+  std::vector<uint32_t> order(ncirc);
+  std::iota(order.begin(), order.end(), 0u);
+  std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return cost[a] > cost[b]; });
+  size_t max_passes = 0;
+  for (auto& v : circuit_passes) max_passes = std::max(max_passes, v.size());
+  for (size_t lvl = 0; lvl < max_passes; ++lvl)
+    for (uint32_t ci : order)
+      if (lvl < circuit_passes[ci].size()) {
+        const uint32_t pi = circuit_passes[ci][lvl];
+        for (uint32_t t = 0; t < bp->passes[pi].ntiles; ++t) bp->items.push_back({pi, t});
+      }
+  QSVB_REQUIRE(bp->items.size() < (1ull << 31), "batch too large");
+  bp->stats.n_gates_in = 0;
+  for (size_t ci = 0; ci < ncirc; ++ci) bp->stats.n_gates_in += circuits[ci].n_gates;
+  bp->stats.n_sweeps = bp->passes.size();
+  bp->stats.n_sweeps_by_kind[0] = bp->phases.size();  // register phases
+  bp->stats.algorithmic_bytes = bytes;
+  bp->stats.full_sweep_bytes = double(bp->prob_total) * 8.0;
+  bp->stats.flops = flops;
+  return bp;
+}
+
+}  // namespace qsvb
+
+// ----------------------------------------------------------------------------- batch object
+struct qsvb_batch {
+  std::unique_ptr<qsvb::BatchPlan> plan;
+  int device = 0;
+  void* d_items = nullptr;
+  void* d_passes = nullptr;
+  void* d_phases = nullptr;
+  void* d_prog = nullptr;
+  void* d_coef = nullptr;
+  void* d_sre = nullptr;
+  void* d_sim = nullptr;
+  void* d_zcnt = nullptr;
+  void* d_zoff = nullptr;
+  double* d_probs = nullptr;
+  double* d_zpart = nullptr;
+  double* d_z0 = nullptr;
+  uint32_t* d_done = nullptr;
+  uint32_t* d_queue = nullptr;
+  long long* d_prof = nullptr;  // per-block cycle counters (QSVB_BATCH_PROFILE)
+  cudaGraphExec_t graph = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  int grid = 0;
+  size_t smem = 0;
+  ~qsvb_batch() {
+    if (graph) cudaGraphExecDestroy(graph);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    void* ptrs[] = {d_items, d_passes, d_phases, d_prog, d_coef, d_sre, d_sim, d_zcnt, d_zoff,
+                    d_probs, d_zpart, d_z0, d_done, d_queue, d_prof};
+    for (void* p : ptrs)
+      if (p) cudaFree(p);
+  }
+};
+
+namespace qsvb {
+namespace {
+
+template <class T> void upload_vec(void** dst, const std::vector<T>& v, cudaStream_t s) {
+  QSVB_CK(cudaMalloc(dst, std::max<size_t>(v.size(), 1) * sizeof(T)));
+  if (!v.empty()) QSVB_CK(cudaMemcpyAsync(*dst, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s));
+}
+
+template <class R, int RB, int W> void configure(qsvb_batch* b, qsvb_ctx* c) {
+  auto fn = k_batch<R, RB, W>;
+  QSVB_CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(b->smem)));
+  QSVB_CK(cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout,
+                               int(cudaSharedmemCarveoutMaxShared)));
+  int occ = 0;
+  QSVB_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, kBatchThreads, b->smem));
+  QSVB_REQUIRE(occ >= 1, "batched kernel does not fit on an SM");
+  b->grid = c->num_sms * occ;
+}
+
+template <class R, int RB, int W> void launch(qsvb_batch* b, qsvb_ctx* c, cudaStream_t s) {
+  const BatchPlan& bp = *b->plan;
+  k_batch<R, RB, W><<<unsigned(b->grid), kBatchThreads, b->smem, s>>>(
+      static_cast<const Item*>(b->d_items), uint32_t(bp.items.size()), static_cast<const PassDev*>(b->d_passes),
+      static_cast<const PhaseDev*>(b->d_phases), static_cast<const Instr*>(b->d_prog),
+      static_cast<const R*>(b->d_coef), static_cast<R*>(b->d_sre), static_cast<R*>(b->d_sim), b->d_probs,
+      b->d_zpart, b->d_done, b->d_queue, c->d_err, bp.local_bits, b->d_prof);
+}
+
+}  // namespace
+
+uint32_t batch_max_local_bits(int dtype) { return dtype == QSVB_C128 ? 13u : 14u; }
+
+qsvb_batch* batch_create(qsvb_ctx* c, const qsvb_circuit* circuits, size_t n, int dtype, uint32_t local_qubits) {
+  QSVB_REQUIRE(dtype == QSVB_C64 || dtype == QSVB_C128, "dtype must be QSVB_C64 or QSVB_C128");
+  const uint32_t cap = batch_max_local_bits(dtype);
+  QSVB_REQUIRE(local_qubits <= cap, "local qubits above " + std::to_string(cap) + " do not fit in shared memory");
+  auto b = std::make_unique<qsvb_batch>();
+  b->plan = build_batch(circuits, n, dtype, local_qubits ? local_qubits : cap);
+  const BatchPlan& bp = *b->plan;
+  b->device = c->device;
+  const bool f64 = dtype == QSVB_C128;
+  const size_t rb = f64 ? 8 : 4;
+  {
+    size_t free_b = 0, total_b = 0;
+    QSVB_CK(cudaMemGetInfo(&free_b, &total_b));
+    const double need = double(bp.state_amps) * 2.0 * double(rb) + double(bp.prob_total) * 8.0 +
+                        double(bp.items.size()) * sizeof(Item) + double(bp.passes.size()) * (sizeof(PassDev) + 4) +
+                        double(bp.prog.size()) * sizeof(Instr) + double(bp.coef.size()) * 8.0;
+    if (need > double(free_b))
+      throw Error(QSVB_E_OOM, "batch needs " + std::to_string(need / 1e9) + " GB of device memory, " +
+                                  std::to_string(double(free_b) / 1e9) + " GB free");
+  }
+  cudaStream_t s = c->stream;
+  upload_vec(&b->d_items, bp.items, s);
+  upload_vec(&b->d_passes, bp.passes, s);
+  upload_vec(&b->d_phases, bp.phases, s);
+  upload_vec(&b->d_prog, bp.prog, s);
+  if (f64) {
+    upload_vec(&b->d_coef, bp.coef, s);
+  } else {
+    const std::vector<float> cf(bp.coef.begin(), bp.coef.end());
+    upload_vec(&b->d_coef, cf, s);
+    QSVB_CK(cudaStreamSynchronize(s));
+  }
+  upload_vec(&b->d_zcnt, bp.zcnt, s);
+  upload_vec(&b->d_zoff, bp.zoff, s);
+  QSVB_CK(cudaMalloc(&b->d_sre, std::max<uint64_t>(bp.state_amps, 1) * rb));
+  QSVB_CK(cudaMalloc(&b->d_sim, std::max<uint64_t>(bp.state_amps, 1) * rb));
+  QSVB_CK(cudaMalloc(reinterpret_cast<void**>(&b->d_probs), bp.prob_total * 8));
+  QSVB_CK(cudaMalloc(reinterpret_cast<void**>(&b->d_zpart), bp.zslots * 8));
+  QSVB_CK(cudaMalloc(reinterpret_cast<void**>(&b->d_z0), size_t(bp.ncirc) * 8));
+  QSVB_CK(cudaMalloc(reinterpret_cast<void**>(&b->d_done), bp.passes.size() * 4));
+  QSVB_CK(cudaMalloc(reinterpret_cast<void**>(&b->d_queue), 4));
+  QSVB_CK(cudaStreamSynchronize(s));
+  b->smem = (size_t(2) * rb) << bp.local_bits;
+  if (f64) configure<double, 4, 4>(b.get(), c);
+  else configure<float, 5, 5>(b.get(), c);
+  // QSVB_BATCH_PROFILE=1: per-block cycles spent waiting, filling, in gates and writing out,
+  // averaged over blocks and printed to stderr after each run
+  if (std::getenv("QSVB_BATCH_PROFILE"))
+    QSVB_CK(cudaMalloc(reinterpret_cast<void**>(&b->d_prof), 5 * 8 * size_t(b->grid)));
+  QSVB_CK(cudaEventCreate(&b->e0));
+  QSVB_CK(cudaEventCreate(&b->e1));
+  // the per-run device work as one graph: counter resets, the persistent kernel, the <Z_0> sums
+  cudaGraph_t g = nullptr;
+  QSVB_CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+  cudaError_t cap_err = cudaMemsetAsync(b->d_done, 0, bp.passes.size() * 4, s);
+  if (cap_err == cudaSuccess) cap_err = cudaMemsetAsync(b->d_queue, 0, 4, s);
+  if (cap_err == cudaSuccess) {
+    if (f64) launch<double, 4, 4>(b.get(), c, s);
+    else launch<float, 5, 5>(b.get(), c, s);
+    cap_err = cudaGetLastError();
+  }
+  if (cap_err == cudaSuccess) {
+    k_batch_z0<<<(bp.ncirc + 255) / 256, 256, 0, s>>>(b->d_zpart, static_cast<const uint64_t*>(b->d_zoff),
+                                                       static_cast<const uint32_t*>(b->d_zcnt), bp.ncirc, b->d_z0);
+    cap_err = cudaGetLastError();
+  }
+  const cudaError_t end_err = cudaStreamEndCapture(s, &g);
+  if (cap_err != cudaSuccess || end_err != cudaSuccess) {
+    if (g) cudaGraphDestroy(g);
+    QSVB_CK(cap_err);
+    QSVB_CK(end_err);
+  }
+  const cudaError_t inst = cudaGraphInstantiate(&b->graph, g, 0);
+  cudaGraphDestroy(g);
+  QSVB_CK(inst);
+  return b.release();
+}
+
+void batch_run(qsvb_ctx* c, qsvb_batch* b, double* z0_out, double* probs_out, const uint64_t* probs_offset,
+               qsvb_plan_stats* stats) {
+  QSVB_REQUIRE(b != nullptr && b->plan, "null batch");
+  QSVB_REQUIRE(b->device == c->device, "batch belongs to another device");
+  const BatchPlan& bp = *b->plan;
+  cudaStream_t s = c->stream;
+  QSVB_CK(cudaEventRecord(b->e0, s));
+  QSVB_CK(cudaGraphLaunch(b->graph, s));
+  QSVB_CK(cudaEventRecord(b->e1, s));
+  if (z0_out) QSVB_CK(cudaMemcpyAsync(z0_out, b->d_z0, size_t(bp.ncirc) * 8, cudaMemcpyDeviceToHost, s));
+  QSVB_CK(cudaStreamSynchronize(s));
+  int flag = 0;
+  QSVB_CK(cudaMemcpy(&flag, c->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (flag) {
+    QSVB_CK(cudaMemset(c->d_err, 0, sizeof(int)));
+    throw Error(QSVB_E_TIMEOUT, "a batched-runner dependency wait ran out of its budget; results are invalid");
+  }
+  if (probs_out) {
+    if (probs_offset) {
+      for (size_t i = 0; i < bp.ncirc; ++i)
+        QSVB_CK(cudaMemcpyAsync(probs_out + probs_offset[i], b->d_probs + bp.prob_off[i],
+                                (size_t(1) << bp.nq[i]) * 8, cudaMemcpyDeviceToHost, s));
+    } else {
+      QSVB_CK(cudaMemcpyAsync(probs_out, b->d_probs, bp.prob_total * 8, cudaMemcpyDeviceToHost, s));
+    }
+    QSVB_CK(cudaStreamSynchronize(s));
+  }
+  if (b->d_prof) {
+    std::vector<long long> h(5 * size_t(b->grid));
+    QSVB_CK(cudaMemcpy(h.data(), b->d_prof, h.size() * 8, cudaMemcpyDeviceToHost));
+    double avg[5] = {0, 0, 0, 0, 0};
+    for (int i = 0; i < b->grid; ++i)
+      for (int j = 0; j < 5; ++j) avg[j] += double(h[5 * size_t(i) + size_t(j)]) / b->grid;
+    std::fprintf(stderr,
+                 "{\"batch_profile\": {\"wait\": %.0f, \"fill\": %.0f, \"gates\": %.0f, \"out\": %.0f, "
+                 "\"items_per_block\": %.1f}}\n",
+                 avg[0], avg[1], avg[2], avg[3], avg[4]);
+  }
+  if (stats) {
+    float ms = 0;
+    QSVB_CK(cudaEventElapsedTime(&ms, b->e0, b->e1));
+    *stats = bp.stats;
+    stats->predicted_seconds = double(ms) * 1e-3;  // measured device seconds of the batched graph
+  }
+}
+
+// Times every local-qubit count from 9 up to the shared-memory limit on this batch (two runs each,
+// the second timed) and returns the fastest.
+uint32_t batch_autotune(qsvb_ctx* c, const qsvb_circuit* circuits, size_t n, int dtype, double* seconds,
+                        size_t cap, size_t* count) {
+  const uint32_t hi = batch_max_local_bits(dtype), lo = 9;
+  if (count) *count = hi - lo + 1;
+  uint32_t best = hi;
+  double best_t = 1e300;
+  for (uint32_t L = lo; L <= hi; ++L) {
+    std::unique_ptr<qsvb_batch> b(batch_create(c, circuits, n, dtype, L));
+    qsvb_plan_stats st{};
+    batch_run(c, b.get(), nullptr, nullptr, nullptr, &st);
+    batch_run(c, b.get(), nullptr, nullptr, nullptr, &st);
+    if (seconds && size_t(L - lo) < cap) seconds[L - lo] = st.predicted_seconds;
+    if (st.predicted_seconds < best_t) {
+      best_t = st.predicted_seconds;
+      best = L;
+    }
+  }
+  return best;
+}
+
+}  // namespace qsvb
+
+void run_batch(qsvb_ctx* c, const qsvb_circuit* circuits, size_t n_circuits, int dtype, uint32_t local_qubits,
+               double* z0_out, double* probs_out, const uint64_t* probs_offset, qsvb_plan_stats* stats) {
+  std::unique_ptr<qsvb_batch> b(qsvb::batch_create(c, circuits, n_circuits, dtype, local_qubits));
+  qsvb::batch_run(c, b.get(), z0_out, probs_out, probs_offset, stats);
+}
+
+void free_batch(qsvb_batch* b) { delete b; }

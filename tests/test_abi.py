@@ -127,3 +127,24 @@ def test_qaoa_generator_graph_rule():
     assert deg[0] == 4 and np.all(deg[1:] == 3) and len(set(e)) == len(e) == 50
     c = qaoa_maxcut(12, 2, 3)
     assert c.n_qubits() == 12
+
+
+def test_packed_batch_matches_per_circuit_packing():
+    """The numpy-built batch packing lays out the same gate structs as PackedCircuit."""
+    import ctypes as C
+    from rustatevec_b200.circuits import ansatz_batch, random_circuit
+    circuits = ansatz_batch(5, 1, n_lo=3, n_hi=9, d_lo=1, d_hi=3) + [random_circuit(6, 40, 3)]
+    pb = L.PackedBatch(circuits)
+    assert pb.count == len(circuits)
+    for i, circ in enumerate(circuits):
+        pc = L.PackedCircuit(circ)
+        row = pb.circs[i]
+        assert int(row["n"]) == circ.n_qubits() and int(row["ngates"]) == pc.struct.n_gates
+        g = np.frombuffer((C.c_char * (40 * pc.struct.n_gates)).from_address(int(row["gates"])), dtype=L._GATE_DT)
+        for k in range(pc.struct.n_gates):
+            a = pc.gates[k]
+            m = a.n_qubits
+            assert int(g[k]["n"]) == m and list(a.qubits)[:m] == [int(x) for x in g[k]["q"][:m]]
+            want = np.ctypeslib.as_array(a.matrix, shape=(2 << (2 * m),))
+            got = np.ctypeslib.as_array(C.cast(int(g[k]["mat"]), C.POINTER(C.c_double)), shape=(2 << (2 * m),))
+            assert np.array_equal(want, got)
