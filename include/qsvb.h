@@ -228,26 +228,28 @@ int qsvb_execute_batch(qsvb_ctx* ctx, const qsvb_circuit* circuits, size_t n_cir
                        qsvb_plan_stats* stats);
 /* A reusable batch: the plan (passes over HBM, register phases, work queue), its device buffers
  * and one CUDA graph with the per-run device work, built once; each run replays the graph and
- * copies <Z_0> (and, when asked, the probabilities) to the host. local_qubits as in
- * qsvb_execute_batch_ex. No trait counterpart. */
+ * copies <Z_0> (and, when asked, the probabilities) to the host. local_qubits / register_qubits
+ * as in qsvb_execute_batch_ex. No trait counterpart. */
 typedef struct qsvb_batch qsvb_batch;
 int qsvb_batch_create(qsvb_ctx* ctx, const qsvb_circuit* circuits, size_t n_circuits, int dtype,
-                      uint32_t local_qubits, qsvb_batch** out);
+                      uint32_t local_qubits, uint32_t register_qubits, qsvb_batch** out);
 int qsvb_batch_run(qsvb_ctx* ctx, qsvb_batch* batch, double* z0_out, double* probs_out,
                    const uint64_t* probs_offset, qsvb_plan_stats* stats);
 int qsvb_batch_free(qsvb_ctx* ctx, qsvb_batch* batch);
-/* Times each local-qubit count from 9 up to the limit on this batch; writes the fastest to *best
- * and, when seconds != NULL, the device seconds of each candidate (ascending count, at most cap;
- * *count = number of candidates). */
+/* Times each tile shape (local qubits from two below the limit up to it, both register widths)
+ * on this batch; writes the fastest to *best_local / *best_register and, when seconds != NULL,
+ * the device seconds of each candidate (local-major order, at most cap; *count = number of
+ * candidates). */
 int qsvb_batch_autotune(qsvb_ctx* ctx, const qsvb_circuit* circuits, size_t n_circuits, int dtype,
-                        uint32_t* best, double* seconds, size_t cap, size_t* count);
-/* Same as qsvb_execute_batch, with the number of local qubits per shared-memory tile chosen by
- * the caller (7..14 for complex64, 7..13 for complex128; 0 = the engine's choice). Circuits with
- * at most that many qubits run whole in one thread block; larger ones take several passes over
- * HBM. */
+                        uint32_t* best_local, uint32_t* best_register, double* seconds, size_t cap,
+                        size_t* count);
+/* Same as qsvb_execute_batch with the tile shape chosen by the caller: local_qubits per
+ * shared-memory tile (7..14 for complex64, 7..13 for complex128) and register_qubits per thread
+ * (4 or 5 for complex64, 3 or 4 for complex128); 0 = the engine's choice. Circuits with at most
+ * local_qubits qubits run whole in one thread block; larger ones take several passes over HBM. */
 int qsvb_execute_batch_ex(qsvb_ctx* ctx, const qsvb_circuit* circuits, size_t n_circuits, int dtype,
-                          uint32_t local_qubits, double* z0_out, double* probs_out,
-                          const uint64_t* probs_offset, qsvb_plan_stats* stats);
+                          uint32_t local_qubits, uint32_t register_qubits, double* z0_out,
+                          double* probs_out, const uint64_t* probs_offset, qsvb_plan_stats* stats);
 
 #ifdef __cplusplus
 }

@@ -123,11 +123,12 @@ SIGNATURES = {
     "qsvb_costmodel_predict": (_i, [C.c_void_p, _sz, C.c_void_p]),
     "qsvb_execute_batch": (_i, [_vp, C.POINTER(CircuitS), _sz, _i, _dp, _dp, C.POINTER(_u64),
                                 C.POINTER(PlanStats)]),
-    "qsvb_batch_create": (_i, [_vp, C.POINTER(CircuitS), _sz, _i, _u32, C.POINTER(_vp)]),
+    "qsvb_batch_create": (_i, [_vp, C.POINTER(CircuitS), _sz, _i, _u32, _u32, C.POINTER(_vp)]),
     "qsvb_batch_run": (_i, [_vp, _vp, _dp, _dp, C.POINTER(_u64), C.POINTER(PlanStats)]),
     "qsvb_batch_free": (_i, [_vp, _vp]),
-    "qsvb_batch_autotune": (_i, [_vp, C.POINTER(CircuitS), _sz, _i, C.POINTER(_u32), _dp, _sz, C.POINTER(_sz)]),
-    "qsvb_execute_batch_ex": (_i, [_vp, C.POINTER(CircuitS), _sz, _i, _u32, _dp, _dp, C.POINTER(_u64),
+    "qsvb_batch_autotune": (_i, [_vp, C.POINTER(CircuitS), _sz, _i, C.POINTER(_u32), C.POINTER(_u32), _dp, _sz,
+                                 C.POINTER(_sz)]),
+    "qsvb_execute_batch_ex": (_i, [_vp, C.POINTER(CircuitS), _sz, _i, _u32, _u32, _dp, _dp, C.POINTER(_u64),
                                    C.POINTER(PlanStats)]),
 }
 

@@ -192,7 +192,7 @@ class B200Backend:
         self.run(state, circuit)
         return state
 
-    def execute_batch(self, circuits, probabilities: bool = True, local_qubits: int = 0):
+    def execute_batch(self, circuits, probabilities: bool = True, local_qubits: int = 0, register_qubits: int = 0):
         """Run many small circuits (each from |0..0>) in one persistent kernel: the batched form of
         ``execute`` followed by ``expectation_z(probs, 1)`` (sample.rs:177-200) per circuit.
 
@@ -209,7 +209,7 @@ class B200Backend:
             pptr = probs_flat.ctypes.data_as(C.POINTER(C.c_double))
         st = L.PlanStats()
         L.check(L.lib().qsvb_execute_batch_ex(self.ctx, pb.ptr(), pb.count, self.dtype, local_qubits,
-                                              z0.ctypes.data_as(C.POINTER(C.c_double)), pptr, None,
+                                              register_qubits, z0.ctypes.data_as(C.POINTER(C.c_double)), pptr, None,
                                               C.byref(st)))
         if probabilities:
             edges = np.concatenate([[0], np.cumsum(sizes)])

@@ -632,18 +632,18 @@ int qsvb_execute_batch(qsvb_ctx* c, const qsvb_circuit* circuits, size_t n_circu
   return guarded([&] {
     check_ctx(c);
     DeviceGuard dg(c->device);
-    run_batch(c, circuits, n_circuits, dtype, 0, z0_out, probs_out, probs_offset, stats);
+    run_batch(c, circuits, n_circuits, dtype, 0, 0, z0_out, probs_out, probs_offset, stats);
   });
 }
 
 int qsvb_batch_create(qsvb_ctx* c, const qsvb_circuit* circuits, size_t n_circuits, int dtype, uint32_t local_qubits,
-                      qsvb_batch** out) {
+                      uint32_t register_qubits, qsvb_batch** out) {
   return guarded([&] {
     check_ctx(c);
     QSVB_REQUIRE(out != nullptr, "null output");
     *out = nullptr;
     DeviceGuard dg(c->device);
-    *out = qsvb::batch_create(c, circuits, n_circuits, dtype, local_qubits);
+    *out = qsvb::batch_create(c, circuits, n_circuits, dtype, local_qubits, register_qubits);
   });
 }
 
@@ -664,23 +664,23 @@ int qsvb_batch_free(qsvb_ctx* c, qsvb_batch* b) {
   });
 }
 
-int qsvb_batch_autotune(qsvb_ctx* c, const qsvb_circuit* circuits, size_t n_circuits, int dtype, uint32_t* best,
-                        double* seconds, size_t cap, size_t* count) {
+int qsvb_batch_autotune(qsvb_ctx* c, const qsvb_circuit* circuits, size_t n_circuits, int dtype,
+                        uint32_t* best_local, uint32_t* best_register, double* seconds, size_t cap, size_t* count) {
   return guarded([&] {
     check_ctx(c);
-    QSVB_REQUIRE(best != nullptr, "null output");
+    QSVB_REQUIRE(best_local != nullptr && best_register != nullptr, "null output");
     DeviceGuard dg(c->device);
-    *best = qsvb::batch_autotune(c, circuits, n_circuits, dtype, seconds, cap, count);
+    qsvb::batch_autotune(c, circuits, n_circuits, dtype, best_local, best_register, seconds, cap, count);
   });
 }
 
 int qsvb_execute_batch_ex(qsvb_ctx* c, const qsvb_circuit* circuits, size_t n_circuits, int dtype,
-                          uint32_t local_qubits, double* z0_out, double* probs_out, const uint64_t* probs_offset,
-                          qsvb_plan_stats* stats) {
+                          uint32_t local_qubits, uint32_t register_qubits, double* z0_out, double* probs_out,
+                          const uint64_t* probs_offset, qsvb_plan_stats* stats) {
   return guarded([&] {
     check_ctx(c);
     DeviceGuard dg(c->device);
-    run_batch(c, circuits, n_circuits, dtype, local_qubits, z0_out, probs_out, probs_offset, stats);
+    run_batch(c, circuits, n_circuits, dtype, local_qubits, register_qubits, z0_out, probs_out, probs_offset, stats);
   });
 }
 

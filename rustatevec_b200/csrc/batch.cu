@@ -36,6 +36,7 @@
 #include <cstdlib>
 #include <memory>
 #include <numeric>
+#include <type_traits>
 #include <string>
 #include <vector>
 
@@ -44,10 +45,10 @@
 namespace qsvb {
 namespace {
 
-constexpr int kBatchThreads = 256;
 constexpr int kMaxLocal = 14;
 constexpr int kMaxHi = 512;                   // 2^(kMaxLocal - 5): entries of the address / swizzle tables
 constexpr long long kSpinBudget = 1ll << 32;  // clock64 cycles (about 2 s)
+constexpr uint32_t kStageBytes = 32768;       // shared memory for one pass's program
 
 enum BatchOp : uint32_t { OP_PHASE = 0, OP_1Q = 1, OP_D1 = 2, OP_CX = 3, OP_2Q = 4, OP_D2 = 5 };
 
@@ -73,6 +74,8 @@ struct PassDev {
   uint64_t state_off;    // amplitude offset of the circuit's state
   uint64_t prob_off;     // offset of the circuit's probabilities
   uint64_t zslot;        // first <Z_0> partial slot (last pass)
+  uint32_t phase_off, nphase, coef_off, ncoef;  // the pass's phases and coefficients (complex units)
+  uint32_t staged;       // program fits the shared-memory staging area
 };
 
 struct Item {
@@ -107,61 +110,129 @@ __device__ __forceinline__ void cmac(R& yr, R& yi, R ar, R ai, R xr, R xi) {
   yi = fma(ai, xr, yi);
 }
 
+// ---- register storage of one group: complex64 keeps amplitude pairs (s, s^1) in float2 registers
+// so a gate on any register bit but 0 runs on Blackwell's paired FP32 FMA (two amplitudes per
+// instruction); complex128 keeps one amplitude per register.
+template <class R, int RB> struct Regs;
+template <int RB> struct Regs<float, RB> {
+  float2 r[(1 << RB) / 2], i[(1 << RB) / 2];
+  __device__ __forceinline__ float& re(int s) { return (s & 1) ? r[s >> 1].y : r[s >> 1].x; }
+  __device__ __forceinline__ float& im(int s) { return (s & 1) ? i[s >> 1].y : i[s >> 1].x; }
+};
+template <int RB> struct Regs<double, RB> {
+  double r[1 << RB], i[1 << RB];
+  __device__ __forceinline__ double& re(int s) { return r[s]; }
+  __device__ __forceinline__ double& im(int s) { return i[s]; }
+};
+
+__device__ __forceinline__ float2 bc(float x) { return make_float2(x, x); }
+
 // ---- gates on register bits (compile-time bit positions, so the amplitudes stay in registers)
 template <int J, class R, int RB>
-__device__ __forceinline__ void g1q(R* vr, R* vi, const R* __restrict__ c) {
+__device__ __forceinline__ void g1q(Regs<R, RB>& v, const R* __restrict__ c) {
   if constexpr (J < RB) {
     const R a0 = c[0], a1 = c[1], b0 = c[2], b1 = c[3], c0 = c[4], c1 = c[5], d0 = c[6], d1 = c[7];
+    if constexpr (std::is_same<R, float>::value && J >= 1) {
+      // two amplitudes per instruction; same operation order as the scalar path below
+      constexpr int HJ = 1 << (J - 1);
 #pragma unroll
-    for (int s = 0; s < (1 << RB); ++s) {
-      if (s & (1 << J)) continue;
-      const int t = s | (1 << J);
-      const R xr0 = vr[s], xi0 = vi[s], xr1 = vr[t], xi1 = vi[t];
-      R yr0 = 0, yi0 = 0, yr1 = 0, yi1 = 0;
-      cmac(yr0, yi0, a0, a1, xr0, xi0);
-      cmac(yr0, yi0, b0, b1, xr1, xi1);
-      cmac(yr1, yi1, c0, c1, xr0, xi0);
-      cmac(yr1, yi1, d0, d1, xr1, xi1);
-      vr[s] = yr0;
-      vi[s] = yi0;
-      vr[t] = yr1;
-      vi[t] = yi1;
+      for (int h = 0; h < (1 << RB) / 2; ++h) {
+        if (h & HJ) continue;
+        const int t = h | HJ;
+        const float2 xr0 = v.r[h], xi0 = v.i[h], xr1 = v.r[t], xi1 = v.i[t];
+        float2 yr0 = __fmul2_rn(bc(a0), xr0), yi0 = __fmul2_rn(bc(a0), xi0);
+        float2 yr1 = __fmul2_rn(bc(c0), xr0), yi1 = __fmul2_rn(bc(c0), xi0);
+        yr0 = __ffma2_rn(bc(-a1), xi0, yr0);
+        yi0 = __ffma2_rn(bc(a1), xr0, yi0);
+        yr1 = __ffma2_rn(bc(-c1), xi0, yr1);
+        yi1 = __ffma2_rn(bc(c1), xr0, yi1);
+        yr0 = __ffma2_rn(bc(b0), xr1, yr0);
+        yi0 = __ffma2_rn(bc(b0), xi1, yi0);
+        yr1 = __ffma2_rn(bc(d0), xr1, yr1);
+        yi1 = __ffma2_rn(bc(d0), xi1, yi1);
+        yr0 = __ffma2_rn(bc(-b1), xi1, yr0);
+        yi0 = __ffma2_rn(bc(b1), xr1, yi0);
+        yr1 = __ffma2_rn(bc(-d1), xi1, yr1);
+        yi1 = __ffma2_rn(bc(d1), xr1, yi1);
+        v.r[h] = yr0;
+        v.i[h] = yi0;
+        v.r[t] = yr1;
+        v.i[t] = yi1;
+      }
+    } else {
+#pragma unroll
+      for (int s = 0; s < (1 << RB); ++s) {
+        if (s & (1 << J)) continue;
+        const int t = s | (1 << J);
+        const R xr0 = v.re(s), xi0 = v.im(s), xr1 = v.re(t), xi1 = v.im(t);
+        R yr0 = a0 * xr0, yi0 = a0 * xi0, yr1 = c0 * xr0, yi1 = c0 * xi0;
+        yr0 = fma(-a1, xi0, yr0);
+        yi0 = fma(a1, xr0, yi0);
+        yr1 = fma(-c1, xi0, yr1);
+        yi1 = fma(c1, xr0, yi1);
+        yr0 = fma(b0, xr1, yr0);
+        yi0 = fma(b0, xi1, yi0);
+        yr1 = fma(d0, xr1, yr1);
+        yi1 = fma(d0, xi1, yi1);
+        yr0 = fma(-b1, xi1, yr0);
+        yi0 = fma(b1, xr1, yi0);
+        yr1 = fma(-d1, xi1, yr1);
+        yi1 = fma(d1, xr1, yi1);
+        v.re(s) = yr0;
+        v.im(s) = yi0;
+        v.re(t) = yr1;
+        v.im(t) = yi1;
+      }
     }
   }
 }
 
 template <int J, class R, int RB>
-__device__ __forceinline__ void gd1(R* vr, R* vi, const R* __restrict__ c) {
+__device__ __forceinline__ void gd1(Regs<R, RB>& v, const R* __restrict__ c) {
   if constexpr (J < RB) {
     const R p0r = c[0], p0i = c[1], p1r = c[2], p1i = c[3];
+    if constexpr (std::is_same<R, float>::value) {
+      // the pair (s, s^1) shares bit J unless J == 0, where the lanes take the two phases
+      const float2 pr0 = J == 0 ? make_float2(p0r, p1r) : bc(p0r), pi0 = J == 0 ? make_float2(p0i, p1i) : bc(p0i);
+      const float2 pr1 = J == 0 ? pr0 : bc(p1r), pi1 = J == 0 ? pi0 : bc(p1i);
 #pragma unroll
-    for (int s = 0; s < (1 << RB); ++s) {
-      const R pr = (s & (1 << J)) ? p1r : p0r, pi = (s & (1 << J)) ? p1i : p0i;
-      const R xr = vr[s], xi = vi[s];
-      vr[s] = fma(pr, xr, -pi * xi);
-      vi[s] = fma(pr, xi, pi * xr);
+      for (int h = 0; h < (1 << RB) / 2; ++h) {
+        const bool one = J >= 1 && (h & (1 << (J - 1 < 0 ? 0 : J - 1)));
+        const float2 pr = one ? pr1 : pr0, pi = one ? pi1 : pi0;
+        const float2 xr = v.r[h], xi = v.i[h];
+        v.r[h] = __ffma2_rn(pr, xr, __fmul2_rn(make_float2(-pi.x, -pi.y), xi));
+        v.i[h] = __ffma2_rn(pr, xi, __fmul2_rn(pi, xr));
+      }
+    } else {
+#pragma unroll
+      for (int s = 0; s < (1 << RB); ++s) {
+        const R pr = (s & (1 << J)) ? p1r : p0r, pi = (s & (1 << J)) ? p1i : p0i;
+        const R xr = v.re(s), xi = v.im(s);
+        v.re(s) = fma(pr, xr, -pi * xi);
+        v.im(s) = fma(pr, xi, pi * xr);
+      }
     }
   }
 }
 
 template <int J, int K, class R, int RB>
-__device__ __forceinline__ void gcx(R* vr, R* vi) {
+__device__ __forceinline__ void gcx(Regs<R, RB>& v) {
   if constexpr (J < RB && K < RB && J != K) {
 #pragma unroll
     for (int s = 0; s < (1 << RB); ++s) {
       if (!(s & (1 << J)) || (s & (1 << K))) continue;
       const int t = s | (1 << K);
-      const R tr = vr[s], ti = vi[s];
-      vr[s] = vr[t];
-      vi[s] = vi[t];
-      vr[t] = tr;
-      vi[t] = ti;
+      const R tr = v.re(s), ti = v.im(s);
+      v.re(s) = v.re(t);
+      v.im(s) = v.im(t);
+      v.re(t) = tr;
+      v.im(t) = ti;
     }
   }
 }
 
 template <int J, int K, class R, int RB>
-__device__ __forceinline__ void g2q(R* vr, R* vi, const R* __restrict__ c) {
+__device__ __forceinline__ void g2q(Regs<R, RB>& v, const R* __restrict__ c) {
   if constexpr (J < K && K < RB) {
 #pragma unroll
     for (int s = 0; s < (1 << RB); ++s) {
@@ -170,31 +241,31 @@ __device__ __forceinline__ void g2q(R* vr, R* vi, const R* __restrict__ c) {
       R xr[4], xi[4];
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
-        xr[q] = vr[idx[q]];
-        xi[q] = vi[idx[q]];
+        xr[q] = v.re(idx[q]);
+        xi[q] = v.im(idx[q]);
       }
 #pragma unroll
       for (int r = 0; r < 4; ++r) {
         R yr = 0, yi = 0;
 #pragma unroll
         for (int q = 0; q < 4; ++q) cmac(yr, yi, c[2 * (4 * r + q)], c[2 * (4 * r + q) + 1], xr[q], xi[q]);
-        vr[idx[r]] = yr;
-        vi[idx[r]] = yi;
+        v.re(idx[r]) = yr;
+        v.im(idx[r]) = yi;
       }
     }
   }
 }
 
 template <int J, int K, class R, int RB>
-__device__ __forceinline__ void gd2(R* vr, R* vi, const R* __restrict__ c) {
+__device__ __forceinline__ void gd2(Regs<R, RB>& v, const R* __restrict__ c) {
   if constexpr (J < K && K < RB) {
 #pragma unroll
     for (int s = 0; s < (1 << RB); ++s) {
       const int d = ((s >> J) & 1) | (((s >> K) & 1) << 1);
       const R pr = c[2 * d], pi = c[2 * d + 1];
-      const R xr = vr[s], xi = vi[s];
-      vr[s] = fma(pr, xr, -pi * xi);
-      vi[s] = fma(pr, xi, pi * xr);
+      const R xr = v.re(s), xi = v.im(s);
+      v.re(s) = fma(pr, xr, -pi * xi);
+      v.im(s) = fma(pr, xi, pi * xr);
     }
   }
 }
@@ -212,35 +283,35 @@ __device__ __forceinline__ void gd2(R* vr, R* vi, const R* __restrict__ c) {
   case 3 * 8 + 4: F<3, 4, R, RB>(__VA_ARGS__); break;
 
 template <class R, int RB>
-__device__ __forceinline__ void apply_instr(const Instr& in, R* vr, R* vi, const R* __restrict__ coef) {
+__device__ __forceinline__ void apply_instr(const Instr& in, Regs<R, RB>& v, const R* __restrict__ coef) {
   const R* c = coef + 2 * size_t(in.coef);
   switch (in.op) {
     case OP_1Q:
       switch (in.a) {
-        case 0: g1q<0, R, RB>(vr, vi, c); break;
-        case 1: g1q<1, R, RB>(vr, vi, c); break;
-        case 2: g1q<2, R, RB>(vr, vi, c); break;
-        case 3: g1q<3, R, RB>(vr, vi, c); break;
-        case 4: g1q<4, R, RB>(vr, vi, c); break;
+        case 0: g1q<0, R, RB>(v, c); break;
+        case 1: g1q<1, R, RB>(v, c); break;
+        case 2: g1q<2, R, RB>(v, c); break;
+        case 3: g1q<3, R, RB>(v, c); break;
+        case 4: g1q<4, R, RB>(v, c); break;
       }
       break;
     case OP_D1:
       switch (in.a) {
-        case 0: gd1<0, R, RB>(vr, vi, c); break;
-        case 1: gd1<1, R, RB>(vr, vi, c); break;
-        case 2: gd1<2, R, RB>(vr, vi, c); break;
-        case 3: gd1<3, R, RB>(vr, vi, c); break;
-        case 4: gd1<4, R, RB>(vr, vi, c); break;
+        case 0: gd1<0, R, RB>(v, c); break;
+        case 1: gd1<1, R, RB>(v, c); break;
+        case 2: gd1<2, R, RB>(v, c); break;
+        case 3: gd1<3, R, RB>(v, c); break;
+        case 4: gd1<4, R, RB>(v, c); break;
       }
       break;
     case OP_CX: {
       const uint32_t lo = min(in.a, in.b), hi = max(in.a, in.b);
       const bool fwd = in.a < in.b;  // the control is the lower register bit
       switch (lo * 8 + hi) {
-#define QSVB_CX_CASE(J, K)             \
-  case J * 8 + K:                      \
-    if (fwd) gcx<J, K, R, RB>(vr, vi); \
-    else gcx<K, J, R, RB>(vr, vi);     \
+#define QSVB_CX_CASE(J, K)       \
+  case J * 8 + K:                \
+    if (fwd) gcx<J, K, R, RB>(v); \
+    else gcx<K, J, R, RB>(v);     \
     break;
         QSVB_CX_CASE(0, 1)
         QSVB_CX_CASE(0, 2)
@@ -257,16 +328,16 @@ __device__ __forceinline__ void apply_instr(const Instr& in, R* vr, R* vi, const
       break;
     }
     case OP_2Q:
-      switch (in.a * 8 + in.b) { QSVB_PAIR_CASES(g2q, vr, vi, c) }
+      switch (in.a * 8 + in.b) { QSVB_PAIR_CASES(g2q, v, c) }
       break;
     case OP_D2:
-      switch (in.a * 8 + in.b) { QSVB_PAIR_CASES(gd2, vr, vi, c) }
+      switch (in.a * 8 + in.b) { QSVB_PAIR_CASES(gd2, v, c) }
       break;
   }
 }
 
-template <class R, int RB, int W>
-__global__ void __launch_bounds__(kBatchThreads, 1)
+template <class R, int RB, int W, int NT>
+__global__ void __launch_bounds__(NT, 1)
     k_batch(const Item* __restrict__ items, uint32_t nitems, const PassDev* __restrict__ passes,
             const PhaseDev* __restrict__ phases, const Instr* __restrict__ prog, const R* __restrict__ coef,
             R* __restrict__ sre, R* __restrict__ sim, double* __restrict__ probs, double* __restrict__ zpart,
@@ -275,21 +346,23 @@ __global__ void __launch_bounds__(kBatchThreads, 1)
   extern __shared__ __align__(16) uint8_t smem_raw[];
   R* xr = reinterpret_cast<R*>(smem_raw);
   R* xi = xr + (size_t(1) << lbits);  // every pass has nlocal <= lbits
+  uint8_t* stage = reinterpret_cast<uint8_t*>(xi + (size_t(1) << lbits));  // the pass's program
   __shared__ uint64_t s_gaddr[kMaxHi];
   __shared__ uint16_t s_swz[kMaxHi];
   __shared__ uint32_t s_item;
-  __shared__ double s_red[kBatchThreads / 32];
+  __shared__ double s_red[NT / 32];
   __shared__ int s_ok;
   const int tid = threadIdx.x;
   constexpr int NV = 1 << RB;
   // swizzle table over the index bits above W
-  for (uint32_t h = tid; h < (1u << (lbits - W)); h += kBatchThreads) {
+  for (uint32_t h = tid; h < (1u << (lbits - W)); h += NT) {
     uint32_t v = 0;
     for (int i = 0; i < int(lbits) - W; ++i)
       if ((h >> i) & 1u) v ^= swz_col(W + i, W);
     s_swz[h] = uint16_t(v);
   }
   long long t_wait = 0, t_fill = 0, t_gates = 0, t_out = 0, n_items = 0, t_mark = prof ? clock64() : 0;
+  uint32_t staged_pass = ~0u;
   while (true) {
     if (tid == 0) s_item = atomicAdd(queue, 1u);
     __syncthreads();
@@ -327,7 +400,7 @@ __global__ void __launch_bounds__(kBatchThreads, 1)
     {
       uint64_t base = 0;
       for (uint32_t j = 0; j < P.nnon; ++j) base |= uint64_t((item.tile >> j) & 1u) << P.nonlocal[j];
-      for (uint32_t h = tid; h < (1u << nhi); h += kBatchThreads) {
+      for (uint32_t h = tid; h < (1u << nhi); h += NT) {
         uint64_t a = base;
         for (uint32_t j = 0; j < nhi; ++j) a |= uint64_t((h >> j) & 1u) << P.local[5 + j];
         s_gaddr[h] = a;
@@ -336,42 +409,61 @@ __global__ void __launch_bounds__(kBatchThreads, 1)
     __syncthreads();
     if (prof) t_wait += clock64() - t_mark, t_mark = clock64(), ++n_items;
     if (!s_ok) continue;
+    // the pass's instructions, phases and coefficients into shared memory (kept while the next
+    // item is a tile of the same pass), overlapped with the tile fill
+    const uint32_t ph_bytes = P.prog_len * uint32_t(sizeof(Instr));
+    const uint32_t co_bytes = (ph_bytes + P.nphase * uint32_t(sizeof(PhaseDev)) + 7u) & ~7u;
+    if (P.staged && staged_pass != item.pass) {
+      const uint32_t* src0 = reinterpret_cast<const uint32_t*>(prog + P.prog_off);
+      const uint32_t* src1 = reinterpret_cast<const uint32_t*>(phases + P.phase_off);
+      const uint32_t* src2 = reinterpret_cast<const uint32_t*>(coef + 2 * size_t(P.coef_off));
+      uint32_t* dst = reinterpret_cast<uint32_t*>(stage);
+      const uint32_t n0 = ph_bytes / 4, n1 = P.nphase * uint32_t(sizeof(PhaseDev)) / 4;
+      const uint32_t n2 = P.ncoef * 2u * uint32_t(sizeof(R)) / 4;
+      for (uint32_t w = tid; w < n0; w += NT) cp_async_elem(dst + w, src0 + w);
+      for (uint32_t w = tid; w < n1; w += NT) cp_async_elem(dst + n0 + w, src1 + w);
+      for (uint32_t w = tid; w < n2; w += NT) cp_async_elem(dst + co_bytes / 4 + w, src2 + w);
+    }
+    staged_pass = P.staged ? item.pass : ~0u;
+    const Instr* pprog = P.staged ? reinterpret_cast<const Instr*>(stage) : prog + P.prog_off;
+    const PhaseDev* pph = P.staged ? reinterpret_cast<const PhaseDev*>(stage + ph_bytes) : phases + P.phase_off;
+    const R* pcoef = P.staged ? reinterpret_cast<const R*>(stage + co_bytes) : coef + 2 * size_t(P.coef_off);
     const uint32_t lowmask = L >= 5 ? 31u : (T - 1u);
     R* gre = sre + P.state_off;
     R* gim = sim + P.state_off;
     if (P.first) {
-      for (uint32_t x = tid; x < T; x += kBatchThreads) {
+      for (uint32_t x = tid; x < T; x += NT) {
         xr[x] = R(0);
         xi[x] = R(0);
       }
       __syncthreads();
       if (tid == 0 && item.tile == 0) xr[0] = R(1);  // the swizzle maps 0 to 0
     } else {
-      for (uint32_t x = tid; x < T; x += kBatchThreads) {
+      for (uint32_t x = tid; x < T; x += NT) {
         const uint64_t a = s_gaddr[x >> 5] | (x & lowmask);
         const uint32_t y = x ^ s_swz[x >> W];
         cp_async_elem(xr + y, gre + a);
         cp_async_elem(xi + y, gim + a);
       }
-      asm volatile("cp.async.wait_all;" ::: "memory");
     }
+    asm volatile("cp.async.wait_all;" ::: "memory");
     __syncthreads();
     if (prof) t_fill += clock64() - t_mark, t_mark = clock64();
     // register phases: each group of 2^r amplitudes (fixed non-register bits) is loaded into one
     // thread's registers, takes all of the phase's gates there, and is written back
     uint32_t k = 0;
     while (k < P.prog_len) {
-      const PhaseDev& D = phases[prog[P.prog_off + k].coef];
+      const PhaseDev& D = pph[pprog[k].coef];
       const uint32_t r = D.r, nt = D.nt;
-      const uint32_t kbeg = P.prog_off + k + 1, kend = kbeg + D.ninstr;
+      const uint32_t kbeg = k + 1, kend = kbeg + D.ninstr;
       uint32_t rp[RB];
 #pragma unroll
       for (int j = 0; j < RB; ++j) rp[j] = D.rphys[j];
-      for (uint32_t grp = tid; grp < (1u << nt); grp += kBatchThreads) {
+      for (uint32_t grp = tid; grp < (1u << nt); grp += NT) {
         uint32_t x0 = 0;
         for (uint32_t i = 0; i < nt; ++i) x0 |= ((grp >> i) & 1u) << D.tpos[i];
         const uint32_t p0 = x0 ^ s_swz[x0 >> W];
-        R vr[NV], vi[NV];
+        Regs<R, RB> v;
 #pragma unroll
         for (int s = 0; s < NV; ++s) {
           if (uint32_t(s) >> r) continue;
@@ -379,10 +471,10 @@ __global__ void __launch_bounds__(kBatchThreads, 1)
 #pragma unroll
           for (int j = 0; j < RB; ++j)
             if (s & (1 << j)) off ^= rp[j];
-          vr[s] = xr[off];
-          vi[s] = xi[off];
+          v.re(s) = xr[off];
+          v.im(s) = xi[off];
         }
-        for (uint32_t kk = kbeg; kk < kend; ++kk) apply_instr<R, RB>(prog[kk], vr, vi, coef);
+        for (uint32_t kk = kbeg; kk < kend; ++kk) apply_instr<R, RB>(pprog[kk], v, pcoef);
 #pragma unroll
         for (int s = 0; s < NV; ++s) {
           if (uint32_t(s) >> r) continue;
@@ -390,11 +482,11 @@ __global__ void __launch_bounds__(kBatchThreads, 1)
 #pragma unroll
           for (int j = 0; j < RB; ++j)
             if (s & (1 << j)) off ^= rp[j];
-          xr[off] = vr[s];
-          xi[off] = vi[s];
+          xr[off] = v.re(s);
+          xi[off] = v.im(s);
         }
       }
-      k = kend - P.prog_off;
+      k = kend;
       __syncthreads();
     }
     if (prof) t_gates += clock64() - t_mark, t_mark = clock64();
@@ -402,7 +494,7 @@ __global__ void __launch_bounds__(kBatchThreads, 1)
       // FP64 probabilities and the <Z_0> partial (state bit 0 is local position 0)
       double z = 0.0;
       double* pout = probs + P.prob_off;
-      for (uint32_t x = tid; x < T; x += kBatchThreads) {
+      for (uint32_t x = tid; x < T; x += NT) {
         const uint32_t y = x ^ s_swz[x >> W];
         const double p = double(xr[y]) * double(xr[y]) + double(xi[y]) * double(xi[y]);
         __stcs(pout + (s_gaddr[x >> 5] | (x & lowmask)), p);
@@ -414,11 +506,11 @@ __global__ void __launch_bounds__(kBatchThreads, 1)
       __syncthreads();
       if (tid == 0) {
         double s = 0.0;
-        for (int w = 0; w < kBatchThreads / 32; ++w) s += s_red[w];
+        for (int w = 0; w < NT / 32; ++w) s += s_red[w];
         zpart[P.zslot + item.tile] = s;
       }
     } else {
-      for (uint32_t x = tid; x < T; x += kBatchThreads) {
+      for (uint32_t x = tid; x < T; x += NT) {
         const uint64_t a = s_gaddr[x >> 5] | (x & lowmask);
         const uint32_t y = x ^ s_swz[x >> W];
         __stcg(gre + a, xr[y]);
@@ -536,6 +628,8 @@ void push_coef(BatchPlan& bp, const cd& v) {
 
 // Splits a pass's gates into register phases and appends them to the plan's program.
 void emit_phases(BatchPlan& bp, const std::vector<LGate>& G, uint32_t nlocal) {
+  // phase and coefficient indices are relative to the pass (its program is staged as one block)
+  const size_t phase_base = bp.phases.size(), coef_base = bp.coef.size() / 2;
   const uint32_t rb = std::min(bp.rb, nlocal);
   const uint32_t W = bp.swz_w;
   const uint32_t all = (1u << nlocal) - 1u;
@@ -608,11 +702,11 @@ void emit_phases(BatchPlan& bp, const std::vector<LGate>& G, uint32_t nlocal) {
     D.nt = uint32_t(nonr.size());
     for (size_t i = 0; i < lanes.size(); ++i) D.tpos[i] = uint8_t(lanes[i]);
     D.ninstr = uint32_t(taken.size());
-    bp.prog.push_back(Instr{OP_PHASE, 0, 0, uint32_t(bp.phases.size())});
+    bp.prog.push_back(Instr{OP_PHASE, 0, 0, uint32_t(bp.phases.size() - phase_base)});
     bp.phases.push_back(D);
     for (size_t i : taken) {
       const LGate& g = G[i];
-      Instr in{g.kind, uint32_t(regbit[g.p[0]]), 0, uint32_t(bp.coef.size() / 2)};
+      Instr in{g.kind, uint32_t(regbit[g.p[0]]), 0, uint32_t(bp.coef.size() / 2 - coef_base)};
       const std::vector<cd>& a = g.g->a;
       switch (g.kind) {
         case LK_1Q:
@@ -647,7 +741,8 @@ void emit_phases(BatchPlan& bp, const std::vector<LGate>& G, uint32_t nlocal) {
 
 }  // namespace
 
-std::unique_ptr<BatchPlan> build_batch(const qsvb_circuit* circuits, size_t ncirc, int dtype, uint32_t local_bits) {
+std::unique_ptr<BatchPlan> build_batch(const qsvb_circuit* circuits, size_t ncirc, int dtype, uint32_t local_bits,
+                                       uint32_t reg_bits) {
   QSVB_REQUIRE(circuits != nullptr && ncirc > 0, "empty batch");
   QSVB_REQUIRE(ncirc <= (1u << 20), "at most 2^20 circuits per batch");
   QSVB_REQUIRE(dtype == QSVB_C64 || dtype == QSVB_C128, "dtype must be QSVB_C64 or QSVB_C128");
@@ -655,7 +750,7 @@ std::unique_ptr<BatchPlan> build_batch(const qsvb_circuit* circuits, size_t ncir
   auto bp = std::make_unique<BatchPlan>();
   bp->dtype = dtype;
   bp->local_bits = local_bits;
-  bp->rb = dtype == QSVB_C128 ? 4u : 5u;
+  bp->rb = reg_bits;
   bp->swz_w = dtype == QSVB_C128 ? 4u : 5u;
   bp->ncirc = uint32_t(ncirc);
   std::vector<std::vector<uint32_t>> circuit_passes(ncirc);
@@ -735,8 +830,17 @@ std::unique_ptr<BatchPlan> build_batch(const qsvb_circuit* circuits, size_t ncir
         }
       }
       P.prog_off = uint32_t(bp->prog.size());
+      P.phase_off = uint32_t(bp->phases.size());
+      P.coef_off = uint32_t(bp->coef.size() / 2);
       emit_phases(*bp, G, P.nlocal);
       P.prog_len = uint32_t(bp->prog.size()) - P.prog_off;
+      P.nphase = uint32_t(bp->phases.size()) - P.phase_off;
+      P.ncoef = uint32_t(bp->coef.size() / 2) - P.coef_off;
+      {
+        const size_t rsz = dtype == QSVB_C128 ? 8 : 4;
+        const size_t co = (P.prog_len * sizeof(Instr) + P.nphase * sizeof(PhaseDev) + 7) & ~size_t(7);
+        P.staged = co + size_t(P.ncoef) * 2 * rsz <= kStageBytes ? 1u : 0u;
+      }
       P.first = circuit_passes[ci].empty() ? 1u : 0u;
       P.prev = circuit_passes[ci].empty() ? ~0u : circuit_passes[ci].back();
       circuit_passes[ci].push_back(uint32_t(bp->passes.size()));
@@ -820,36 +924,64 @@ template <class T> void upload_vec(void** dst, const std::vector<T>& v, cudaStre
   if (!v.empty()) QSVB_CK(cudaMemcpyAsync(*dst, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s));
 }
 
-template <class R, int RB, int W> void configure(qsvb_batch* b, qsvb_ctx* c) {
-  auto fn = k_batch<R, RB, W>;
+template <class R, int RB, int W, int NT> void configure(qsvb_batch* b, qsvb_ctx* c) {
+  auto fn = k_batch<R, RB, W, NT>;
   QSVB_CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(b->smem)));
   QSVB_CK(cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout,
                                int(cudaSharedmemCarveoutMaxShared)));
   int occ = 0;
-  QSVB_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, kBatchThreads, b->smem));
+  QSVB_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, NT, b->smem));
   QSVB_REQUIRE(occ >= 1, "batched kernel does not fit on an SM");
   b->grid = c->num_sms * occ;
 }
 
-template <class R, int RB, int W> void launch(qsvb_batch* b, qsvb_ctx* c, cudaStream_t s) {
+template <class R, int RB, int W, int NT> void launch(qsvb_batch* b, qsvb_ctx* c, cudaStream_t s) {
   const BatchPlan& bp = *b->plan;
-  k_batch<R, RB, W><<<unsigned(b->grid), kBatchThreads, b->smem, s>>>(
+  k_batch<R, RB, W, NT><<<unsigned(b->grid), NT, b->smem, s>>>(
       static_cast<const Item*>(b->d_items), uint32_t(bp.items.size()), static_cast<const PassDev*>(b->d_passes),
       static_cast<const PhaseDev*>(b->d_phases), static_cast<const Instr*>(b->d_prog),
       static_cast<const R*>(b->d_coef), static_cast<R*>(b->d_sre), static_cast<R*>(b->d_sim), b->d_probs,
       b->d_zpart, b->d_done, b->d_queue, c->d_err, bp.local_bits, b->d_prof);
 }
 
+// The kernel variants: register bits (a group of 2^RB amplitudes per thread) and block size. The
+// widest register tile runs 256 threads with up to 255 registers each; one bit less fits 128
+// registers and runs 512 threads.
+void configure_any(qsvb_batch* b, qsvb_ctx* c, int dtype, uint32_t rb) {
+  if (dtype == QSVB_C128) {
+    if (rb == 4) configure<double, 4, 4, 256>(b, c);
+    else configure<double, 3, 4, 512>(b, c);
+  } else {
+    if (rb == 5) configure<float, 5, 5, 256>(b, c);
+    else configure<float, 4, 5, 512>(b, c);
+  }
+}
+
+void launch_any(qsvb_batch* b, qsvb_ctx* c, cudaStream_t s, int dtype, uint32_t rb) {
+  if (dtype == QSVB_C128) {
+    if (rb == 4) launch<double, 4, 4, 256>(b, c, s);
+    else launch<double, 3, 4, 512>(b, c, s);
+  } else {
+    if (rb == 5) launch<float, 5, 5, 256>(b, c, s);
+    else launch<float, 4, 5, 512>(b, c, s);
+  }
+}
+
 }  // namespace
 
 uint32_t batch_max_local_bits(int dtype) { return dtype == QSVB_C128 ? 13u : 14u; }
+uint32_t batch_max_register_bits(int dtype) { return dtype == QSVB_C128 ? 4u : 5u; }
 
-qsvb_batch* batch_create(qsvb_ctx* c, const qsvb_circuit* circuits, size_t n, int dtype, uint32_t local_qubits) {
+qsvb_batch* batch_create(qsvb_ctx* c, const qsvb_circuit* circuits, size_t n, int dtype, uint32_t local_qubits,
+                         uint32_t register_qubits) {
   QSVB_REQUIRE(dtype == QSVB_C64 || dtype == QSVB_C128, "dtype must be QSVB_C64 or QSVB_C128");
-  const uint32_t cap = batch_max_local_bits(dtype);
+  const uint32_t cap = batch_max_local_bits(dtype), rcap = batch_max_register_bits(dtype);
   QSVB_REQUIRE(local_qubits <= cap, "local qubits above " + std::to_string(cap) + " do not fit in shared memory");
+  QSVB_REQUIRE(register_qubits == 0 || register_qubits == rcap || register_qubits == rcap - 1,
+               "register qubits must be " + std::to_string(rcap - 1) + " or " + std::to_string(rcap));
+  const uint32_t regb = register_qubits ? register_qubits : rcap;
   auto b = std::make_unique<qsvb_batch>();
-  b->plan = build_batch(circuits, n, dtype, local_qubits ? local_qubits : cap);
+  b->plan = build_batch(circuits, n, dtype, local_qubits ? local_qubits : cap, regb);
   const BatchPlan& bp = *b->plan;
   b->device = c->device;
   const bool f64 = dtype == QSVB_C128;
@@ -886,9 +1018,8 @@ qsvb_batch* batch_create(qsvb_ctx* c, const qsvb_circuit* circuits, size_t n, in
   QSVB_CK(cudaMalloc(reinterpret_cast<void**>(&b->d_done), bp.passes.size() * 4));
   QSVB_CK(cudaMalloc(reinterpret_cast<void**>(&b->d_queue), 4));
   QSVB_CK(cudaStreamSynchronize(s));
-  b->smem = (size_t(2) * rb) << bp.local_bits;
-  if (f64) configure<double, 4, 4>(b.get(), c);
-  else configure<float, 5, 5>(b.get(), c);
+  b->smem = ((size_t(2) * rb) << bp.local_bits) + kStageBytes;
+  configure_any(b.get(), c, dtype, regb);
   // QSVB_BATCH_PROFILE=1: per-block cycles spent waiting, filling, in gates and writing out,
   // averaged over blocks and printed to stderr after each run
   if (std::getenv("QSVB_BATCH_PROFILE"))
@@ -901,8 +1032,7 @@ qsvb_batch* batch_create(qsvb_ctx* c, const qsvb_circuit* circuits, size_t n, in
   cudaError_t cap_err = cudaMemsetAsync(b->d_done, 0, bp.passes.size() * 4, s);
   if (cap_err == cudaSuccess) cap_err = cudaMemsetAsync(b->d_queue, 0, 4, s);
   if (cap_err == cudaSuccess) {
-    if (f64) launch<double, 4, 4>(b.get(), c, s);
-    else launch<float, 5, 5>(b.get(), c, s);
+    launch_any(b.get(), c, s, dtype, regb);
     cap_err = cudaGetLastError();
   }
   if (cap_err == cudaSuccess) {
@@ -968,33 +1098,37 @@ void batch_run(qsvb_ctx* c, qsvb_batch* b, double* z0_out, double* probs_out, co
   }
 }
 
-// Times every local-qubit count from 9 up to the shared-memory limit on this batch (two runs each,
-// the second timed) and returns the fastest.
-uint32_t batch_autotune(qsvb_ctx* c, const qsvb_circuit* circuits, size_t n, int dtype, double* seconds,
-                        size_t cap, size_t* count) {
-  const uint32_t hi = batch_max_local_bits(dtype), lo = 9;
-  if (count) *count = hi - lo + 1;
-  uint32_t best = hi;
+// Times every tile shape (local qubits 12 up to the shared-memory limit, either register width) on
+// this batch, two runs each with the second timed, and returns the fastest.
+void batch_autotune(qsvb_ctx* c, const qsvb_circuit* circuits, size_t n, int dtype, uint32_t* best_local,
+                    uint32_t* best_reg, double* seconds, size_t cap, size_t* count) {
+  const uint32_t hi = batch_max_local_bits(dtype), rhi = batch_max_register_bits(dtype);
+  size_t idx = 0;
   double best_t = 1e300;
-  for (uint32_t L = lo; L <= hi; ++L) {
-    std::unique_ptr<qsvb_batch> b(batch_create(c, circuits, n, dtype, L));
-    qsvb_plan_stats st{};
-    batch_run(c, b.get(), nullptr, nullptr, nullptr, &st);
-    batch_run(c, b.get(), nullptr, nullptr, nullptr, &st);
-    if (seconds && size_t(L - lo) < cap) seconds[L - lo] = st.predicted_seconds;
-    if (st.predicted_seconds < best_t) {
-      best_t = st.predicted_seconds;
-      best = L;
+  *best_local = hi;
+  *best_reg = rhi;
+  for (uint32_t L = hi - 2; L <= hi; ++L)
+    for (uint32_t rb = rhi - 1; rb <= rhi; ++rb, ++idx) {
+      std::unique_ptr<qsvb_batch> b(batch_create(c, circuits, n, dtype, L, rb));
+      qsvb_plan_stats st{};
+      batch_run(c, b.get(), nullptr, nullptr, nullptr, &st);
+      batch_run(c, b.get(), nullptr, nullptr, nullptr, &st);
+      if (seconds && idx < cap) seconds[idx] = st.predicted_seconds;
+      if (st.predicted_seconds < best_t) {
+        best_t = st.predicted_seconds;
+        *best_local = L;
+        *best_reg = rb;
+      }
     }
-  }
-  return best;
+  if (count) *count = idx;
 }
 
 }  // namespace qsvb
 
 void run_batch(qsvb_ctx* c, const qsvb_circuit* circuits, size_t n_circuits, int dtype, uint32_t local_qubits,
-               double* z0_out, double* probs_out, const uint64_t* probs_offset, qsvb_plan_stats* stats) {
-  std::unique_ptr<qsvb_batch> b(qsvb::batch_create(c, circuits, n_circuits, dtype, local_qubits));
+               uint32_t register_qubits, double* z0_out, double* probs_out, const uint64_t* probs_offset,
+               qsvb_plan_stats* stats) {
+  std::unique_ptr<qsvb_batch> b(qsvb::batch_create(c, circuits, n_circuits, dtype, local_qubits, register_qubits));
   qsvb::batch_run(c, b.get(), z0_out, probs_out, probs_offset, stats);
 }
 

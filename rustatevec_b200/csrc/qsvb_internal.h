@@ -149,15 +149,18 @@ struct qsvb_ctx {
 };
 
 void run_batch(qsvb_ctx* c, const qsvb_circuit* circuits, size_t n_circuits, int dtype, uint32_t local_qubits,
-               double* z0_out, double* probs_out, const uint64_t* probs_offset, qsvb_plan_stats* stats);
+               uint32_t register_qubits, double* z0_out, double* probs_out, const uint64_t* probs_offset,
+               qsvb_plan_stats* stats);
 void free_batch(qsvb_batch* b);
 namespace qsvb {
 uint32_t batch_max_local_bits(int dtype);
-qsvb_batch* batch_create(qsvb_ctx* c, const qsvb_circuit* circuits, size_t n, int dtype, uint32_t local_qubits);
+uint32_t batch_max_register_bits(int dtype);
+qsvb_batch* batch_create(qsvb_ctx* c, const qsvb_circuit* circuits, size_t n, int dtype, uint32_t local_qubits,
+                         uint32_t register_qubits);
 void batch_run(qsvb_ctx* c, qsvb_batch* b, double* z0_out, double* probs_out, const uint64_t* probs_offset,
                qsvb_plan_stats* stats);
-uint32_t batch_autotune(qsvb_ctx* c, const qsvb_circuit* circuits, size_t n, int dtype, double* seconds,
-                        size_t cap, size_t* count);
+void batch_autotune(qsvb_ctx* c, const qsvb_circuit* circuits, size_t n, int dtype, uint32_t* best_local,
+                    uint32_t* best_reg, double* seconds, size_t cap, size_t* count);
 }  // namespace qsvb
 
 struct qsvb_plan {

@@ -31,14 +31,14 @@ def oracle_probs(c):
     return re * re + im * im
 
 
-def check_batch(be, circuits, local_qubits=0):
+def check_batch(be, circuits, local_qubits=0, register_qubits=0):
     pb = L.PackedBatch(circuits)
     z0 = np.zeros(len(circuits))
     sizes = [1 << c.n_qubits() for c in circuits]
     probs = np.zeros(sum(sizes))
     st = L.PlanStats()
     L.check(L.lib().qsvb_execute_batch_ex(be.ctx, pb.ptr(), len(circuits), be.dtype, local_qubits,
-                                          z0.ctypes.data_as(C.POINTER(C.c_double)),
+                                          register_qubits, z0.ctypes.data_as(C.POINTER(C.c_double)),
                                           probs.ctypes.data_as(C.POINTER(C.c_double)), None, C.byref(st)))
     off = 0
     for i, c in enumerate(circuits):
@@ -56,12 +56,17 @@ def test_ansatz_batch_whole_circuits_in_shared_memory(be):
     assert st["n_sweeps"] == 64  # one pass per circuit
 
 
+def register_widths(be):
+    return (3, 4) if be.precision == "f64" else (4, 5)
+
+
 @pytest.mark.parametrize("local_qubits", [7, 9, 12])
-def test_multi_pass_circuits(be, local_qubits):
+@pytest.mark.parametrize("narrow", [False, True])
+def test_multi_pass_circuits(be, local_qubits, narrow):
     rng = SplitMix64(local_qubits)
     circuits = [ansatz_circuit(n, 3 + n % 4, rng) for n in (8, 11, 13, 16)]
     circuits += [random_circuit(n, 30 * n, 100 + n) for n in (9, 12, 15, 17)]
-    st = check_batch(be, circuits, local_qubits)
+    st = check_batch(be, circuits, local_qubits, register_widths(be)[0 if narrow else 1])
     assert st["n_sweeps"] > len(circuits)
 
 
@@ -69,7 +74,8 @@ def test_uneven_mix_default_tiles(be):
     rng = SplitMix64(5)
     circuits = [ansatz_circuit(n, d, rng) for n, d in ((18, 5), (3, 12), (14, 9), (16, 4), (2, 1), (15, 7))]
     circuits += [random_circuit(n, 200, n) for n in (4, 10, 17)]
-    check_batch(be, circuits)
+    for rq in register_widths(be):
+        check_batch(be, circuits, 0, rq)
 
 
 def test_generic_two_qubit_gates_any_order(be):
@@ -78,8 +84,9 @@ def test_generic_two_qubit_gates_any_order(be):
         c.h(q)
     for a, b in ((11, 0), (3, 9), (0, 11), (7, 2), (5, 6), (10, 1)):
         c.rzz(a, b, 0.3 + a).cx(a, b).swap(b, a).cz(a, b)
-    check_batch(be, [c], 7)
-    check_batch(be, [c], 0)
+    for rq in register_widths(be):
+        check_batch(be, [c], 7, rq)
+        check_batch(be, [c], 0, rq)
 
 
 def test_empty_circuits_and_probability_offsets(be):
@@ -104,7 +111,7 @@ def test_reusable_batch_object_and_autotune(be):
     pb = L.PackedBatch(circuits)
     lib = L.lib()
     h = C.c_void_p()
-    L.check(lib.qsvb_batch_create(be.ctx, pb.ptr(), pb.count, be.dtype, 0, C.byref(h)))
+    L.check(lib.qsvb_batch_create(be.ctx, pb.ptr(), pb.count, be.dtype, 0, 0, C.byref(h)))
     try:
         runs = []
         for _ in range(3):  # graph replays: same results every time
@@ -116,14 +123,15 @@ def test_reusable_batch_object_and_autotune(be):
             assert abs(runs[0][i] - oracle.expectation_z(oracle_probs(c), 1)) <= 1e-4
     finally:
         L.check(lib.qsvb_batch_free(be.ctx, h))
-    best = C.c_uint32()
+    best_l, best_r = C.c_uint32(), C.c_uint32()
     secs = np.zeros(8)
     count = C.c_size_t()
-    L.check(lib.qsvb_batch_autotune(be.ctx, pb.ptr(), pb.count, be.dtype, C.byref(best),
+    L.check(lib.qsvb_batch_autotune(be.ctx, pb.ptr(), pb.count, be.dtype, C.byref(best_l), C.byref(best_r),
                                     secs.ctypes.data_as(C.POINTER(C.c_double)), 8, C.byref(count)))
-    assert 9 <= best.value <= (13 if be.precision == "f64" else 14)
-    assert count.value == (13 if be.precision == "f64" else 14) - 9 + 1
-    assert np.all(secs[:count.value] > 0)
+    top = 13 if be.precision == "f64" else 14
+    assert top - 2 <= best_l.value <= top and best_r.value in register_widths(be)
+    assert count.value == 6 and np.all(secs[:6] > 0)
+    assert np.min(secs[:6]) == secs[2 * (best_l.value - (top - 2)) + register_widths(be).index(best_r.value)]
 
 
 def test_backend_execute_batch_matches_single_circuit_path(be):
@@ -141,10 +149,12 @@ def test_backend_execute_batch_matches_single_circuit_path(be):
 def test_batch_rejects_invalid_input(be):
     three = Circuit(4)
     three.push(DenseGate(3, np.eye(8, dtype=complex)), [0, 1, 2])
-    for circuits, lq in (([three], 0), ([Circuit(31)], 0), ([Circuit(4)], 15), ([Circuit(4)], 5)):
+    cases = (([three], 0, 0), ([Circuit(31)], 0, 0), ([Circuit(4)], 15, 0), ([Circuit(4)], 5, 0),
+             ([Circuit(4)], 0, 2), ([Circuit(4)], 0, 6))
+    for circuits, lq, rq in cases:
         pb = L.PackedBatch(circuits)
         z0 = np.zeros(1)
-        rc = L.lib().qsvb_execute_batch_ex(be.ctx, pb.ptr(), 1, be.dtype, lq, z0.ctypes.data_as(C.POINTER(C.c_double)),
-                                           None, None, None)
-        assert rc == L.QSVB_E_INVALID, (circuits[0].n_qubits(), lq)
+        rc = L.lib().qsvb_execute_batch_ex(be.ctx, pb.ptr(), 1, be.dtype, lq, rq,
+                                           z0.ctypes.data_as(C.POINTER(C.c_double)), None, None, None)
+        assert rc == L.QSVB_E_INVALID, (circuits[0].n_qubits(), lq, rq)
     assert L.lib().qsvb_execute_batch(be.ctx, None, 0, be.dtype, None, None, None, None) == L.QSVB_E_INVALID
