@@ -343,6 +343,320 @@ def run_reference(args):
     print(json.dumps(out), flush=True)
 
 
+# ------------------------------------------------------------------ the other configurations
+# Each prints one JSON line with the same keys as the headline (value, roofline, cpu_baseline, e2e,
+# clocks, gpu_launches) for its own workload; they are not the default bench line.
+
+def _events(stream):
+    import torch
+    return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+
+def device_seconds(be, stream, body, steps, warmup):
+    """Mean device seconds of ``body()`` (which queues work on the engine's stream)."""
+    for _ in range(warmup):
+        body()
+    be.synchronize()
+    e0, e1 = _events(stream)
+    e0.record(stream)
+    for _ in range(steps):
+        body()
+    e1.record(stream)
+    e1.synchronize()
+    return e0.elapsed_time(e1) * 1e-3 / steps
+
+
+def plan_roofline(plan, state, reps=1):
+    """Dominant sweep kind of a plan from its per-sweep device times: algorithmic GB/s vs peak."""
+    sweeps = plan.sweeps()
+    per = plan.profile(state, reps=reps)
+    by_kind = {}
+    for s, t in zip(sweeps, per):
+        d = by_kind.setdefault(s["kind"], {"time": 0.0, "bytes": 0.0, "launches": 0})
+        d["time"] += t
+        d["bytes"] += s["algorithmic_bytes"]
+        d["launches"] += 1
+    dom = max(by_kind, key=lambda k: by_kind[k]["time"])
+    d = by_kind[dom]
+    peak, kind = peaks()
+    achieved = d["bytes"] / d["time"] / 1e9
+    return {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+            "frac": round(achieved / peak, 4), "traffic": None, "peak_source": f"{kind} hbm_gbs",
+            "avg_launch_us": round(d["time"] / d["launches"] * 1e6, 1),
+            "algorithmic_bytes_per_launch": d["bytes"] / d["launches"],
+            "by_kind": {k: {"launches": v["launches"], "seconds": round(v["time"], 5),
+                            "GB/s": round(v["bytes"] / v["time"] / 1e9, 1) if v["time"] else None}
+                        for k, v in by_kind.items()}}
+
+
+def _line(metric, value, unit, args, dtype, config, **extra):
+    out = {"metric": metric, "value": value, "unit": unit, "n_gpus": 1, "steps": args.steps,
+           "warmup": args.warmup, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+           "dtype": dtype, "data": "synthetic (seeded)", "config": config}
+    out.update(extra)
+    print(json.dumps(out), flush=True)
+
+
+def run_config_ghz24(args):
+    """GHZ(24) complex128: H(0), CX(i, i+1); all 2^24 FP64 probabilities; p_0 = p_last = 1/2."""
+    import torch
+    from rustatevec_b200 import B200Backend, Plan, PLAN_AS_GIVEN, PLAN_LEARNED, ENGINE_AUTO, ENGINE_CUDA_CORE
+    from rustatevec_b200 import _lib as L
+    from rustatevec_b200.circuits import ghz_chain
+    from rustatevec_b200 import tuning
+    tuning.load()
+    n = 24
+    circ = ghz_chain(n)
+    be = B200Backend(0, precision="f64")
+    stream = torch.cuda.ExternalStream(be.stream())
+    st = be.alloc(n)
+    plans = {"unfused": Plan(be, circ, L.make_opts(PLAN_AS_GIVEN, 1, ENGINE_CUDA_CORE)),
+             "learned": Plan(be, circ, L.make_opts(PLAN_LEARNED, 6, ENGINE_AUTO))}
+    secs = {}
+    for name, p in plans.items():
+        secs[name] = device_seconds(be, stream, lambda: (be.init_basis(st, 0), p.run(st)), args.steps, args.warmup)
+    clocks = ClockSampler(0)
+    clocks.start()
+    t = device_seconds(be, stream, lambda: (be.init_basis(st, 0), plans["learned"].run(st)), args.steps, args.warmup)
+    clk = clocks.stop()
+    probs = be.probabilities(st, fp64=True)
+    ok = abs(probs[0] - 0.5) < 1e-12 and abs(probs[-1] - 0.5) < 1e-12 and abs(probs.sum() - 1) < 1e-12
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        be.init_basis(st, 0)
+        be.run(st, circ, L.make_opts(PLAN_LEARNED, 6, ENGINE_AUTO))
+        probs = be.probabilities(st, fp64=True)
+    e2e = (time.perf_counter() - t0) / args.steps
+    rl = plan_roofline(plans["learned"], st, reps=3)
+    cpu = None
+    if not args.no_cpu:
+        import oracle
+        t0 = time.perf_counter()
+        re, im = oracle.run(circ, oracle.CPU_PARALLEL, oracle.F64)
+        cpu = {"value": round(time.perf_counter() - t0, 4), "unit": "s", "cores": int(oracle.lib().orc_max_threads()),
+               "kind": "port", "sample": "whole circuit (24 gates) on the CpuBackend restatement, FP64"}
+    _line("GHZ(24) c128 circuit seconds (graph) + FP64 probabilities", round(t, 7), "s", args, "f64 (complex128)",
+          {"workload": "GHZ chain H(0), CX(i,i+1), 24 qubits, complex128", "plan_sweeps":
+           plans["learned"].stats()["n_sweeps"], "l2": "256 MiB state (> L2)"},
+          methods_seconds={k: round(v, 7) for k, v in secs.items()}, known_answer_ok=bool(ok),
+          roofline=rl, cpu_baseline=cpu, clocks=clk, gpu_launches=args.steps * (plans["learned"].stats()["n_sweeps"] + 1),
+          e2e={"value": round(e2e, 6), "unit": "s", "h2d_bytes_per_step": sum(32 * (1 << (2 * len(o.qubits))) // 2 for o in circ.ops()),
+               "d2h_bytes_per_step": 8 << n, "path": "run(host circuit) + probabilities(fp64) download"})
+    st.free()
+    be.close()
+
+
+def run_config_qft32(args):
+    """QFT(32) complex64 on an i.i.d. complex Gaussian state: learned vs greedy k=5 vs unfused, with
+    the fidelity of each against an FP64 (complex128) run of the same circuit on the same input."""
+    import torch
+    from rustatevec_b200 import (B200Backend, Plan, PLAN_AS_GIVEN, PLAN_GREEDY, PLAN_LEARNED, ENGINE_AUTO,
+                                 ENGINE_CUDA_CORE)
+    from rustatevec_b200 import _lib as L
+    from rustatevec_b200.circuits import qft
+    from rustatevec_b200 import tuning
+    tuning.load()
+    n = args.qubits if args.qubits != 30 else 32
+    seed = SEED
+    circ = qft(n)
+    be = B200Backend(0, precision="f32")
+    stream = torch.cuda.ExternalStream(be.stream())
+    st = be.alloc(n)
+    methods = {"unfused": L.make_opts(PLAN_AS_GIVEN, 1, ENGINE_CUDA_CORE),
+               "greedy_k5": L.make_opts(PLAN_GREEDY, 5, ENGINE_CUDA_CORE),
+               "learned": L.make_opts(PLAN_LEARNED, 6, ENGINE_AUTO)}
+    plans = {k: Plan(be, circ, o) for k, o in methods.items()}
+    secs = {}
+    for name, p in plans.items():
+        reps = 1 if name == "unfused" else args.steps
+        secs[name] = device_seconds(be, stream, lambda: (be.init_gaussian(st, seed), p.run(st)), reps,
+                                    1 if name == "unfused" else args.warmup)
+    # FP64 reference state, then the fidelity of every method's result against it
+    be64 = B200Backend(0, precision="f64")
+    s64 = be64.alloc(n)
+    be64.init_gaussian(s64, seed)
+    be64.run(s64, circ, L.make_opts(PLAN_GREEDY, 4, ENGINE_CUDA_CORE))
+    be64.synchronize()
+    fids = {}
+    for name, p in plans.items():
+        be.init_gaussian(st, seed)
+        p.run(st)
+        be.synchronize()
+        ip = be.inner_product(st, s64)
+        fids[name] = float(1.0 - abs(ip) ** 2 / be.norm_sqr(st))
+    s64.free()
+    be64.close()
+    clocks = ClockSampler(0)
+    clocks.start()
+    t = device_seconds(be, stream, lambda: (be.init_gaussian(st, seed), plans["learned"].run(st)), args.steps,
+                       args.warmup)
+    clk = clocks.stop()
+    rl = plan_roofline(plans["learned"], st)
+    t0 = time.perf_counter()
+    be.init_gaussian(st, seed)
+    be.run(st, circ, methods["learned"])
+    z = be.expectation_z(st, 1)
+    e2e = time.perf_counter() - t0
+    cpu = None
+    if not args.no_cpu:
+        cpu = cpu_baseline(circ, budget_s=args.cpu_budget)
+    _line(f"QFT({n}) c64 circuit seconds on a Gaussian state: learned vs greedy k=5 vs unfused", round(t, 6), "s",
+          args, "f32 state (complex64); plan composed in FP64",
+          {"workload": f"QFT({n}) complex64, input i.i.d. complex Gaussian (seed {seed}), normalised in FP64",
+           "plan_sweeps": {k: p.stats()["n_sweeps"] for k, p in plans.items()}, "l2": "32 GiB state (> L2)"},
+          methods_seconds={k: round(v, 5) for k, v in secs.items()}, infidelity_vs_fp64=fids,
+          speedup_learned_vs_greedy_k5=round(secs["greedy_k5"] / t, 3),
+          speedup_learned_vs_unfused=round(secs["unfused"] / t, 3),
+          roofline=rl, cpu_baseline=cpu, clocks=clk, gpu_launches=args.steps * (plans["learned"].stats()["n_sweeps"] + 3),
+          e2e={"value": round(e2e, 6), "unit": "s", "h2d_bytes_per_step": sum(16 << (2 * len(o.qubits)) for o in circ.ops()),
+               "d2h_bytes_per_step": 8, "path": "init_gaussian + run(host circuit) + expectation_z(mask=1)",
+               "z0": z})
+    st.free()
+    be.close()
+
+
+def run_config_qaoa33(args):
+    """QAOA MaxCut 33 qubits complex128 (137 GB state), p=4: learned vs greedy, FP64 invariants."""
+    import torch
+    from rustatevec_b200 import B200Backend, Plan, PLAN_GREEDY, PLAN_LEARNED, ENGINE_AUTO, ENGINE_CUDA_CORE
+    from rustatevec_b200 import _lib as L
+    from rustatevec_b200.circuits import qaoa_maxcut
+    from rustatevec_b200 import tuning
+    tuning.load()
+    n = args.qubits if args.qubits != 30 else 33
+    circ = qaoa_maxcut(n, 4, SEED)
+    be = B200Backend(0, precision="f64")
+    stream = torch.cuda.ExternalStream(be.stream())
+    st = be.alloc(n)
+    methods = {"greedy_k4": L.make_opts(PLAN_GREEDY, 4, ENGINE_CUDA_CORE),
+               "learned": L.make_opts(PLAN_LEARNED, 6, ENGINE_AUTO)}
+    plans = {k: Plan(be, circ, o) for k, o in methods.items()}
+    secs, checks = {}, {}
+    masks = [1, 3, 1 << (n - 1), (1 << n) - 1, 0x5555555555555555 & ((1 << n) - 1)]
+    for name, p in plans.items():
+        secs[name] = device_seconds(be, stream, lambda: (be.init_basis(st, 0), p.run(st)), 1, 1)
+        checks[name] = {"norm": be.norm_sqr(st), "z": [be.expectation_z(st, m) for m in masks],
+                        "amp": [be.amplitude(st, i) for i in (0, 12345, (1 << n) - 1)]}
+    g, l = checks["greedy_k4"], checks["learned"]
+    diff = max([abs(a - b) for a, b in zip(g["z"], l["z"])] + [abs(a - b) for a, b in zip(g["amp"], l["amp"])])
+    clocks = ClockSampler(0)
+    clocks.start()
+    t = device_seconds(be, stream, lambda: (be.init_basis(st, 0), plans["learned"].run(st)), max(1, args.steps // 2), 1)
+    clk = clocks.stop()
+    rl = plan_roofline(plans["learned"], st)
+    _line(f"QAOA MaxCut {n}q c128 p=4 circuit seconds: learned vs greedy", round(t, 5), "s", args,
+          "f64 (complex128) throughout",
+          {"workload": f"QAOA MaxCut {n} qubits, p=4, 3-regular graph (odd n: node 0 degree 4), seed {SEED}",
+           "plan_sweeps": {k: p.stats()["n_sweeps"] for k, p in plans.items()},
+           "plan_by_kind": {k: p.stats()["by_kind"] for k, p in plans.items()}, "state_GB": 16 * 2 ** n / 1e9},
+          methods_seconds={k: round(v, 5) for k, v in secs.items()},
+          speedup_learned_vs_greedy=round(secs["greedy_k4"] / t, 3),
+          fp64_invariants={"norm_minus_1": {k: v["norm"] - 1.0 for k, v in checks.items()},
+                           "max_abs_diff_learned_vs_greedy": diff, "z_masks": masks, "z_learned": l["z"]},
+          roofline=rl, cpu_baseline={"value": None, "unit": "s", "cores": None, "kind": "port",
+                                     "sample": "not run (RAM): the 137 GB state does not fit the host"},
+          clocks=clk, gpu_launches=max(1, args.steps // 2) * (plans["learned"].stats()["n_sweeps"] + 1),
+          e2e={"value": None, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0,
+               "note": "device-resident workload; see value"})
+    st.free()
+    be.close()
+
+
+def run_config_batched(args):
+    """4096 uneven ansatz circuits (n ~ U{10..20}, depth ~ U{4..12}) in one persistent kernel from a
+    captured graph, complex64 and complex128, autotuned tiles; <Z_0> + FP64 probabilities per circuit."""
+    import ctypes as C
+    from rustatevec_b200 import B200Backend
+    from rustatevec_b200 import _lib as L
+    from rustatevec_b200.circuits import ansatz_batch
+    from rustatevec_b200.shard import lpt_partition, circuit_cost
+    world, rank, local = dist_setup()
+    count = args.circuits
+    circuits = ansatz_batch(count, SEED)
+    parts = lpt_partition([circuit_cost(c) for c in circuits], world)
+    mine = [circuits[i] for i in parts[rank]]
+    pb = L.PackedBatch(mine)
+    res = {}
+    clk = None
+    for prec in ("f32", "f64"):
+        be = B200Backend(local, precision=prec)
+        best_l, best_r = C.c_uint32(), C.c_uint32()
+        secs = np.zeros(6)
+        cnt = C.c_size_t()
+        L.check(L.lib().qsvb_batch_autotune(be.ctx, pb.ptr(), pb.count, be.dtype, C.byref(best_l), C.byref(best_r),
+                                            secs.ctypes.data_as(L._dp), 6, C.byref(cnt)))
+        h = C.c_void_p()
+        L.check(L.lib().qsvb_batch_create(be.ctx, pb.ptr(), pb.count, be.dtype, best_l.value, best_r.value,
+                                          C.byref(h)))
+        z0 = np.zeros(pb.count)
+        stt = L.PlanStats()
+        for _ in range(args.warmup):
+            L.check(L.lib().qsvb_batch_run(be.ctx, h, None, None, None, C.byref(stt)))
+        if prec == "f32":
+            clocks = ClockSampler(local)
+            clocks.start()
+        barrier(world)
+        ts = []
+        for _ in range(args.steps):
+            L.check(L.lib().qsvb_batch_run(be.ctx, h, None, None, None, C.byref(stt)))
+            ts.append(stt.predicted_seconds)
+        if prec == "f32":
+            clk = clocks.stop()
+        t = allreduce_max(float(np.mean(ts)), world)
+        # end to end: host circuits -> plan + graph -> run -> <Z_0> and all FP64 probabilities on the host
+        t0 = time.perf_counter()
+        z0, probs, st2 = be.execute_batch(mine, probabilities=True, local_qubits=best_l.value,
+                                          register_qubits=best_r.value)
+        e2e = allreduce_max(time.perf_counter() - t0, world)
+        d = stt.to_dict()
+        L.check(L.lib().qsvb_batch_free(be.ctx, h))
+        res[prec] = {"seconds": t, "tile": [best_l.value, best_r.value],
+                     "autotune_seconds": [round(x, 5) for x in secs[:cnt.value]],
+                     "passes": d["n_sweeps"], "phases": d["by_kind"].get("1q"),
+                     "algorithmic_GB": d["algorithmic_bytes"] / 1e9, "flops": d["flops"], "e2e": e2e,
+                     "probs_bytes": int(sum(p.nbytes for p in probs)), "z0_sample": [float(x) for x in z0[:3]]}
+        be.close()
+    if rank != 0:
+        return
+    peak, kind = peaks()
+    r32 = res["f32"]
+    ach = r32["algorithmic_GB"] * world / r32["seconds"]
+    cpu = None
+    if not args.no_cpu:
+        import oracle
+        rng = np.random.default_rng(0)
+        pick = rng.permutation(count)
+        t0 = time.perf_counter()
+        done_cost = 0.0
+        for i in pick:
+            c = circuits[int(i)]
+            re, im = oracle.run(c, oracle.CPU_PARALLEL, oracle.F32)
+            oracle.expectation_z((re.astype(np.float64) ** 2 + im.astype(np.float64) ** 2), 1)
+            done_cost += circuit_cost(c)
+            if time.perf_counter() - t0 > args.cpu_budget:
+                break
+        dt = time.perf_counter() - t0
+        total = sum(circuit_cost(c) for c in circuits)
+        cpu = {"value": round(dt * total / done_cost, 3), "unit": "s", "cores": int(oracle.lib().orc_max_threads()),
+               "kind": "port", "sample": f"random circuits of the batch on the CpuBackend restatement (f32) for "
+                                         f"{dt:.1f} s, extrapolated by sum(2^n * gates)"}
+    _line("batched ansatz: 4096 circuits, seconds per batch (c64; c128 beside)", round(r32["seconds"] / 1.0, 6), "s",
+          args, "f32 state (complex64); c128 run beside",
+          {"workload": f"{count} ansatz circuits n~U{{10..20}} depth~U{{4..12}} RY.RZ + CX ladder, seed {SEED}",
+           "parallelism": f"circuits sharded over {world} GPU(s) by cost (LPT), no collective" if world > 1 else
+           "single GPU", "l2": "states and probabilities (6.2 GB) exceed L2"},
+          n_gpus=world, by_precision=res, circuits_per_second=round(count / r32["seconds"], 1),
+          roofline={"bound": "fp32 (CUDA-core register tiles)", "achieved": round(ach, 1), "peak": peak,
+                    "unit": "GB/s", "frac": round(ach / peak, 4), "traffic": None,
+                    "achieved_tflops": round(r32["flops"] * world / r32["seconds"] / 1e12, 2),
+                    "note": "algorithmic HBM bytes (multi-pass tiles + probabilities) / device time; the kernel "
+                            "works out of shared memory and registers, so the HBM fraction is low by design"},
+          cpu_baseline=cpu, clocks=clk, gpu_launches=2 * args.steps,
+          e2e={"value": round(r32["e2e"], 4), "unit": "s", "h2d_bytes_per_step": None,
+               "d2h_bytes_per_step": r32["probs_bytes"] + 8 * count,
+               "path": "execute_batch(host circuits): plan + upload + graph run + <Z_0> and probabilities to host"})
+
+
 KERNEL_CASES = {
     # name: (precision, builder(n) -> circuit with one sweep of that kind, engine)
     "1q_low": ("f32", lambda n: [("h", [1])]),
@@ -420,9 +734,22 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--ref-budget", type=float, default=6.0)
+    ap.add_argument("--config", default="brickwork30", choices=["brickwork30", "ghz24", "qft32", "qaoa33", "batched"],
+                    help="workload (the default is the headline bench line)")
+    ap.add_argument("--circuits", type=int, default=4096, help="batched config: number of circuits")
     args = ap.parse_args()
     if args.kernel_case:
         run_kernel_case(args)
+    elif args.impl == "reference" and args.config == "brickwork30":
+        run_reference(args)
+    elif args.config == "ghz24":
+        run_config_ghz24(args)
+    elif args.config == "qft32":
+        run_config_qft32(args)
+    elif args.config == "qaoa33":
+        run_config_qaoa33(args)
+    elif args.config == "batched":
+        run_config_batched(args)
     elif args.impl == "reference":
         run_reference(args)
     else:
