@@ -202,6 +202,7 @@ def run_gpu(args):
         "window_k4_cuda": L.make_opts(PLAN_WINDOW, 4, ENGINE_CUDA_CORE),
         "learned_cuda": L.make_opts(PLAN_LEARNED, 6, ENGINE_CUDA_CORE),
         "greedy_k6_tc": L.make_opts(PLAN_GREEDY, 6, ENGINE_TENSOR_CORE),
+        "tile": L.make_opts(L.PLAN_TILE, 4, ENGINE_AUTO),
         "learned_tc": L.make_opts(PLAN_LEARNED, 6, ENGINE_AUTO),
     }
     headline = "learned_tc"
@@ -411,6 +412,7 @@ def run_config_ghz24(args):
     stream = torch.cuda.ExternalStream(be.stream())
     st = be.alloc(n)
     plans = {"unfused": Plan(be, circ, L.make_opts(PLAN_AS_GIVEN, 1, ENGINE_CUDA_CORE)),
+             "tile": Plan(be, circ, L.make_opts(L.PLAN_TILE, 4, ENGINE_AUTO)),
              "learned": Plan(be, circ, L.make_opts(PLAN_LEARNED, 6, ENGINE_AUTO))}
     secs = {}
     for name, p in plans.items():
@@ -464,6 +466,7 @@ def run_config_qft32(args):
     st = be.alloc(n)
     methods = {"unfused": L.make_opts(PLAN_AS_GIVEN, 1, ENGINE_CUDA_CORE),
                "greedy_k5": L.make_opts(PLAN_GREEDY, 5, ENGINE_CUDA_CORE),
+               "tile": L.make_opts(L.PLAN_TILE, 4, ENGINE_AUTO),
                "learned": L.make_opts(PLAN_LEARNED, 6, ENGINE_AUTO)}
     plans = {k: Plan(be, circ, o) for k, o in methods.items()}
     secs = {}
@@ -529,6 +532,7 @@ def run_config_qaoa33(args):
     stream = torch.cuda.ExternalStream(be.stream())
     st = be.alloc(n)
     methods = {"greedy_k4": L.make_opts(PLAN_GREEDY, 4, ENGINE_CUDA_CORE),
+               "tile": L.make_opts(L.PLAN_TILE, 4, ENGINE_AUTO),
                "learned": L.make_opts(PLAN_LEARNED, 6, ENGINE_AUTO)}
     plans = {k: Plan(be, circ, o) for k, o in methods.items()}
     secs, checks = {}, {}
@@ -670,6 +674,8 @@ KERNEL_CASES = {
     "tc6": ("f32", lambda n: [("u6", list(range(6)))]),
     "tc6_high": ("f32", lambda n: [("u6", list(range(n - 6, n)))]),
     "phase15": ("f32", lambda n: [("cz", [i, i + 1]) for i in range(0, n - 1, 2)]),
+    "tile_h_all": ("f32", lambda n: [("h", [q]) for q in range(13)]),
+    "tile_h_all_c128": ("f64", lambda n: [("h", [q]) for q in range(12)]),
     "1q_low_c128": ("f64", lambda n: [("h", [1])]),
     "dense4_c128": ("f64", lambda n: [("u4", [0, 1, 2, 3])]),
 }
@@ -697,6 +703,8 @@ def run_kernel_case(args):
             c.push(G.LIBRARY[name](), qs)
     engine = ENGINE_TENSOR_CORE if args.kernel_case.startswith("tc") else ENGINE_CUDA_CORE
     planner = PLAN_LEARNED if args.kernel_case.startswith("phase") else PLAN_AS_GIVEN
+    if args.kernel_case.startswith("tile"):
+        planner = L.PLAN_TILE
     be = B200Backend(0, precision=prec)
     st = be.alloc(n)
     be.init_basis(st, 0)

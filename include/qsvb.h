@@ -64,7 +64,12 @@ typedef enum qsvb_planner {
   QSVB_PLAN_AS_GIVEN = 0, /* one sweep per gate, in order (the trait's default execute loop) */
   QSVB_PLAN_GREEDY = 1,   /* qsv fuse semantics (fusion.rs:39-77), composition in FP64 */
   QSVB_PLAN_WINDOW = 2,   /* commutation-aware windows: gates on disjoint qubits reorder */
-  QSVB_PLAN_LEARNED = 3   /* cost-model planner (MLP cost model; greedy fallback) */
+  QSVB_PLAN_LEARNED = 3,  /* cost-model planner (MLP cost model; greedy fallback); also weighs
+                             tile passes against fused sweeps */
+  QSVB_PLAN_TILE = 4      /* tile passes: the 1- and 2-qubit gates acting inside a set of up to
+                             13 qubits (12 for complex128) that commute past the gates left for
+                             later, applied on shared-memory tiles in one read and one write of
+                             the state; diagonal runs become phase sweeps, wider gates fused sweeps */
 } qsvb_planner;
 
 typedef enum qsvb_engine {

@@ -22,11 +22,11 @@ QSVB_E_UNSUPPORTED = -4
 QSVB_E_TIMEOUT = -5
 
 C64, C128 = 0, 1
-PLAN_AS_GIVEN, PLAN_GREEDY, PLAN_WINDOW, PLAN_LEARNED = 0, 1, 2, 3
+PLAN_AS_GIVEN, PLAN_GREEDY, PLAN_WINDOW, PLAN_LEARNED, PLAN_TILE = 0, 1, 2, 3, 4
 ENGINE_AUTO, ENGINE_CUDA_CORE, ENGINE_TENSOR_CORE = 0, 1, 2
 MAX_GATE_QUBITS = 6
 
-SWEEP_KINDS = ("1q", "ctrl1q", "diag", "phase", "dense", "dense_tc", "swap", "other")
+SWEEP_KINDS = ("1q", "ctrl1q", "diag", "phase", "dense", "dense_tc", "tile", "other")
 
 
 class QsvbError(RuntimeError):

@@ -34,7 +34,9 @@
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
+#include <cstring>
 #include <memory>
+#include <mutex>
 #include <numeric>
 #include <type_traits>
 #include <string>
@@ -336,13 +338,13 @@ __device__ __forceinline__ void apply_instr(const Instr& in, Regs<R, RB>& v, con
   }
 }
 
-template <class R, int RB, int W, int NT>
-__global__ void __launch_bounds__(NT, 1)
+template <class R, int RB, int W, int NT, int MINB = 1>
+__global__ void __launch_bounds__(NT, MINB)
     k_batch(const Item* __restrict__ items, uint32_t nitems, const PassDev* __restrict__ passes,
             const PhaseDev* __restrict__ phases, const Instr* __restrict__ prog, const R* __restrict__ coef,
             R* __restrict__ sre, R* __restrict__ sim, double* __restrict__ probs, double* __restrict__ zpart,
             uint32_t* __restrict__ done, uint32_t* __restrict__ queue, int* __restrict__ err, uint32_t lbits,
-            long long* __restrict__ prof) {
+            long long* __restrict__ prof, uint32_t fixed) {
   extern __shared__ __align__(16) uint8_t smem_raw[];
   R* xr = reinterpret_cast<R*>(smem_raw);
   R* xi = xr + (size_t(1) << lbits);  // every pass has nlocal <= lbits
@@ -363,12 +365,14 @@ __global__ void __launch_bounds__(NT, 1)
   }
   long long t_wait = 0, t_fill = 0, t_gates = 0, t_out = 0, n_items = 0, t_mark = prof ? clock64() : 0;
   uint32_t staged_pass = ~0u;
+  // fixed != 0: one pass (passes[0]) over one state, tile i handled by block i mod grid, no queue
+  uint32_t iter = 0;
   while (true) {
-    if (tid == 0) s_item = atomicAdd(queue, 1u);
+    if (!fixed && tid == 0) s_item = atomicAdd(queue, 1u);
     __syncthreads();
-    const uint32_t it = s_item;
+    const uint32_t it = fixed ? blockIdx.x + (iter++) * gridDim.x : s_item;
     if (it >= nitems) break;
-    const Item item = items[it];
+    const Item item = fixed ? Item{0u, it} : items[it];
     const PassDev& P = passes[item.pass];
     const uint32_t L = P.nlocal, T = 1u << L;
     if (tid == 0) {
@@ -518,7 +522,7 @@ __global__ void __launch_bounds__(NT, 1)
       }
     }
     __syncthreads();
-    if (tid == 0) {
+    if (tid == 0 && !fixed) {
       __threadfence();
       cuda::atomic_ref<uint32_t, cuda::thread_scope_device> d(done[item.pass]);
       d.fetch_add(1u, cuda::memory_order_release);
@@ -639,21 +643,26 @@ void emit_phases(BatchPlan& bp, const std::vector<LGate>& G, uint32_t nlocal) {
   while (true) {
     while (first < G.size() && done[first]) ++first;
     if (first == G.size()) break;
-    uint32_t Rm = 0, blocked = 0;
+    // blocked: positions of skipped non-diagonal gates; dblocked: of skipped diagonal gates (a
+    // diagonal gate may still pass those)
+    uint32_t Rm = 0, blocked = 0, dblocked = 0;
     taken.clear();
     for (size_t i = first; i < G.size(); ++i) {
       if (done[i]) continue;
       const LGate& g = G[i];
       const uint32_t m = (1u << g.p[0]) | (g.kind >= LK_CX ? (1u << g.p[1]) : 0u);
-      if ((m & blocked) == 0 && uint32_t(__builtin_popcount(Rm | m)) <= rb) {
+      const bool diag = g.kind == LK_D1 || g.kind == LK_D2;
+      if ((m & blocked) == 0 && (diag || (m & dblocked) == 0) && uint32_t(__builtin_popcount(Rm | m)) <= rb) {
         Rm |= m;
         done[i] = 1;
         taken.push_back(i);
+      } else if (diag) {
+        dblocked |= m;
       } else {
         blocked |= m;
       }
       const bool full = uint32_t(__builtin_popcount(Rm)) == rb;
-      if (blocked == all || (full && (Rm & ~blocked) == 0)) break;
+      if ((blocked | dblocked) == all || (full && (Rm & ~(blocked | dblocked)) == 0)) break;
     }
     for (uint32_t p = 0; p < nlocal && uint32_t(__builtin_popcount(Rm)) < rb; ++p) Rm |= 1u << p;
     // register bits: the phase's local positions in ascending order
@@ -813,18 +822,21 @@ std::unique_ptr<BatchPlan> build_batch(const qsvb_circuit* circuits, size_t ncir
       P.state_off = state_off;
       P.prob_off = bp->prob_off.back();
       std::vector<LGate> G;
-      uint64_t blocked = 0;
+      uint64_t blocked = 0, dblocked = 0;  // qubits of skipped non-diagonal / diagonal gates
       for (size_t i = first_open; i < gates.size(); ++i) {
         if (done[i]) continue;
         uint64_t m = 0;
         for (uint32_t j = 0; j < gates[i].m; ++j) m |= 1ull << gates[i].q[j];
-        if ((m & ~S) == 0 && (m & blocked) == 0) {
+        const bool diag = kinds[i] == LK_D1 || kinds[i] == LK_D2;
+        if ((m & ~S) == 0 && (m & blocked) == 0 && (diag || (m & dblocked) == 0)) {
           done[i] = 1;
           const LGate g{kinds[i],
                         {uint32_t(pos[gates[i].q[0]]), gates[i].m == 2 ? uint32_t(pos[gates[i].q[1]]) : 0u},
                         &gates[i]};
           G.push_back(g);
           flops += amps * (g.kind == LK_1Q ? 16.0 : g.kind == LK_2Q ? 32.0 : g.kind == LK_CX ? 0.0 : 6.0);
+        } else if (diag) {
+          dblocked |= m;
         } else {
           blocked |= m;
         }
@@ -941,7 +953,7 @@ template <class R, int RB, int W, int NT> void launch(qsvb_batch* b, qsvb_ctx* c
       static_cast<const Item*>(b->d_items), uint32_t(bp.items.size()), static_cast<const PassDev*>(b->d_passes),
       static_cast<const PhaseDev*>(b->d_phases), static_cast<const Instr*>(b->d_prog),
       static_cast<const R*>(b->d_coef), static_cast<R*>(b->d_sre), static_cast<R*>(b->d_sim), b->d_probs,
-      b->d_zpart, b->d_done, b->d_queue, c->d_err, bp.local_bits, b->d_prof);
+      b->d_zpart, b->d_done, b->d_queue, c->d_err, bp.local_bits, b->d_prof, 0u);
 }
 
 // The kernel variants: register bits (a group of 2^RB amplitudes per thread) and block size. The
@@ -1133,3 +1145,136 @@ void run_batch(qsvb_ctx* c, const qsvb_circuit* circuits, size_t n_circuits, int
 }
 
 void free_batch(qsvb_batch* b) { delete b; }
+
+// ----------------------------------------------------------------------------- tile sweeps
+// A tile sweep runs one pass of the batched kernel over one state (any n up to 34): the gates of a
+// plan segment that act inside the local set S, applied tile by tile in shared memory, each tile
+// read and written once. Blocks take tiles i, i + grid, ... (no queue, no dependencies).
+namespace qsvb {
+
+uint32_t tile_local_bits(int dtype, uint32_t n) {
+  const uint32_t lmax = batch_max_local_bits(dtype) - 1;  // half the shared memory: two blocks per SM
+  if (n >= lmax + 8) return lmax;  // at least 256 tiles to spread over the SMs
+  if (n >= 15) return n - 8;
+  return 0;
+}
+
+namespace {
+uint32_t tile_reg_bits(int dtype) { return dtype == QSVB_C128 ? 3u : 4u; }
+size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
+constexpr size_t kTileSmemMax = (size_t(2) * 4 << 14) + kStageBytes;  // equal for both precisions
+
+template <class R, int RB, int NT, int MINB>
+void launch_tile_variant(const LaunchEnv& e, R* re, R* im, const Sweep& s, const uint8_t* base) {
+  auto fn = k_batch<R, RB, sizeof(R) == 8 ? 4 : 5, NT, MINB>;
+  static std::once_flag once;
+  std::call_once(once, [&] {
+    QSVB_CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kTileSmemMax)));
+    QSVB_CK(cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 int(cudaSharedmemCarveoutMaxShared)));
+  });
+  const size_t smem = ((size_t(2) * sizeof(R)) << s.tile_lbits) + kStageBytes;
+  int occ = 0;
+  QSVB_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, NT, smem));
+  QSVB_REQUIRE(occ >= 1, "tile kernel does not fit on an SM");
+  const uint32_t grid = uint32_t(std::min<uint64_t>(s.tile_ntiles, uint64_t(e.num_sms) * uint64_t(occ)));
+  fn<<<grid, NT, smem, e.stream>>>(nullptr, s.tile_ntiles, reinterpret_cast<const PassDev*>(base),
+                                   reinterpret_cast<const PhaseDev*>(base + s.tile_off_phase),
+                                   reinterpret_cast<const Instr*>(base + s.tile_off_prog),
+                                   reinterpret_cast<const R*>(base + s.tile_off_coef), re, im, nullptr, nullptr,
+                                   nullptr, nullptr, e.err_flag, s.tile_lbits, nullptr, 1u);
+  QSVB_CK(cudaGetLastError());
+}
+}  // namespace
+
+void tile_prepare(Sweep& s, uint32_t n, int dtype) {
+  const uint64_t S = s.tile_mask;
+  BatchPlan bp;
+  bp.dtype = dtype;
+  bp.rb = tile_reg_bits(dtype);
+  bp.swz_w = dtype == QSVB_C128 ? 4u : 5u;
+  PassDev P{};
+  P.nlocal = uint32_t(__builtin_popcountll(S));
+  QSVB_REQUIRE((S & 31u) == 31u && P.nlocal >= 7 && P.nlocal <= batch_max_local_bits(dtype) - 1 && n <= QSVB_MAX_QUBITS &&
+                   (n >= 64 || (S >> n) == 0),
+               "tile sweep: the local set must hold qubits 0..4 and 7..13 (12 for complex128) qubits of the state");
+  bp.local_bits = P.nlocal;
+  int pos[64];
+  uint32_t nl = 0, nn = 0;
+  for (uint32_t b = 0; b < n; ++b) {
+    if ((S >> b) & 1u) {
+      pos[b] = int(nl);
+      P.local[nl++] = uint8_t(b);
+    } else {
+      pos[b] = -1;
+      P.nonlocal[nn++] = uint8_t(b);
+    }
+  }
+  P.nnon = nn;
+  P.ntiles = 1u << nn;
+  P.prev = ~0u;
+  const double dim = std::ldexp(1.0, int(n));
+  std::vector<HostGate> hg(s.tile_gates.size());
+  std::vector<LGate> G;
+  double flops = 0;
+  for (size_t i = 0; i < s.tile_gates.size(); ++i) {
+    const Gate& g = s.tile_gates[i];
+    QSVB_REQUIRE(g.m >= 1 && g.m <= 2, "tile sweeps take 1- and 2-qubit gates");
+    hg[i].m = g.m;
+    hg[i].q[0] = g.q[0];
+    hg[i].q[1] = g.m == 2 ? g.q[1] : 0u;
+    hg[i].a = g.a;
+    for (uint32_t j = 0; j < g.m; ++j) QSVB_REQUIRE(g.q[j] < n && pos[g.q[j]] >= 0, "tile gate outside the local set");
+    const uint32_t kind = gate_kind(hg[i]);
+    G.push_back(LGate{kind, {uint32_t(pos[g.q[0]]), g.m == 2 ? uint32_t(pos[g.q[1]]) : 0u}, &hg[i]});
+    flops += dim * (kind == LK_1Q ? 16.0 : kind == LK_2Q ? 32.0 : kind == LK_CX ? 0.0 : 6.0);
+  }
+  emit_phases(bp, G, P.nlocal);
+  P.prog_len = uint32_t(bp.prog.size());
+  P.nphase = uint32_t(bp.phases.size());
+  P.ncoef = uint32_t(bp.coef.size() / 2);
+  const size_t rsz = dtype == QSVB_C128 ? 8 : 4;
+  {
+    const size_t co = (P.prog_len * sizeof(Instr) + P.nphase * sizeof(PhaseDev) + 7) & ~size_t(7);
+    P.staged = co + size_t(P.ncoef) * 2 * rsz <= kStageBytes ? 1u : 0u;
+  }
+  const size_t off_phase = align16(sizeof(PassDev));
+  const size_t off_prog = align16(off_phase + bp.phases.size() * sizeof(PhaseDev));
+  const size_t off_coef = align16(off_prog + bp.prog.size() * sizeof(Instr));
+  const size_t total = off_coef + bp.coef.size() * rsz;
+  s.tile_blob.assign(total, 0);
+  std::memcpy(s.tile_blob.data(), &P, sizeof(P));
+  if (!bp.phases.empty()) std::memcpy(s.tile_blob.data() + off_phase, bp.phases.data(), bp.phases.size() * sizeof(PhaseDev));
+  if (!bp.prog.empty()) std::memcpy(s.tile_blob.data() + off_prog, bp.prog.data(), bp.prog.size() * sizeof(Instr));
+  for (size_t i = 0; i < bp.coef.size(); ++i) {
+    if (rsz == 8) {
+      std::memcpy(s.tile_blob.data() + off_coef + 8 * i, &bp.coef[i], 8);
+    } else {
+      const float f = float(bp.coef[i]);
+      std::memcpy(s.tile_blob.data() + off_coef + 4 * i, &f, 4);
+    }
+  }
+  s.tile_rb = bp.rb;
+  s.tile_lbits = P.nlocal;
+  s.tile_ntiles = P.ntiles;
+  s.tile_off_phase = uint32_t(off_phase);
+  s.tile_off_prog = uint32_t(off_prog);
+  s.tile_off_coef = uint32_t(off_coef);
+  s.tile_flops = flops;
+  s.n_gates = s.tile_gates.size();
+}
+
+template <class R>
+void launch_tile(const LaunchEnv& e, R* re, R* im, uint32_t n, const Sweep& s, const void* dev_blob) {
+  QSVB_REQUIRE(dev_blob != nullptr && !s.tile_blob.empty(), "tile sweep without a program");
+  QSVB_REQUIRE(n >= s.tile_lbits, "tile sweep larger than the state");
+  const uint8_t* base = static_cast<const uint8_t*>(dev_blob);
+  // two blocks per SM (one streams its tile while the other computes): <= 128 registers a thread
+  if constexpr (sizeof(R) == 8) launch_tile_variant<double, 3, 256, 2>(e, re, im, s, base);
+  else launch_tile_variant<float, 4, 256, 2>(e, re, im, s, base);
+}
+
+template void launch_tile<float>(const LaunchEnv&, float*, float*, uint32_t, const Sweep&, const void*);
+template void launch_tile<double>(const LaunchEnv&, double*, double*, uint32_t, const Sweep&, const void*);
+
+}  // namespace qsvb

@@ -18,6 +18,8 @@ constexpr double kFp32FmaFlops = 40.0e12;   // CUDA-core complex GEMM, achieved
 constexpr double kFp64FmaFlops = 25.0e12;
 constexpr double kTcFlops = 1.2e15;         // bf16 tcgen05, achieved
 constexpr double kLaunchSeconds = 2.5e-6;
+constexpr double kTileFp32Flops = 22.0e12;  // tile-sweep gate arithmetic, achieved (register tiles)
+constexpr double kTileFp64Flops = 12.0e12;
 
 int lowest_bit(const Sweep& s) {
   uint32_t lo = 64;
@@ -81,6 +83,11 @@ double analytic_sweep_seconds(const Sweep& s, uint32_t n, int dtype) {
     comp = 8.0 * std::ldexp(1.0, int(s.m)) * dim / (dtype == QSVB_C128 ? kFp64FmaFlops : kFp32FmaFlops);
   if (s.kind == SK_DENSE_TC) comp = 3.0 * 8.0 * std::ldexp(1.0, int(s.m)) * dim / kTcFlops;
   if (s.kind == SK_PHASE) comp = double(s.terms.size()) * 4.0 * dim / 30.0e12 + 40.0 * dim / kFp64FmaFlops;
+  if (s.kind == SK_TILE) {
+    // each block loads, updates and stores its tile in turn: memory and arithmetic add up
+    const double rate = dtype == QSVB_C128 ? kTileFp64Flops : kTileFp32Flops;
+    return mem + s.tile_flops / rate + kLaunchSeconds;
+  }
   return std::max(mem, comp) + kLaunchSeconds;
 }
 
@@ -112,7 +119,7 @@ float mlp_forward_host(const MlpModel& m, const float* feat) {
 
 double predict_sweep_seconds(const Sweep& s, uint32_t n, int dtype) {
   const MlpModel& m = g_model;
-  if (m.hidden > 0) {
+  if (m.hidden > 0 && s.kind != SK_TILE) {  // the model has not been trained on tile sweeps
     float f[kNumFeatures];
     sweep_features(s, n, dtype, f);
     return std::exp2(double(mlp_forward_host(m, f)));

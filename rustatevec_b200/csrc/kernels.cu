@@ -970,6 +970,7 @@ size_t sweep_matrix_bytes(const Sweep& s, int dtype) {
     case SK_DENSE: return 2 * r * (size_t(1) << (2 * s.m));
     case SK_DENSE_TC: return tc_matrix_bytes(s);
     case SK_PHASE: return s.terms.size() * sizeof(PhaseTermDev);
+    case SK_TILE: return s.tile_blob.size();
     default: return 0;
   }
 }
@@ -989,6 +990,8 @@ void pack_sweep_matrix(const Sweep& s, int dtype, void* dst) {
           static_cast<float*>(dst)[o + 1] = float(v.imag());
         }
       }
+  } else if (s.kind == SK_TILE) {
+    std::memcpy(dst, s.tile_blob.data(), s.tile_blob.size());
   } else if (s.kind == SK_DENSE_TC) {
     tc_pack_matrix(s, dst);
   } else if (s.kind == SK_PHASE) {
@@ -1015,6 +1018,7 @@ void launch_sweep(const LaunchEnv& env, R* re, R* im, uint32_t n, const Sweep& s
         break;
       }
       throw Error(QSVB_E_UNSUPPORTED, "tensor-core sweeps need a complex64 state");
+    case SK_TILE: launch_tile<R>(env, re, im, n, s, dev_mat); break;
     case SK_NONE: break;
     default: throw Error(QSVB_E_UNSUPPORTED, "unknown sweep kind");
   }

@@ -305,36 +305,139 @@ Sweep classify_gate(const Gate& g) {
 }
 
 namespace {
+enum TileMode { TILE_NO = 0, TILE_ALWAYS = 1, TILE_CHOOSE = 2 };
 std::vector<Sweep> plan_with(const std::vector<Gate>& in, uint32_t n, const qsvb_plan_opts& o, int dtype,
-                             bool phase_runs);
+                             bool phase_runs, TileMode tile);
 }
 
 std::vector<Sweep> plan_sweeps(const std::vector<Gate>& in, uint32_t n, const qsvb_plan_opts& o0, int dtype) {
   qsvb_plan_opts o = o0;
   if (o.max_fused_qubits == 0) o.max_fused_qubits = 1;
   o.max_fused_qubits = std::min<uint32_t>(o.max_fused_qubits, std::min<uint32_t>(QSVB_MAX_GATE_QUBITS, n));
-  if (o.planner != QSVB_PLAN_LEARNED) return plan_with(in, n, o, dtype, false);
-  // learned: merging long diagonal runs into phase-polynomial sweeps is itself a candidate choice
-  std::vector<Sweep> a = plan_with(in, n, o, dtype, true), b = plan_with(in, n, o, dtype, false);
-  return predict_plan_seconds(a, n, dtype) <= predict_plan_seconds(b, n, dtype) ? a : b;
+  if (o.planner == QSVB_PLAN_TILE) return plan_with(in, n, o, dtype, true, TILE_ALWAYS);
+  if (o.planner != QSVB_PLAN_LEARNED) return plan_with(in, n, o, dtype, false, TILE_NO);
+  // learned: merging long diagonal runs into phase-polynomial sweeps, and running gate runs as
+  // tile passes, are candidate choices weighed by predicted time
+  std::vector<Sweep> best;
+  double best_t = 1e300;
+  for (int c = 0; c < 3; ++c) {
+    std::vector<Sweep> cand = c == 0   ? plan_with(in, n, o, dtype, true, TILE_NO)
+                              : c == 1 ? plan_with(in, n, o, dtype, false, TILE_NO)
+                                       : plan_with(in, n, o, dtype, true, TILE_CHOOSE);
+    const double t = predict_plan_seconds(cand, n, dtype);
+    if (t < best_t) {
+      best_t = t;
+      best = std::move(cand);
+    }
+  }
+  return best;
 }
 
 namespace {
+// Fused sweeps for a run of gates (the planner's fusion, then classification).
+std::vector<Sweep> fused_sweeps(const std::vector<Gate>& seg, uint32_t n, const qsvb_plan_opts& o, int dtype) {
+  std::vector<Sweep> out;
+  if (seg.empty()) return out;
+  std::vector<Gate> fused;
+  if (o.planner == QSVB_PLAN_LEARNED) {
+    fused = learned_fuse(seg, n, o, dtype);
+  } else if (o.planner == QSVB_PLAN_TILE) {
+    fused = fuse_greedy(seg, o.max_fused_qubits);
+  } else {
+    fused = fuse_gates(seg, n, o, dtype);
+  }
+  for (const Gate& g : fused) {
+    Sweep s = classify_gate(g);
+    if (s.kind == SK_NONE) continue;
+    out.push_back(std::move(s));
+  }
+  return out;
+}
+
+// Tile passes over a run of gates. Each pass takes a local set S (qubits 0..4 plus the qubits of
+// the first pending gates, up to the tile width) and every pending 1- or 2-qubit gate inside S
+// that commutes past the pending gates it skips (disjoint qubits, or both diagonal); wider gates
+// end the run and become fused sweeps. TILE_CHOOSE keeps a pass as a tile sweep only when it is
+// predicted faster than the fused sweeps of the same gates.
+void tile_segment(const std::vector<Gate>& seg, uint32_t n, const qsvb_plan_opts& o, int dtype, TileMode mode,
+                  std::vector<Sweep>& out) {
+  const uint32_t L = tile_local_bits(dtype, n);
+  auto append = [&](std::vector<Sweep>&& v) {
+    for (Sweep& s : v) out.push_back(std::move(s));
+  };
+  if (L == 0) {
+    append(fused_sweeps(seg, n, o, dtype));
+    return;
+  }
+  std::vector<Gate> pend;
+  auto flush = [&] {
+    std::vector<char> done(pend.size(), 0);
+    size_t first = 0;
+    while (true) {
+      while (first < pend.size() && done[first]) ++first;
+      if (first == pend.size()) break;
+      uint64_t S = 31;
+      for (size_t i = first; i < pend.size() && uint32_t(__builtin_popcountll(S)) < L; ++i) {
+        if (done[i]) continue;
+        const uint64_t m = qmask(pend[i]);
+        if (uint32_t(__builtin_popcountll(S | m)) <= L) S |= m;
+      }
+      for (uint32_t b = 5; b < n && uint32_t(__builtin_popcountll(S)) < L; ++b) S |= 1ull << b;
+      uint64_t blocked = 0, dblocked = 0;
+      Sweep t;
+      t.kind = SK_TILE;
+      t.tile_mask = S;
+      for (size_t i = first; i < pend.size(); ++i) {
+        if (done[i]) continue;
+        const uint64_t m = qmask(pend[i]);
+        const bool diag = is_diag(pend[i]);
+        if ((m & ~S) == 0 && (m & blocked) == 0 && (diag || (m & dblocked) == 0)) {
+          done[i] = 1;
+          t.tile_gates.push_back(pend[i]);
+        } else if (diag) {
+          dblocked |= m;
+        } else {
+          blocked |= m;
+        }
+      }
+      if (mode == TILE_CHOOSE) {
+        std::vector<Sweep> alt = fused_sweeps(t.tile_gates, n, o, dtype);
+        select_engines(alt, n, o, dtype);
+        tile_prepare(t, n, dtype);
+        if (predict_plan_seconds(alt, n, dtype) <= predict_sweep_seconds(t, n, dtype)) {
+          append(std::move(alt));
+          continue;
+        }
+      } else {
+        tile_prepare(t, n, dtype);
+      }
+      out.push_back(std::move(t));
+    }
+    pend.clear();
+  };
+  for (const Gate& g : seg) {
+    if (g.m <= 2) {
+      pend.push_back(g);
+    } else {
+      flush();
+      append(fused_sweeps(std::vector<Gate>{g}, n, o, dtype));
+    }
+  }
+  flush();
+}
+
 std::vector<Sweep> plan_with(const std::vector<Gate>& in, uint32_t n, const qsvb_plan_opts& o, int dtype,
-                             bool phase_runs) {
+                             bool phase_runs, TileMode tile) {
 
   // split into segments: phase-polynomial runs vs ordinary gates
   std::vector<Sweep> out;
   auto run_segment = [&](const std::vector<Gate>& seg) {
     if (seg.empty()) return;
-    std::vector<Gate> fused;
-    if (o.planner == QSVB_PLAN_LEARNED) fused = learned_fuse(seg, n, o, dtype);
-    else fused = fuse_gates(seg, n, o, dtype);
-    for (const Gate& g : fused) {
-      Sweep s = classify_gate(g);
-      if (s.kind == SK_NONE) continue;
-      out.push_back(std::move(s));
+    if (tile != TILE_NO) {
+      tile_segment(seg, n, o, dtype, tile, out);
+      return;
     }
+    for (Sweep& s : fused_sweeps(seg, n, o, dtype)) out.push_back(std::move(s));
   };
   std::vector<Gate> seg;
   size_t i = 0;
@@ -390,6 +493,7 @@ void sweep_costs(const std::vector<Sweep>& sw, uint32_t n, int dtype, qsvb_plan_
     st->algorithmic_bytes += 2.0 * amps * b;
     st->full_sweep_bytes += 2.0 * dim * b;
     if (s.kind == SK_DENSE || s.kind == SK_DENSE_TC) st->flops += 8.0 * std::ldexp(1.0, int(s.m)) * dim;
+    if (s.kind == SK_TILE) st->flops += s.tile_flops;
   }
   st->predicted_seconds = predict_plan_seconds(sw, n, dtype);
 }

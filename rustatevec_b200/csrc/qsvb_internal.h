@@ -41,8 +41,14 @@ enum SweepKind : int {
   SK_PHASE = 3,     // phase polynomial: product of many <= 2-qubit diagonal terms
   SK_DENSE = 4,     // dense 2^k x 2^k on CUDA cores
   SK_DENSE_TC = 5,  // dense 2^k x 2^k on tcgen05 tensor cores (complex64 only)
-  SK_SWAP = 6,      // reserved
+  SK_TILE = 6,      // gate program on shared-memory tiles of 2^L amplitudes (one read + one write)
   SK_NONE = 7       // identity (dropped)
+};
+
+struct Gate {  // host copy of an input gate, FP64
+  uint32_t m = 0;
+  uint32_t q[6] = {0, 0, 0, 0, 0, 0};
+  std::vector<cd> a;  // row-major 2^m x 2^m
 };
 
 struct PhaseTerm {
@@ -61,12 +67,14 @@ struct Sweep {
   uint32_t ctrl[6] = {0, 0, 0, 0, 0, 0};
   std::vector<PhaseTerm> terms;   // phase polynomial
   uint64_t n_gates = 0;           // input gates covered
-};
-
-struct Gate {  // host copy of an input gate, FP64
-  uint32_t m = 0;
-  uint32_t q[6] = {0, 0, 0, 0, 0, 0};
-  std::vector<cd> a;  // row-major 2^m x 2^m
+  // tile sweeps: the local qubit set, the gate program (1q/2q, in order) and its packed device
+  // image with the launch parameters (filled by tile_prepare)
+  uint64_t tile_mask = 0;
+  std::vector<Gate> tile_gates;
+  std::vector<uint8_t> tile_blob;
+  uint32_t tile_rb = 0, tile_lbits = 0, tile_ntiles = 0;
+  uint32_t tile_off_phase = 0, tile_off_prog = 0, tile_off_coef = 0;
+  double tile_flops = 0;
 };
 
 std::vector<Gate> gates_from_circuit(const qsvb_circuit* c);
@@ -114,6 +122,13 @@ void launch_inner_mixed(const LaunchEnv& e, const RA* are, const RA* aim, const 
 template <class R>
 void launch_probabilities(const LaunchEnv& e, const R* re, const R* im, uint64_t offset, uint64_t count,
                           void* out, int out_f64);
+
+// Tile sweeps (batch.cu): local-qubit count for an n-qubit state (0 = state too small for tiles),
+// program construction, and the launch.
+uint32_t tile_local_bits(int dtype, uint32_t n);
+void tile_prepare(Sweep& s, uint32_t n, int dtype);
+template <class R>
+void launch_tile(const LaunchEnv& e, R* re, R* im, uint32_t n, const Sweep& s, const void* dev_blob);
 
 // Tensor-core dense sweep (complex64): implemented in tc_dense.cu.
 bool tc_dense_supported(const Sweep& s, uint32_t n);
