@@ -33,6 +33,13 @@ N_QUBITS, DEPTH, SEED = 30, 20, 0
 WORKLOAD = f"random brickwork {N_QUBITS}q depth {DEPTH}, complex64, Haar SU(2) + CZ, seed {SEED}"
 
 
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum, one ncu capture of one launch at 26
+# qubits, scaled by the amplitudes a launch processes) per algorithmic byte, for the kernels the
+# roofline object can name
+TRAFFIC_PER_ALGORITHMIC_BYTE = {"dense_tc": (537.092608 + 476.665344) / 1073.741824,
+                                "1q": (536.916992 + 479.222272) / 1073.741824}
+
+
 def peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -261,8 +268,11 @@ def run_gpu(args):
         d = by_kind[dom]
         peak, peak_kind = peaks()
         achieved = d["bytes"] / d["time"] / 1e9
+        ratio = TRAFFIC_PER_ALGORITHMIC_BYTE.get(dom)
         roofline = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak,
-                    "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": None,
+                    "unit": "GB/s", "frac": round(achieved / peak, 4),
+                    "traffic": round(ratio * d["bytes"] / d["launches"]) if ratio else None,
+                    "traffic_source": "ncu dram bytes of one launch at 26 qubits, scaled by amplitudes" if ratio else None,
                     "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback",
                     "avg_launch_us": round(d["time"] / d["launches"] * 1e6, 1),
                     "algorithmic_bytes_per_launch": d["bytes"] / d["launches"],
@@ -584,11 +594,12 @@ def run_config_batched(args):
     clk = None
     for prec in ("f32", "f64"):
         be = B200Backend(local, precision=prec)
-        best_l, best_r = C.c_uint32(), C.c_uint32()
+        best_l, best_r = C.c_uint32(0), C.c_uint32(0)
         secs = np.zeros(6)
-        cnt = C.c_size_t()
-        L.check(L.lib().qsvb_batch_autotune(be.ctx, pb.ptr(), pb.count, be.dtype, C.byref(best_l), C.byref(best_r),
-                                            secs.ctypes.data_as(L._dp), 6, C.byref(cnt)))
+        cnt = C.c_size_t(0)
+        if not args.no_autotune:
+            L.check(L.lib().qsvb_batch_autotune(be.ctx, pb.ptr(), pb.count, be.dtype, C.byref(best_l),
+                                                C.byref(best_r), secs.ctypes.data_as(L._dp), 6, C.byref(cnt)))
         h = C.c_void_p()
         L.check(L.lib().qsvb_batch_create(be.ctx, pb.ptr(), pb.count, be.dtype, best_l.value, best_r.value,
                                           C.byref(h)))
@@ -745,6 +756,7 @@ def main():
     ap.add_argument("--config", default="brickwork30", choices=["brickwork30", "ghz24", "qft32", "qaoa33", "batched"],
                     help="workload (the default is the headline bench line)")
     ap.add_argument("--circuits", type=int, default=4096, help="batched config: number of circuits")
+    ap.add_argument("--no-autotune", action="store_true", help="batched config: engine's default tile shape")
     args = ap.parse_args()
     if args.kernel_case:
         run_kernel_case(args)
