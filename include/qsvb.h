@@ -67,7 +67,7 @@ typedef enum qsvb_planner {
   QSVB_PLAN_LEARNED = 3,  /* cost-model planner (MLP cost model; greedy fallback); also weighs
                              tile passes against fused sweeps */
   QSVB_PLAN_TILE = 4      /* tile passes: the 1- and 2-qubit gates acting inside a set of up to
-                             13 qubits (12 for complex128) that commute past the gates left for
+                             12 qubits (11 for complex128) that commute past the gates left for
                              later, applied on shared-memory tiles in one read and one write of
                              the state; diagonal runs become phase sweeps, wider gates fused sweeps */
 } qsvb_planner;

@@ -51,6 +51,7 @@ constexpr int kMaxLocal = 14;
 constexpr int kMaxHi = 512;                   // 2^(kMaxLocal - 5): entries of the address / swizzle tables
 constexpr long long kSpinBudget = 1ll << 32;  // clock64 cycles (about 2 s)
 constexpr uint32_t kStageBytes = 32768;       // shared memory for one pass's program
+constexpr uint32_t kTileStageBytes = 16384;   // the same for tile sweeps (four blocks per SM)
 
 enum BatchOp : uint32_t { OP_PHASE = 0, OP_1Q = 1, OP_D1 = 2, OP_CX = 3, OP_2Q = 4, OP_D2 = 5 };
 
@@ -62,9 +63,11 @@ struct Instr {
 
 struct PhaseDev {
   uint32_t rphys[5];  // swizzled shared-memory offset of each register bit's unit vector
-  uint8_t tpos[12];   // group bit i -> local position (bits 0..4 are the warp lanes)
   uint32_t r, nt;     // register bits used, group bits (2^nt groups of 2^r amplitudes)
   uint32_t ninstr;    // gate instructions that follow the phase instruction
+  // swizzled shared-memory offset of a group's first amplitude, split by the group index's low 5
+  // bits (the warp lanes) and the bits above: offset(g) = lo[g & 31] ^ hi[g >> 5]
+  uint16_t lo[32], hi[32];
 };
 
 struct PassDev {
@@ -104,6 +107,25 @@ __device__ __forceinline__ void cp_async_elem(R* dst, const R* src) {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src) : "memory");
 }
 
+// 16-byte vectors of amplitude components (4 floats / 2 doubles) for the tile fill and write-back.
+template <class R> struct Vec16;
+template <> struct Vec16<float> {
+  using T = float4;
+  static constexpr int N = 4;
+  __device__ static float get(const float4& v, int e) { return e == 0 ? v.x : e == 1 ? v.y : e == 2 ? v.z : v.w; }
+  __device__ static void set(float4& v, int e, float x) {
+    if (e == 0) v.x = x; else if (e == 1) v.y = x; else if (e == 2) v.z = x; else v.w = x;
+  }
+};
+template <> struct Vec16<double> {
+  using T = double2;
+  static constexpr int N = 2;
+  __device__ static double get(const double2& v, int e) { return e == 0 ? v.x : v.y; }
+  __device__ static void set(double2& v, int e, double x) {
+    if (e == 0) v.x = x; else v.y = x;
+  }
+};
+
 template <class R>
 __device__ __forceinline__ void cmac(R& yr, R& yi, R ar, R ai, R xr, R xi) {
   yr = fma(ar, xr, yr);
@@ -127,41 +149,68 @@ template <int RB> struct Regs<double, RB> {
   __device__ __forceinline__ double& im(int s) { return i[s]; }
 };
 
-__device__ __forceinline__ float2 bc(float x) { return make_float2(x, x); }
-
 // ---- gates on register bits (compile-time bit positions, so the amplitudes stay in registers)
 template <int J, class R, int RB>
 __device__ __forceinline__ void g1q(Regs<R, RB>& v, const R* __restrict__ c) {
   if constexpr (J < RB) {
-    const R a0 = c[0], a1 = c[1], b0 = c[2], b1 = c[3], c0 = c[4], c1 = c[5], d0 = c[6], d1 = c[7];
-    if constexpr (std::is_same<R, float>::value && J >= 1) {
-      // two amplitudes per instruction; same operation order as the scalar path below
-      constexpr int HJ = 1 << (J - 1);
+    if constexpr (std::is_same<R, float>::value) {
+      // complex64 coefficients come pre-broadcast as float2 pairs: for each of a, b, c, d (the 2x2
+      // in row-major order) the pairs (re, re), (im, im), (-im, -im)
+      const float2* cc = reinterpret_cast<const float2*>(c);
+      if constexpr (J >= 1) {
+        // two amplitudes per instruction; same operation order as the scalar path below
+        constexpr int HJ = 1 << (J - 1);
+        const float2 A0 = cc[0], A1 = cc[1], NA1 = cc[2], B0 = cc[3], B1 = cc[4], NB1 = cc[5];
+        const float2 C0 = cc[6], C1 = cc[7], NC1 = cc[8], D0 = cc[9], D1 = cc[10], ND1 = cc[11];
 #pragma unroll
-      for (int h = 0; h < (1 << RB) / 2; ++h) {
-        if (h & HJ) continue;
-        const int t = h | HJ;
-        const float2 xr0 = v.r[h], xi0 = v.i[h], xr1 = v.r[t], xi1 = v.i[t];
-        float2 yr0 = __fmul2_rn(bc(a0), xr0), yi0 = __fmul2_rn(bc(a0), xi0);
-        float2 yr1 = __fmul2_rn(bc(c0), xr0), yi1 = __fmul2_rn(bc(c0), xi0);
-        yr0 = __ffma2_rn(bc(-a1), xi0, yr0);
-        yi0 = __ffma2_rn(bc(a1), xr0, yi0);
-        yr1 = __ffma2_rn(bc(-c1), xi0, yr1);
-        yi1 = __ffma2_rn(bc(c1), xr0, yi1);
-        yr0 = __ffma2_rn(bc(b0), xr1, yr0);
-        yi0 = __ffma2_rn(bc(b0), xi1, yi0);
-        yr1 = __ffma2_rn(bc(d0), xr1, yr1);
-        yi1 = __ffma2_rn(bc(d0), xi1, yi1);
-        yr0 = __ffma2_rn(bc(-b1), xi1, yr0);
-        yi0 = __ffma2_rn(bc(b1), xr1, yi0);
-        yr1 = __ffma2_rn(bc(-d1), xi1, yr1);
-        yi1 = __ffma2_rn(bc(d1), xr1, yi1);
-        v.r[h] = yr0;
-        v.i[h] = yi0;
-        v.r[t] = yr1;
-        v.i[t] = yi1;
+        for (int h = 0; h < (1 << RB) / 2; ++h) {
+          if (h & HJ) continue;
+          const int t = h | HJ;
+          const float2 xr0 = v.r[h], xi0 = v.i[h], xr1 = v.r[t], xi1 = v.i[t];
+          float2 yr0 = __fmul2_rn(A0, xr0), yi0 = __fmul2_rn(A0, xi0);
+          float2 yr1 = __fmul2_rn(C0, xr0), yi1 = __fmul2_rn(C0, xi0);
+          yr0 = __ffma2_rn(NA1, xi0, yr0);
+          yi0 = __ffma2_rn(A1, xr0, yi0);
+          yr1 = __ffma2_rn(NC1, xi0, yr1);
+          yi1 = __ffma2_rn(C1, xr0, yi1);
+          yr0 = __ffma2_rn(B0, xr1, yr0);
+          yi0 = __ffma2_rn(B0, xi1, yi0);
+          yr1 = __ffma2_rn(D0, xr1, yr1);
+          yi1 = __ffma2_rn(D0, xi1, yi1);
+          yr0 = __ffma2_rn(NB1, xi1, yr0);
+          yi0 = __ffma2_rn(B1, xr1, yi0);
+          yr1 = __ffma2_rn(ND1, xi1, yr1);
+          yi1 = __ffma2_rn(D1, xr1, yi1);
+          v.r[h] = yr0;
+          v.i[h] = yi0;
+          v.r[t] = yr1;
+          v.i[t] = yi1;
+        }
+      } else {
+        const float a0 = cc[0].x, a1 = cc[1].x, b0 = cc[3].x, b1 = cc[4].x;
+        const float c0 = cc[6].x, c1 = cc[7].x, d0 = cc[9].x, d1 = cc[10].x;
+#pragma unroll
+        for (int h = 0; h < (1 << RB) / 2; ++h) {
+          const float xr0 = v.r[h].x, xi0 = v.i[h].x, xr1 = v.r[h].y, xi1 = v.i[h].y;
+          float yr0 = a0 * xr0, yi0 = a0 * xi0, yr1 = c0 * xr0, yi1 = c0 * xi0;
+          yr0 = fmaf(-a1, xi0, yr0);
+          yi0 = fmaf(a1, xr0, yi0);
+          yr1 = fmaf(-c1, xi0, yr1);
+          yi1 = fmaf(c1, xr0, yi1);
+          yr0 = fmaf(b0, xr1, yr0);
+          yi0 = fmaf(b0, xi1, yi0);
+          yr1 = fmaf(d0, xr1, yr1);
+          yi1 = fmaf(d0, xi1, yi1);
+          yr0 = fmaf(-b1, xi1, yr0);
+          yi0 = fmaf(b1, xr1, yi0);
+          yr1 = fmaf(-d1, xi1, yr1);
+          yi1 = fmaf(d1, xr1, yi1);
+          v.r[h] = make_float2(yr0, yr1);
+          v.i[h] = make_float2(yi0, yi1);
+        }
       }
     } else {
+      const R a0 = c[0], a1 = c[1], b0 = c[2], b1 = c[3], c0 = c[4], c1 = c[5], d0 = c[6], d1 = c[7];
 #pragma unroll
       for (int s = 0; s < (1 << RB); ++s) {
         if (s & (1 << J)) continue;
@@ -192,20 +241,21 @@ __device__ __forceinline__ void g1q(Regs<R, RB>& v, const R* __restrict__ c) {
 template <int J, class R, int RB>
 __device__ __forceinline__ void gd1(Regs<R, RB>& v, const R* __restrict__ c) {
   if constexpr (J < RB) {
-    const R p0r = c[0], p0i = c[1], p1r = c[2], p1i = c[3];
     if constexpr (std::is_same<R, float>::value) {
-      // the pair (s, s^1) shares bit J unless J == 0, where the lanes take the two phases
-      const float2 pr0 = J == 0 ? make_float2(p0r, p1r) : bc(p0r), pi0 = J == 0 ? make_float2(p0i, p1i) : bc(p0i);
-      const float2 pr1 = J == 0 ? pr0 : bc(p1r), pi1 = J == 0 ? pi0 : bc(p1i);
+      // pre-broadcast pairs (re, im, -im) for the 0 side and the 1 side of bit J; for J == 0 the
+      // pair (s, s^1) straddles bit J, so both sets hold (value at s, value at s^1)
+      const float2* cc = reinterpret_cast<const float2*>(c);
+      const float2 pr0 = cc[0], pi0 = cc[1], npi0 = cc[2], pr1 = cc[3], pi1 = cc[4], npi1 = cc[5];
 #pragma unroll
       for (int h = 0; h < (1 << RB) / 2; ++h) {
-        const bool one = J >= 1 && (h & (1 << (J - 1 < 0 ? 0 : J - 1)));
-        const float2 pr = one ? pr1 : pr0, pi = one ? pi1 : pi0;
+        const bool one = J >= 1 && (h & (1 << (J >= 1 ? J - 1 : 0)));
+        const float2 pr = one ? pr1 : pr0, pi = one ? pi1 : pi0, npi = one ? npi1 : npi0;
         const float2 xr = v.r[h], xi = v.i[h];
-        v.r[h] = __ffma2_rn(pr, xr, __fmul2_rn(make_float2(-pi.x, -pi.y), xi));
+        v.r[h] = __ffma2_rn(pr, xr, __fmul2_rn(npi, xi));
         v.i[h] = __ffma2_rn(pr, xi, __fmul2_rn(pi, xr));
       }
     } else {
+      const R p0r = c[0], p0i = c[1], p1r = c[2], p1i = c[3];
 #pragma unroll
       for (int s = 0; s < (1 << RB); ++s) {
         const R pr = (s & (1 << J)) ? p1r : p0r, pi = (s & (1 << J)) ? p1i : p0i;
@@ -284,26 +334,28 @@ __device__ __forceinline__ void gd2(Regs<R, RB>& v, const R* __restrict__ c) {
   case 2 * 8 + 4: F<2, 4, R, RB>(__VA_ARGS__); break; \
   case 3 * 8 + 4: F<3, 4, R, RB>(__VA_ARGS__); break;
 
-template <class R, int RB>
-__device__ __forceinline__ void apply_instr(const Instr& in, Regs<R, RB>& v, const R* __restrict__ coef) {
+// Applies one instruction to G groups held by this thread (the dispatch and the coefficient loads
+// are shared; the G independent updates interleave).
+template <class R, int RB, int G>
+__device__ __forceinline__ void apply_instr(const Instr& in, Regs<R, RB>* v, const R* __restrict__ coef) {
   const R* c = coef + 2 * size_t(in.coef);
   switch (in.op) {
     case OP_1Q:
       switch (in.a) {
-        case 0: g1q<0, R, RB>(v, c); break;
-        case 1: g1q<1, R, RB>(v, c); break;
-        case 2: g1q<2, R, RB>(v, c); break;
-        case 3: g1q<3, R, RB>(v, c); break;
-        case 4: g1q<4, R, RB>(v, c); break;
+        case 0: for (int g = 0; g < G; ++g) g1q<0, R, RB>(v[g], c); break;
+        case 1: for (int g = 0; g < G; ++g) g1q<1, R, RB>(v[g], c); break;
+        case 2: for (int g = 0; g < G; ++g) g1q<2, R, RB>(v[g], c); break;
+        case 3: for (int g = 0; g < G; ++g) g1q<3, R, RB>(v[g], c); break;
+        case 4: for (int g = 0; g < G; ++g) g1q<4, R, RB>(v[g], c); break;
       }
       break;
     case OP_D1:
       switch (in.a) {
-        case 0: gd1<0, R, RB>(v, c); break;
-        case 1: gd1<1, R, RB>(v, c); break;
-        case 2: gd1<2, R, RB>(v, c); break;
-        case 3: gd1<3, R, RB>(v, c); break;
-        case 4: gd1<4, R, RB>(v, c); break;
+        case 0: for (int g = 0; g < G; ++g) gd1<0, R, RB>(v[g], c); break;
+        case 1: for (int g = 0; g < G; ++g) gd1<1, R, RB>(v[g], c); break;
+        case 2: for (int g = 0; g < G; ++g) gd1<2, R, RB>(v[g], c); break;
+        case 3: for (int g = 0; g < G; ++g) gd1<3, R, RB>(v[g], c); break;
+        case 4: for (int g = 0; g < G; ++g) gd1<4, R, RB>(v[g], c); break;
       }
       break;
     case OP_CX: {
@@ -312,8 +364,9 @@ __device__ __forceinline__ void apply_instr(const Instr& in, Regs<R, RB>& v, con
       switch (lo * 8 + hi) {
 #define QSVB_CX_CASE(J, K)       \
   case J * 8 + K:                \
-    if (fwd) gcx<J, K, R, RB>(v); \
-    else gcx<K, J, R, RB>(v);     \
+    for (int g = 0; g < G; ++g)       \
+      if (fwd) gcx<J, K, R, RB>(v[g]); \
+      else gcx<K, J, R, RB>(v[g]);     \
     break;
         QSVB_CX_CASE(0, 1)
         QSVB_CX_CASE(0, 2)
@@ -330,15 +383,81 @@ __device__ __forceinline__ void apply_instr(const Instr& in, Regs<R, RB>& v, con
       break;
     }
     case OP_2Q:
-      switch (in.a * 8 + in.b) { QSVB_PAIR_CASES(g2q, v, c) }
+      for (int g = 0; g < G; ++g) switch (in.a * 8 + in.b) { QSVB_PAIR_CASES(g2q, v[g], c) }
       break;
     case OP_D2:
-      switch (in.a * 8 + in.b) { QSVB_PAIR_CASES(gd2, v, c) }
+      for (int g = 0; g < G; ++g) switch (in.a * 8 + in.b) { QSVB_PAIR_CASES(gd2, v[g], c) }
       break;
   }
 }
 
-template <class R, int RB, int W, int NT, int MINB = 1>
+// One register phase for G groups of this thread: load 2^r amplitudes per group from the swizzled
+// tile, apply the phase's instructions, store them back.
+template <class R, int RB, int G>
+__device__ __forceinline__ void phase_groups(const uint32_t* grp, const PhaseDev& D, const uint32_t* rp, R* xr, R* xi,
+                                             const Instr* pprog, uint32_t kbeg, uint32_t kend, const R* pcoef) {
+  constexpr int NV = 1 << RB;
+  const uint32_t r = D.r;
+  uint32_t p0[G];
+  Regs<R, RB> v[G];
+#pragma unroll
+  for (int g = 0; g < G; ++g) p0[g] = uint32_t(D.lo[grp[g] & 31u]) ^ uint32_t(D.hi[grp[g] >> 5]);
+  if (r == uint32_t(RB)) {  // full register tile (every pass with at least RB local qubits)
+#pragma unroll
+    for (int g = 0; g < G; ++g)
+#pragma unroll
+      for (int s = 0; s < NV; ++s) {
+        uint32_t off = p0[g];
+#pragma unroll
+        for (int j = 0; j < RB; ++j)
+          if (s & (1 << j)) off ^= rp[j];
+        v[g].re(s) = xr[off];
+        v[g].im(s) = xi[off];
+      }
+  } else {
+#pragma unroll
+    for (int g = 0; g < G; ++g)
+#pragma unroll
+      for (int s = 0; s < NV; ++s) {
+        if (uint32_t(s) >> r) continue;
+        uint32_t off = p0[g];
+#pragma unroll
+        for (int j = 0; j < RB; ++j)
+          if (s & (1 << j)) off ^= rp[j];
+        v[g].re(s) = xr[off];
+        v[g].im(s) = xi[off];
+      }
+  }
+  for (uint32_t kk = kbeg; kk < kend; ++kk) apply_instr<R, RB, G>(pprog[kk], v, pcoef);
+  if (r == uint32_t(RB)) {
+#pragma unroll
+    for (int g = 0; g < G; ++g)
+#pragma unroll
+      for (int s = 0; s < NV; ++s) {
+        uint32_t off = p0[g];
+#pragma unroll
+        for (int j = 0; j < RB; ++j)
+          if (s & (1 << j)) off ^= rp[j];
+        xr[off] = v[g].re(s);
+        xi[off] = v[g].im(s);
+      }
+  } else {
+#pragma unroll
+    for (int g = 0; g < G; ++g)
+#pragma unroll
+      for (int s = 0; s < NV; ++s) {
+        if (uint32_t(s) >> r) continue;
+        uint32_t off = p0[g];
+#pragma unroll
+        for (int j = 0; j < RB; ++j)
+          if (s & (1 << j)) off ^= rp[j];
+        xr[off] = v[g].re(s);
+        xi[off] = v[g].im(s);
+      }
+  }
+}
+
+template <class R, int RB, int W, int NT, int MINB = 1, int GP = 1>
 __global__ void __launch_bounds__(NT, MINB)
     k_batch(const Item* __restrict__ items, uint32_t nitems, const PassDev* __restrict__ passes,
             const PhaseDev* __restrict__ phases, const Instr* __restrict__ prog, const R* __restrict__ coef,
@@ -355,7 +474,6 @@ __global__ void __launch_bounds__(NT, MINB)
   __shared__ double s_red[NT / 32];
   __shared__ int s_ok;
   const int tid = threadIdx.x;
-  constexpr int NV = 1 << RB;
   // swizzle table over the index bits above W
   for (uint32_t h = tid; h < (1u << (lbits - W)); h += NT) {
     uint32_t v = 0;
@@ -442,6 +560,36 @@ __global__ void __launch_bounds__(NT, MINB)
       }
       __syncthreads();
       if (tid == 0 && item.tile == 0) xr[0] = R(1);  // the swizzle maps 0 to 0
+    } else if (L >= 5) {
+      // 16-byte loads of contiguous amplitudes (a run of 32 shares its global offset), several in
+      // flight per thread, then scattered through the swizzle (it only flips bits below W, so the
+      // VN amplitudes of a vector land at y ^ e)
+      using VT = typename Vec16<R>::T;
+      constexpr int VN = Vec16<R>::N, UNR = 4;
+      for (uint32_t xb = tid * VN; xb < T; xb += NT * VN * UNR) {
+        VT vr[UNR], vi[UNR];
+#pragma unroll
+        for (int u = 0; u < UNR; ++u) {
+          const uint32_t x = xb + uint32_t(u) * NT * VN;
+          if (x < T) {
+            const uint64_t a = s_gaddr[x >> 5] | (x & 31u);
+            vr[u] = __ldcg(reinterpret_cast<const VT*>(gre + a));
+            vi[u] = __ldcg(reinterpret_cast<const VT*>(gim + a));
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < UNR; ++u) {
+          const uint32_t x = xb + uint32_t(u) * NT * VN;
+          if (x < T) {
+            const uint32_t y = x ^ s_swz[x >> W];
+#pragma unroll
+            for (int e = 0; e < VN; ++e) {
+              xr[y ^ uint32_t(e)] = Vec16<R>::get(vr[u], e);
+              xi[y ^ uint32_t(e)] = Vec16<R>::get(vi[u], e);
+            }
+          }
+        }
+      }
     } else {
       for (uint32_t x = tid; x < T; x += NT) {
         const uint64_t a = s_gaddr[x >> 5] | (x & lowmask);
@@ -458,37 +606,23 @@ __global__ void __launch_bounds__(NT, MINB)
     uint32_t k = 0;
     while (k < P.prog_len) {
       const PhaseDev& D = pph[pprog[k].coef];
-      const uint32_t r = D.r, nt = D.nt;
+      const uint32_t nt = D.nt;
       const uint32_t kbeg = k + 1, kend = kbeg + D.ninstr;
       uint32_t rp[RB];
 #pragma unroll
       for (int j = 0; j < RB; ++j) rp[j] = D.rphys[j];
-      for (uint32_t grp = tid; grp < (1u << nt); grp += NT) {
-        uint32_t x0 = 0;
-        for (uint32_t i = 0; i < nt; ++i) x0 |= ((grp >> i) & 1u) << D.tpos[i];
-        const uint32_t p0 = x0 ^ s_swz[x0 >> W];
-        Regs<R, RB> v;
-#pragma unroll
-        for (int s = 0; s < NV; ++s) {
-          if (uint32_t(s) >> r) continue;
-          uint32_t off = p0;
-#pragma unroll
-          for (int j = 0; j < RB; ++j)
-            if (s & (1 << j)) off ^= rp[j];
-          v.re(s) = xr[off];
-          v.im(s) = xi[off];
+      // two groups at a time where the thread has two (independent updates interleave), then one
+      const uint32_t ngrp = 1u << nt;
+      uint32_t grp = tid;
+      if constexpr (GP == 2) {
+        for (; grp + NT < ngrp; grp += 2 * NT) {
+          const uint32_t gg[2] = {grp, grp + NT};
+          phase_groups<R, RB, 2>(gg, D, rp, xr, xi, pprog, kbeg, kend, pcoef);
         }
-        for (uint32_t kk = kbeg; kk < kend; ++kk) apply_instr<R, RB>(pprog[kk], v, pcoef);
-#pragma unroll
-        for (int s = 0; s < NV; ++s) {
-          if (uint32_t(s) >> r) continue;
-          uint32_t off = p0;
-#pragma unroll
-          for (int j = 0; j < RB; ++j)
-            if (s & (1 << j)) off ^= rp[j];
-          xr[off] = v.re(s);
-          xi[off] = v.im(s);
-        }
+      }
+      for (; grp < ngrp; grp += NT) {
+        const uint32_t gg[1] = {grp};
+        phase_groups<R, RB, 1>(gg, D, rp, xr, xi, pprog, kbeg, kend, pcoef);
       }
       k = kend;
       __syncthreads();
@@ -512,6 +646,21 @@ __global__ void __launch_bounds__(NT, MINB)
         double s = 0.0;
         for (int w = 0; w < NT / 32; ++w) s += s_red[w];
         zpart[P.zslot + item.tile] = s;
+      }
+    } else if (L >= 5) {
+      using VT = typename Vec16<R>::T;
+      constexpr int VN = Vec16<R>::N;
+      for (uint32_t x = tid * VN; x < T; x += NT * VN) {
+        const uint64_t a = s_gaddr[x >> 5] | (x & 31u);
+        const uint32_t y = x ^ s_swz[x >> W];
+        VT vr, vi;
+#pragma unroll
+        for (int e = 0; e < VN; ++e) {
+          Vec16<R>::set(vr, e, xr[y ^ uint32_t(e)]);
+          Vec16<R>::set(vi, e, xi[y ^ uint32_t(e)]);
+        }
+        __stcg(reinterpret_cast<VT*>(gre + a), vr);
+        __stcg(reinterpret_cast<VT*>(gim + a), vi);
       }
     } else {
       for (uint32_t x = tid; x < T; x += NT) {
@@ -709,7 +858,19 @@ void emit_phases(BatchPlan& bp, const std::vector<LGate>& G, uint32_t nlocal) {
     for (size_t i = 0; i < nonr.size(); ++i)
       if (!used[i]) lanes.push_back(nonr[i]);
     D.nt = uint32_t(nonr.size());
-    for (size_t i = 0; i < lanes.size(); ++i) D.tpos[i] = uint8_t(lanes[i]);
+    QSVB_REQUIRE(D.nt <= 10, "register phase with more than 2^10 groups");
+    // group index bits -> local positions (lanes first), as swizzled offsets: the swizzle is
+    // linear, so the offset of a group is the XOR of the offsets of its bits
+    auto phys_of = [&](uint32_t pos) { return (1u << pos) ^ swz_col(int(pos), int(W)); };
+    for (uint32_t g = 0; g < 32; ++g) {
+      uint32_t lo = 0, hi = 0;
+      for (uint32_t i = 0; i < 5 && i < D.nt; ++i)
+        if ((g >> i) & 1u) lo ^= phys_of(lanes[i]);
+      for (uint32_t i = 5; i < 10 && i < D.nt; ++i)
+        if ((g >> (i - 5)) & 1u) hi ^= phys_of(lanes[i]);
+      D.lo[g] = uint16_t(lo);
+      D.hi[g] = uint16_t(hi);
+    }
     D.ninstr = uint32_t(taken.size());
     bp.prog.push_back(Instr{OP_PHASE, 0, 0, uint32_t(bp.phases.size() - phase_base)});
     bp.phases.push_back(D);
@@ -719,11 +880,37 @@ void emit_phases(BatchPlan& bp, const std::vector<LGate>& G, uint32_t nlocal) {
       const std::vector<cd>& a = g.g->a;
       switch (g.kind) {
         case LK_1Q:
-          for (int k = 0; k < 4; ++k) push_coef(bp, a[size_t(k)]);
+          if (bp.dtype == QSVB_C64) {  // pre-broadcast pairs (re, re), (im, im), (-im, -im) per entry
+            for (int k = 0; k < 4; ++k) {
+              const cd e = a[size_t(k)];
+              push_coef(bp, cd(e.real(), e.real()));
+              push_coef(bp, cd(e.imag(), e.imag()));
+              push_coef(bp, cd(-e.imag(), -e.imag()));
+            }
+          } else {
+            for (int k = 0; k < 4; ++k) push_coef(bp, a[size_t(k)]);
+          }
           break;
         case LK_D1:
-          push_coef(bp, a[0]);
-          push_coef(bp, a[3]);
+          if (bp.dtype == QSVB_C64) {
+            const cd p0 = a[0], p1 = a[3];
+            if (in.a == 0) {  // lanes of a float2 pair are the two sides of the gate's bit
+              for (int rep = 0; rep < 2; ++rep) {
+                push_coef(bp, cd(p0.real(), p1.real()));
+                push_coef(bp, cd(p0.imag(), p1.imag()));
+                push_coef(bp, cd(-p0.imag(), -p1.imag()));
+              }
+            } else {
+              for (const cd& e : {p0, p1}) {
+                push_coef(bp, cd(e.real(), e.real()));
+                push_coef(bp, cd(e.imag(), e.imag()));
+                push_coef(bp, cd(-e.imag(), -e.imag()));
+              }
+            }
+          } else {
+            push_coef(bp, a[0]);
+            push_coef(bp, a[3]);
+          }
           break;
         case LK_CX:
           in.b = uint32_t(regbit[g.p[1]]);
@@ -1153,7 +1340,7 @@ void free_batch(qsvb_batch* b) { delete b; }
 namespace qsvb {
 
 uint32_t tile_local_bits(int dtype, uint32_t n) {
-  const uint32_t lmax = batch_max_local_bits(dtype) - 1;  // half the shared memory: two blocks per SM
+  const uint32_t lmax = batch_max_local_bits(dtype) - 2;  // a quarter of the shared memory: four blocks per SM
   if (n >= lmax + 8) return lmax;  // at least 256 tiles to spread over the SMs
   if (n >= 15) return n - 8;
   return 0;
@@ -1162,18 +1349,18 @@ uint32_t tile_local_bits(int dtype, uint32_t n) {
 namespace {
 uint32_t tile_reg_bits(int dtype) { return dtype == QSVB_C128 ? 3u : 4u; }
 size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
-constexpr size_t kTileSmemMax = (size_t(2) * 4 << 14) + kStageBytes;  // equal for both precisions
+constexpr size_t kTileSmemMax = (size_t(2) * 4 << 12) + kTileStageBytes;  // equal for both precisions
 
-template <class R, int RB, int NT, int MINB>
+template <class R, int RB, int NT, int MINB, int GP>
 void launch_tile_variant(const LaunchEnv& e, R* re, R* im, const Sweep& s, const uint8_t* base) {
-  auto fn = k_batch<R, RB, sizeof(R) == 8 ? 4 : 5, NT, MINB>;
+  auto fn = k_batch<R, RB, sizeof(R) == 8 ? 4 : 5, NT, MINB, GP>;
   static std::once_flag once;
   std::call_once(once, [&] {
     QSVB_CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kTileSmemMax)));
     QSVB_CK(cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout,
                                  int(cudaSharedmemCarveoutMaxShared)));
   });
-  const size_t smem = ((size_t(2) * sizeof(R)) << s.tile_lbits) + kStageBytes;
+  const size_t smem = ((size_t(2) * sizeof(R)) << s.tile_lbits) + kTileStageBytes;
   int occ = 0;
   QSVB_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, NT, smem));
   QSVB_REQUIRE(occ >= 1, "tile kernel does not fit on an SM");
@@ -1195,9 +1382,9 @@ void tile_prepare(Sweep& s, uint32_t n, int dtype) {
   bp.swz_w = dtype == QSVB_C128 ? 4u : 5u;
   PassDev P{};
   P.nlocal = uint32_t(__builtin_popcountll(S));
-  QSVB_REQUIRE((S & 31u) == 31u && P.nlocal >= 7 && P.nlocal <= batch_max_local_bits(dtype) - 1 && n <= QSVB_MAX_QUBITS &&
+  QSVB_REQUIRE((S & 31u) == 31u && P.nlocal >= 7 && P.nlocal <= batch_max_local_bits(dtype) - 2 && n <= QSVB_MAX_QUBITS &&
                    (n >= 64 || (S >> n) == 0),
-               "tile sweep: the local set must hold qubits 0..4 and 7..13 (12 for complex128) qubits of the state");
+               "tile sweep: the local set must hold qubits 0..4 and 7..12 (11 for complex128) qubits of the state");
   bp.local_bits = P.nlocal;
   int pos[64];
   uint32_t nl = 0, nn = 0;
@@ -1236,7 +1423,7 @@ void tile_prepare(Sweep& s, uint32_t n, int dtype) {
   const size_t rsz = dtype == QSVB_C128 ? 8 : 4;
   {
     const size_t co = (P.prog_len * sizeof(Instr) + P.nphase * sizeof(PhaseDev) + 7) & ~size_t(7);
-    P.staged = co + size_t(P.ncoef) * 2 * rsz <= kStageBytes ? 1u : 0u;
+    P.staged = co + size_t(P.ncoef) * 2 * rsz <= kTileStageBytes ? 1u : 0u;
   }
   const size_t off_phase = align16(sizeof(PassDev));
   const size_t off_prog = align16(off_phase + bp.phases.size() * sizeof(PhaseDev));
@@ -1269,9 +1456,9 @@ void launch_tile(const LaunchEnv& e, R* re, R* im, uint32_t n, const Sweep& s, c
   QSVB_REQUIRE(dev_blob != nullptr && !s.tile_blob.empty(), "tile sweep without a program");
   QSVB_REQUIRE(n >= s.tile_lbits, "tile sweep larger than the state");
   const uint8_t* base = static_cast<const uint8_t*>(dev_blob);
-  // two blocks per SM (one streams its tile while the other computes): <= 128 registers a thread
-  if constexpr (sizeof(R) == 8) launch_tile_variant<double, 3, 256, 2>(e, re, im, s, base);
-  else launch_tile_variant<float, 4, 256, 2>(e, re, im, s, base);
+  // four blocks per SM (some stream their tiles while others compute): <= 128 registers a thread
+  if constexpr (sizeof(R) == 8) launch_tile_variant<double, 3, 128, 4, 1>(e, re, im, s, base);
+  else launch_tile_variant<float, 4, 128, 4, 1>(e, re, im, s, base);
 }
 
 template void launch_tile<float>(const LaunchEnv&, float*, float*, uint32_t, const Sweep&, const void*);

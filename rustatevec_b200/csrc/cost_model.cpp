@@ -18,8 +18,9 @@ constexpr double kFp32FmaFlops = 40.0e12;   // CUDA-core complex GEMM, achieved
 constexpr double kFp64FmaFlops = 25.0e12;
 constexpr double kTcFlops = 1.2e15;         // bf16 tcgen05, achieved
 constexpr double kLaunchSeconds = 2.5e-6;
-constexpr double kTileFp32Flops = 22.0e12;  // tile-sweep gate arithmetic, achieved (register tiles)
-constexpr double kTileFp64Flops = 12.0e12;
+constexpr double kTileFp32Flops = 31.0e12;  // tile-sweep gate arithmetic, achieved (register tiles)
+constexpr double kTileFp64Flops = 20.0e12;
+constexpr double kTileMemFactor = 1.25;     // tile fill / write-back against a plain streaming sweep
 
 int lowest_bit(const Sweep& s) {
   uint32_t lo = 64;
@@ -86,7 +87,7 @@ double analytic_sweep_seconds(const Sweep& s, uint32_t n, int dtype) {
   if (s.kind == SK_TILE) {
     // each block loads, updates and stores its tile in turn: memory and arithmetic add up
     const double rate = dtype == QSVB_C128 ? kTileFp64Flops : kTileFp32Flops;
-    return mem + s.tile_flops / rate + kLaunchSeconds;
+    return kTileMemFactor * mem + s.tile_flops / rate + kLaunchSeconds;
   }
   return std::max(mem, comp) + kLaunchSeconds;
 }
