@@ -31,6 +31,8 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
+#include <map>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -53,11 +55,22 @@ constexpr long long kSpinBudget = 1ll << 32;  // clock64 cycles (about 2 s)
 constexpr uint32_t kStageBytes = 32768;       // shared memory for one pass's program
 constexpr uint32_t kTileStageBytes = 16384;   // the same for tile sweeps (four blocks per SM)
 
-enum BatchOp : uint32_t { OP_PHASE = 0, OP_1Q = 1, OP_D1 = 2, OP_CX = 3, OP_2Q = 4, OP_D2 = 5 };
+// OP_D1T: a diagonal on one register bit whose two entries depend on one bit of the tile index
+// (a 2-qubit diagonal with one qubit outside the tile); OP_DT: a phase that depends only on tile
+// bits (a diagonal whose qubits are all outside the tile), applied to every amplitude.
+// OP_D1P / OP_DTP: the same as OP_D1 / OP_DT with coefficients computed once per tile from a
+// phase sum over tile bits (tile sweeps merge runs of diagonal gates into them).
+enum BatchOp : uint32_t {
+  OP_PHASE = 0, OP_1Q = 1, OP_D1 = 2, OP_CX = 3, OP_2Q = 4, OP_D2 = 5, OP_D1T = 6, OP_DT = 7, OP_D1P = 8, OP_DTP = 9
+};
+constexpr uint32_t kTphSlots = 32;  // per-tile phase operations per pass (tile sweeps)
+constexpr uint32_t kTphSlotR = 12;  // reals per slot (the OP_D1 coefficient block of either precision)
 
 struct Instr {
   uint32_t op;
-  uint32_t a, b;  // register bits (1Q/D1: a; CX: a = control, b = target; 2Q/D2: a < b, matrix bit 0 <-> a)
+  uint32_t a, b;  // register bits (1Q/D1/D1T: a; CX: a = control, b = target; 2Q/D2: a < b, matrix bit 0 <->
+                  // a); D1T: b = tile bit; DT: b = tile bit of entry bit 0 | (tile bit of entry bit 1
+                  // << 8) | (number of tile bits << 16)
   uint32_t coef;  // complex index into the coefficient array (OP_PHASE: phase index)
 };
 
@@ -81,6 +94,7 @@ struct PassDev {
   uint64_t zslot;        // first <Z_0> partial slot (last pass)
   uint32_t phase_off, nphase, coef_off, ncoef;  // the pass's phases and coefficients (complex units)
   uint32_t staged;       // program fits the shared-memory staging area
+  uint32_t tph_n, tph_off;  // per-tile phase sums: count and byte offset from this record
 };
 
 struct Item {
@@ -337,9 +351,60 @@ __device__ __forceinline__ void gd2(Regs<R, RB>& v, const R* __restrict__ c) {
 // Applies one instruction to G groups held by this thread (the dispatch and the coefficient loads
 // are shared; the G independent updates interleave).
 template <class R, int RB, int G>
-__device__ __forceinline__ void apply_instr(const Instr& in, Regs<R, RB>* v, const R* __restrict__ coef) {
+__device__ __forceinline__ void apply_instr(const Instr& in, Regs<R, RB>* v, const R* __restrict__ coef, uint32_t tile,
+                                            const R* tcoef) {
   const R* c = coef + 2 * size_t(in.coef);
   switch (in.op) {
+    case OP_D1P: {
+      c = tcoef + kTphSlotR * in.coef;
+      switch (in.a) {
+        case 0: for (int g = 0; g < G; ++g) gd1<0, R, RB>(v[g], c); break;
+        case 1: for (int g = 0; g < G; ++g) gd1<1, R, RB>(v[g], c); break;
+        case 2: for (int g = 0; g < G; ++g) gd1<2, R, RB>(v[g], c); break;
+        case 3: for (int g = 0; g < G; ++g) gd1<3, R, RB>(v[g], c); break;
+        case 4: for (int g = 0; g < G; ++g) gd1<4, R, RB>(v[g], c); break;
+      }
+      break;
+    }
+    case OP_DTP: {
+      c = tcoef + kTphSlotR * in.coef;
+      const R pr = c[0], pi = c[1];
+      for (int g = 0; g < G; ++g)
+#pragma unroll
+        for (int s = 0; s < (1 << RB); ++s) {
+          const R xr = v[g].re(s), xi = v[g].im(s);
+          v[g].re(s) = fma(pr, xr, -pi * xi);
+          v[g].im(s) = fma(pr, xi, pi * xr);
+        }
+      break;
+    }
+    case OP_D1T: {
+      // two coefficient blocks (tile bit 0 / 1) in the layout of OP_D1
+      constexpr int blk = std::is_same<R, float>::value ? 6 : 2;  // complex entries per block
+      c += 2 * blk * ((tile >> in.b) & 1u);
+      switch (in.a) {
+        case 0: for (int g = 0; g < G; ++g) gd1<0, R, RB>(v[g], c); break;
+        case 1: for (int g = 0; g < G; ++g) gd1<1, R, RB>(v[g], c); break;
+        case 2: for (int g = 0; g < G; ++g) gd1<2, R, RB>(v[g], c); break;
+        case 3: for (int g = 0; g < G; ++g) gd1<3, R, RB>(v[g], c); break;
+        case 4: for (int g = 0; g < G; ++g) gd1<4, R, RB>(v[g], c); break;
+      }
+      break;
+    }
+    case OP_DT: {
+      const uint32_t nb = in.b >> 16;
+      uint32_t idx = (tile >> (in.b & 255u)) & 1u;
+      if (nb == 2) idx |= ((tile >> ((in.b >> 8) & 255u)) & 1u) << 1;
+      const R pr = c[2 * idx], pi = c[2 * idx + 1];
+      for (int g = 0; g < G; ++g)
+#pragma unroll
+        for (int s = 0; s < (1 << RB); ++s) {
+          const R xr = v[g].re(s), xi = v[g].im(s);
+          v[g].re(s) = fma(pr, xr, -pi * xi);
+          v[g].im(s) = fma(pr, xi, pi * xr);
+        }
+      break;
+    }
     case OP_1Q:
       switch (in.a) {
         case 0: for (int g = 0; g < G; ++g) g1q<0, R, RB>(v[g], c); break;
@@ -395,7 +460,8 @@ __device__ __forceinline__ void apply_instr(const Instr& in, Regs<R, RB>* v, con
 // tile, apply the phase's instructions, store them back.
 template <class R, int RB, int G>
 __device__ __forceinline__ void phase_groups(const uint32_t* grp, const PhaseDev& D, const uint32_t* rp, R* xr, R* xi,
-                                             const Instr* pprog, uint32_t kbeg, uint32_t kend, const R* pcoef) {
+                                             const Instr* pprog, uint32_t kbeg, uint32_t kend, const R* pcoef,
+                                             uint32_t tile, const R* tcoef) {
   constexpr int NV = 1 << RB;
   const uint32_t r = D.r;
   uint32_t p0[G];
@@ -428,7 +494,7 @@ __device__ __forceinline__ void phase_groups(const uint32_t* grp, const PhaseDev
         v[g].im(s) = xi[off];
       }
   }
-  for (uint32_t kk = kbeg; kk < kend; ++kk) apply_instr<R, RB, G>(pprog[kk], v, pcoef);
+  for (uint32_t kk = kbeg; kk < kend; ++kk) apply_instr<R, RB, G>(pprog[kk], v, pcoef, tile, tcoef);
   if (r == uint32_t(RB)) {
 #pragma unroll
     for (int g = 0; g < G; ++g)
@@ -468,6 +534,8 @@ __global__ void __launch_bounds__(NT, MINB)
   R* xr = reinterpret_cast<R*>(smem_raw);
   R* xi = xr + (size_t(1) << lbits);  // every pass has nlocal <= lbits
   uint8_t* stage = reinterpret_cast<uint8_t*>(xi + (size_t(1) << lbits));  // the pass's program
+  // per-tile phase coefficients (tile sweeps; sits right after the program staging area)
+  R* tcoef = reinterpret_cast<R*>(stage + (fixed ? kTileStageBytes : kStageBytes));
   __shared__ uint64_t s_gaddr[kMaxHi];
   __shared__ uint16_t s_swz[kMaxHi];
   __shared__ uint32_t s_item;
@@ -600,6 +668,57 @@ __global__ void __launch_bounds__(NT, MINB)
     }
     asm volatile("cp.async.wait_all;" ::: "memory");
     __syncthreads();
+    if (P.tph_n) {
+      // phase sums over the tile bits, one slot per operation: D1 blocks (the 0 and 1 sides of a
+      // register bit) or a single complex factor
+      const uint8_t* tb = reinterpret_cast<const uint8_t*>(&P) + P.tph_off;
+      const uint32_t* offs = reinterpret_cast<const uint32_t*>(tb);
+      const double* dd = reinterpret_cast<const double*>(tb + ((4 * P.tph_n + 7) & ~7u));
+      for (uint32_t i = tid; i < P.tph_n; i += NT) {
+        // unit factors multiplied in FP64: no sin/cos per tile
+        const double* d = dd + offs[i];
+        const int type = int(d[0]), m = int(d[5]);
+        double z0r = d[1], z0i = d[2], z1r = d[3], z1i = d[4];
+        for (int t = 0; t < m; ++t) {
+          const double* term = d + 6 + 6 * t;
+          const uint32_t k = uint32_t(term[0]), l = uint32_t(term[1]);
+          if (((item.tile >> k) & (item.tile >> l) & 1u) == 0u) continue;
+          double r = z0r * term[2] - z0i * term[3];
+          z0i = z0r * term[3] + z0i * term[2];
+          z0r = r;
+          if (type == 1) {
+            r = z1r * term[4] - z1i * term[5];
+            z1i = z1r * term[5] + z1i * term[4];
+            z1r = r;
+          }
+        }
+        const double c0 = z0r, s0 = z0i, c1 = z1r, s1 = z1i;
+        R* o = tcoef + kTphSlotR * i;
+        if (type == 2) {
+          o[0] = R(c0);
+          o[1] = R(s0);
+        } else if constexpr (std::is_same<R, float>::value) {
+          const bool j0 = d[6 + 6 * m] != 0.0;  // register bit 0: lanes take the two sides
+          const float v[3][2] = {{float(c0), float(c1)}, {float(s0), float(s1)}, {float(-s0), float(-s1)}};
+          if (j0) {
+            for (int rep = 0; rep < 2; ++rep)
+              for (int e = 0; e < 3; ++e) {
+                o[6 * rep + 2 * e] = v[e][0];
+                o[6 * rep + 2 * e + 1] = v[e][1];
+              }
+          } else {
+            const float w[6] = {float(c0), float(s0), float(-s0), float(c1), float(s1), float(-s1)};
+            for (int e = 0; e < 6; ++e) o[2 * e] = o[2 * e + 1] = w[e];
+          }
+        } else {
+          o[0] = R(c0);
+          o[1] = R(s0);
+          o[2] = R(c1);
+          o[3] = R(s1);
+        }
+      }
+      __syncthreads();
+    }
     if (prof) t_fill += clock64() - t_mark, t_mark = clock64();
     // register phases: each group of 2^r amplitudes (fixed non-register bits) is loaded into one
     // thread's registers, takes all of the phase's gates there, and is written back
@@ -617,12 +736,12 @@ __global__ void __launch_bounds__(NT, MINB)
       if constexpr (GP == 2) {
         for (; grp + NT < ngrp; grp += 2 * NT) {
           const uint32_t gg[2] = {grp, grp + NT};
-          phase_groups<R, RB, 2>(gg, D, rp, xr, xi, pprog, kbeg, kend, pcoef);
+          phase_groups<R, RB, 2>(gg, D, rp, xr, xi, pprog, kbeg, kend, pcoef, item.tile, tcoef);
         }
       }
       for (; grp < ngrp; grp += NT) {
         const uint32_t gg[1] = {grp};
-        phase_groups<R, RB, 1>(gg, D, rp, xr, xi, pprog, kbeg, kend, pcoef);
+        phase_groups<R, RB, 1>(gg, D, rp, xr, xi, pprog, kbeg, kend, pcoef, item.tile, tcoef);
       }
       k = kend;
       __syncthreads();
@@ -704,13 +823,47 @@ struct HostGate {
   std::vector<cd> a;
 };
 
-enum LKind : uint32_t { LK_1Q = OP_1Q, LK_D1 = OP_D1, LK_CX = OP_CX, LK_2Q = OP_2Q, LK_D2 = OP_D2 };
+enum LKind : uint32_t {
+  LK_1Q = OP_1Q, LK_D1 = OP_D1, LK_CX = OP_CX, LK_2Q = OP_2Q, LK_D2 = OP_D2, LK_D1T = OP_D1T, LK_DT = OP_DT,
+  LK_D1P = OP_D1P, LK_DTP = OP_DTP
+};
+
+// A phase sum evaluated once per tile (type 1: the two sides of one local qubit, linear in tile
+// bits; type 2: one factor, quadratic in tile bits). Angles in FP64.
+struct TphOp {
+  int type = 1;
+  double c0 = 0, c1 = 0;
+  std::vector<std::array<double, 3>> terms;  // type 1: (bit, d0, d1); type 2: (bit k, bit l, angle)
+  bool j0 = false;                           // type 1: lives on register bit 0 of its phase
+};
 
 struct LGate {  // a gate on local positions
   uint32_t kind;
   uint32_t p[2];
   const HostGate* g;
+  // LK_D1T: t[0] = tile bit, swapq = the local qubit is the gate's second qubit (entry bit 1);
+  // LK_DT: nt tile bits t[0] (entry bit 0) and t[1] (entry bit 1)
+  uint32_t t[2] = {0, 0};
+  uint32_t nt = 0;
+  bool swapq = false;
 };
+
+uint32_t lgate_mask(const LGate& g) {
+  switch (g.kind) {
+    case LK_1Q:
+    case LK_D1:
+    case LK_D1P:
+    case LK_D1T: return 1u << g.p[0];
+    case LK_DT:
+    case LK_DTP: return 0u;
+    default: return (1u << g.p[0]) | (1u << g.p[1]);
+  }
+}
+
+bool lgate_diag(const LGate& g) {
+  return g.kind == LK_D1 || g.kind == LK_D2 || g.kind == LK_D1T || g.kind == LK_DT || g.kind == LK_D1P ||
+         g.kind == LK_DTP;
+}
 
 std::vector<HostGate> fuse_single_qubit_runs(const qsvb_circuit& c) {
   // consecutive gates on the same single qubit are composed (exactly, in FP64); the rest stays
@@ -780,7 +933,7 @@ void push_coef(BatchPlan& bp, const cd& v) {
 }
 
 // Splits a pass's gates into register phases and appends them to the plan's program.
-void emit_phases(BatchPlan& bp, const std::vector<LGate>& G, uint32_t nlocal) {
+void emit_phases(BatchPlan& bp, const std::vector<LGate>& G, uint32_t nlocal, std::vector<TphOp>* tph = nullptr) {
   // phase and coefficient indices are relative to the pass (its program is staged as one block)
   const size_t phase_base = bp.phases.size(), coef_base = bp.coef.size() / 2;
   const uint32_t rb = std::min(bp.rb, nlocal);
@@ -799,8 +952,8 @@ void emit_phases(BatchPlan& bp, const std::vector<LGate>& G, uint32_t nlocal) {
     for (size_t i = first; i < G.size(); ++i) {
       if (done[i]) continue;
       const LGate& g = G[i];
-      const uint32_t m = (1u << g.p[0]) | (g.kind >= LK_CX ? (1u << g.p[1]) : 0u);
-      const bool diag = g.kind == LK_D1 || g.kind == LK_D2;
+      const uint32_t m = lgate_mask(g);
+      const bool diag = lgate_diag(g);
       if ((m & blocked) == 0 && (diag || (m & dblocked) == 0) && uint32_t(__builtin_popcount(Rm | m)) <= rb) {
         Rm |= m;
         done[i] = 1;
@@ -915,6 +1068,47 @@ void emit_phases(BatchPlan& bp, const std::vector<LGate>& G, uint32_t nlocal) {
         case LK_CX:
           in.b = uint32_t(regbit[g.p[1]]);
           break;
+        case LK_D1T: {
+          in.b = g.t[0];
+          for (uint32_t v = 0; v < 2; ++v) {  // the D1 block for tile bit v
+            const cd p0 = g.swapq ? a[size_t((v) * 5)] : a[size_t((2 * v) * 5)];
+            const cd p1 = g.swapq ? a[size_t((v + 2) * 5)] : a[size_t((1 + 2 * v) * 5)];
+            if (bp.dtype == QSVB_C64) {
+              if (in.a == 0) {
+                for (int rep = 0; rep < 2; ++rep) {
+                  push_coef(bp, cd(p0.real(), p1.real()));
+                  push_coef(bp, cd(p0.imag(), p1.imag()));
+                  push_coef(bp, cd(-p0.imag(), -p1.imag()));
+                }
+              } else {
+                for (const cd& e : {p0, p1}) {
+                  push_coef(bp, cd(e.real(), e.real()));
+                  push_coef(bp, cd(e.imag(), e.imag()));
+                  push_coef(bp, cd(-e.imag(), -e.imag()));
+                }
+              }
+            } else {
+              push_coef(bp, p0);
+              push_coef(bp, p1);
+            }
+          }
+          break;
+        }
+        case LK_D1P:
+          in.coef = g.t[0];
+          (*tph)[g.t[0]].j0 = in.a == 0;
+          break;
+        case LK_DTP:
+          in.a = 0;
+          in.coef = g.t[0];
+          break;
+        case LK_DT: {
+          in.a = 0;
+          in.b = g.t[0] | (g.t[1] << 8) | (g.nt << 16);
+          const size_t d = size_t(1) << g.g->m;
+          for (size_t e = 0; e < d; ++e) push_coef(bp, a[e * d + e]);
+          break;
+        }
         default: {  // LK_2Q / LK_D2: the kernel wants matrix bit 0 on the lower register bit
           const uint32_t ra = uint32_t(regbit[g.p[0]]), rbit = uint32_t(regbit[g.p[1]]);
           const bool swap = ra > rbit;
@@ -1349,7 +1543,7 @@ uint32_t tile_local_bits(int dtype, uint32_t n) {
 namespace {
 uint32_t tile_reg_bits(int dtype) { return dtype == QSVB_C128 ? 3u : 4u; }
 size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
-constexpr size_t kTileSmemMax = (size_t(2) * 4 << 12) + kTileStageBytes;  // equal for both precisions
+constexpr size_t kTileSmemMax = (size_t(2) * 4 << 12) + kTileStageBytes + kTphSlots * kTphSlotR * 8;
 
 template <class R, int RB, int NT, int MINB, int GP>
 void launch_tile_variant(const LaunchEnv& e, R* re, R* im, const Sweep& s, const uint8_t* base) {
@@ -1360,7 +1554,7 @@ void launch_tile_variant(const LaunchEnv& e, R* re, R* im, const Sweep& s, const
     QSVB_CK(cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout,
                                  int(cudaSharedmemCarveoutMaxShared)));
   });
-  const size_t smem = ((size_t(2) * sizeof(R)) << s.tile_lbits) + kTileStageBytes;
+  const size_t smem = ((size_t(2) * sizeof(R)) << s.tile_lbits) + kTileStageBytes + kTphSlots * kTphSlotR * sizeof(R);
   int occ = 0;
   QSVB_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, NT, smem));
   QSVB_REQUIRE(occ >= 1, "tile kernel does not fit on an SM");
@@ -1411,12 +1605,129 @@ void tile_prepare(Sweep& s, uint32_t n, int dtype) {
     hg[i].q[0] = g.q[0];
     hg[i].q[1] = g.m == 2 ? g.q[1] : 0u;
     hg[i].a = g.a;
-    for (uint32_t j = 0; j < g.m; ++j) QSVB_REQUIRE(g.q[j] < n && pos[g.q[j]] >= 0, "tile gate outside the local set");
+    uint32_t nout = 0;
+    for (uint32_t j = 0; j < g.m; ++j) {
+      QSVB_REQUIRE(g.q[j] < n, "tile gate qubit out of range");
+      nout += pos[g.q[j]] < 0;
+    }
     const uint32_t kind = gate_kind(hg[i]);
-    G.push_back(LGate{kind, {uint32_t(pos[g.q[0]]), g.m == 2 ? uint32_t(pos[g.q[1]]) : 0u}, &hg[i]});
-    flops += dim * (kind == LK_1Q ? 16.0 : kind == LK_2Q ? 32.0 : kind == LK_CX ? 0.0 : 6.0);
+    // the tile index bit of a qubit outside the local set
+    auto tbit = [&](uint32_t q) {
+      for (uint32_t j = 0; j < nn; ++j)
+        if (P.nonlocal[j] == q) return j;
+      return 0u;
+    };
+    if (nout == 0) {
+      G.push_back(LGate{kind, {uint32_t(pos[g.q[0]]), g.m == 2 ? uint32_t(pos[g.q[1]]) : 0u}, &hg[i]});
+      flops += dim * (kind == LK_1Q ? 16.0 : kind == LK_2Q ? 32.0 : kind == LK_CX ? 0.0 : 6.0);
+    } else {
+      QSVB_REQUIRE(kind == LK_D1 || kind == LK_D2, "only diagonal gates may reach qubits outside the tile");
+      LGate lg{};
+      lg.g = &hg[i];
+      if (nout == g.m) {  // all qubits outside: a phase fixed per tile
+        lg.kind = LK_DT;
+        lg.nt = g.m;
+        lg.t[0] = tbit(g.q[0]);
+        lg.t[1] = g.m == 2 ? tbit(g.q[1]) : 0u;
+      } else {  // one qubit inside, one outside
+        lg.kind = LK_D1T;
+        lg.swapq = pos[g.q[0]] < 0;
+        const uint32_t qin = lg.swapq ? g.q[1] : g.q[0], qout = lg.swapq ? g.q[0] : g.q[1];
+        lg.p[0] = uint32_t(pos[qin]);
+        lg.t[0] = tbit(qout);
+      }
+      G.push_back(lg);
+      flops += dim * 6.0;
+    }
   }
-  emit_phases(bp, G, P.nlocal);
+  // merge diagonal gates into per-tile phase sums: per local qubit, every diagonal (local or
+  // coupled to tile bits) up to the next non-diagonal gate on that qubit; and every diagonal whose
+  // qubits are all outside the tile (they commute with the whole pass) into one factor in front
+  std::vector<TphOp> tph;
+  {
+    auto unit = [](const cd& z) { return std::abs(std::abs(z) - 1.0) < 1e-12; };
+    std::vector<LGate> out;
+    int open[32];
+    std::fill(open, open + 32, -1);
+    int global = -1;
+    std::vector<std::map<uint32_t, std::array<double, 2>>> lin;  // per type-1 op: bit -> (d0, d1)
+    std::map<std::pair<uint32_t, uint32_t>, double> quad;         // global op: (k, l) -> angle
+    for (const LGate& g : G) {
+      const std::vector<cd>& a = g.g->a;
+      const size_t d = size_t(1) << g.g->m;
+      bool all_unit = true;
+      for (size_t e = 0; e < d; ++e) all_unit = all_unit && unit(a[e * d + e]);
+      const bool room = tph.size() < kTphSlots;
+      if ((g.kind == LK_D1 || g.kind == LK_D1T) && all_unit && (open[g.p[0]] >= 0 || room)) {
+        const uint32_t p = g.p[0];
+        if (open[p] < 0) {
+          open[p] = int(tph.size());
+          tph.push_back(TphOp{});
+          lin.emplace_back();
+          LGate agg{};
+          agg.kind = LK_D1P;
+          agg.p[0] = p;
+          agg.g = g.g;
+          agg.t[0] = uint32_t(open[p]);
+          out.push_back(agg);
+        }
+        TphOp& op = tph[size_t(open[p])];
+        if (g.kind == LK_D1) {
+          op.c0 += std::arg(a[0]);
+          op.c1 += std::arg(a[3]);
+        } else {
+          auto e = [&](int b, int v) { return g.swapq ? a[size_t((v + 2 * b) * 5)] : a[size_t((b + 2 * v) * 5)]; };
+          op.c0 += std::arg(e(0, 0));
+          op.c1 += std::arg(e(1, 0));
+          auto& t = lin[size_t(open[p])][g.t[0]];
+          t[0] += std::arg(e(0, 1)) - std::arg(e(0, 0));
+          t[1] += std::arg(e(1, 1)) - std::arg(e(1, 0));
+        }
+        continue;
+      }
+      if (g.kind == LK_DT && all_unit && (global >= 0 || room)) {
+        if (global < 0) {
+          global = int(tph.size());
+          tph.push_back(TphOp{});
+          tph.back().type = 2;
+          lin.emplace_back();
+        }
+        TphOp& op = tph[size_t(global)];
+        if (g.nt == 1) {
+          op.c0 += std::arg(a[0]);
+          quad[{g.t[0], g.t[0]}] += std::arg(a[3]) - std::arg(a[0]);
+        } else {
+          const double d0 = std::arg(a[0]), d1 = std::arg(a[5]), d2 = std::arg(a[10]), d3 = std::arg(a[15]);
+          op.c0 += d0;
+          quad[{g.t[0], g.t[0]}] += d1 - d0;
+          quad[{g.t[1], g.t[1]}] += d2 - d0;
+          quad[{std::min(g.t[0], g.t[1]), std::max(g.t[0], g.t[1])}] += d3 - d1 - d2 + d0;
+        }
+        continue;
+      }
+      if (!lgate_diag(g)) {
+        for (uint32_t j = 0; j < 32; ++j)
+          if ((lgate_mask(g) >> j) & 1u) open[j] = -1;
+      }
+      out.push_back(g);
+    }
+    for (size_t i = 0; i < tph.size(); ++i) {
+      if (tph[i].type == 1) {
+        for (auto& kv : lin[i]) tph[i].terms.push_back({double(kv.first), kv.second[0], kv.second[1]});
+      } else {
+        for (auto& kv : quad) tph[i].terms.push_back({double(kv.first.first), double(kv.first.second), kv.second});
+      }
+    }
+    if (global >= 0) {
+      LGate agg{};
+      agg.kind = LK_DTP;
+      agg.g = G.front().g;
+      agg.t[0] = uint32_t(global);
+      out.insert(out.begin(), agg);
+    }
+    G.swap(out);
+  }
+  emit_phases(bp, G, P.nlocal, &tph);
   P.prog_len = uint32_t(bp.prog.size());
   P.nphase = uint32_t(bp.phases.size());
   P.ncoef = uint32_t(bp.coef.size() / 2);
@@ -1428,9 +1739,42 @@ void tile_prepare(Sweep& s, uint32_t n, int dtype) {
   const size_t off_phase = align16(sizeof(PassDev));
   const size_t off_prog = align16(off_phase + bp.phases.size() * sizeof(PhaseDev));
   const size_t off_coef = align16(off_prog + bp.prog.size() * sizeof(Instr));
-  const size_t total = off_coef + bp.coef.size() * rsz;
+  const size_t off_tph = align16(off_coef + bp.coef.size() * rsz);
+  std::vector<uint32_t> toffs;
+  std::vector<double> tdat;
+  // per operation: type, the factors of both sides with no tile bit set, the term count, then per
+  // term (tile bit k, tile bit l, factor of side 0, factor of side 1) applied when bits k and l
+  // are set, then the register-bit-0 flag
+  for (const TphOp& op : tph) {
+    toffs.push_back(uint32_t(tdat.size()));
+    tdat.push_back(double(op.type));
+    tdat.push_back(std::cos(op.c0));
+    tdat.push_back(std::sin(op.c0));
+    tdat.push_back(std::cos(op.c1));
+    tdat.push_back(std::sin(op.c1));
+    tdat.push_back(double(op.terms.size()));
+    for (const auto& t : op.terms) {
+      const bool lin = op.type == 1;
+      const double a0 = lin ? t[1] : t[2], a1 = lin ? t[2] : 0.0;
+      tdat.push_back(t[0]);
+      tdat.push_back(lin ? t[0] : t[1]);
+      tdat.push_back(std::cos(a0));
+      tdat.push_back(std::sin(a0));
+      tdat.push_back(std::cos(a1));
+      tdat.push_back(std::sin(a1));
+    }
+    tdat.push_back(op.j0 ? 1.0 : 0.0);
+  }
+  const size_t tph_bytes = tph.empty() ? 0 : ((4 * toffs.size() + 7) & ~size_t(7)) + 8 * tdat.size();
+  P.tph_n = uint32_t(tph.size());
+  P.tph_off = uint32_t(off_tph);
+  const size_t total = off_tph + tph_bytes;
   s.tile_blob.assign(total, 0);
   std::memcpy(s.tile_blob.data(), &P, sizeof(P));
+  if (!tph.empty()) {
+    std::memcpy(s.tile_blob.data() + off_tph, toffs.data(), 4 * toffs.size());
+    std::memcpy(s.tile_blob.data() + off_tph + ((4 * toffs.size() + 7) & ~size_t(7)), tdat.data(), 8 * tdat.size());
+  }
   if (!bp.phases.empty()) std::memcpy(s.tile_blob.data() + off_phase, bp.phases.data(), bp.phases.size() * sizeof(PhaseDev));
   if (!bp.prog.empty()) std::memcpy(s.tile_blob.data() + off_prog, bp.prog.data(), bp.prog.size() * sizeof(Instr));
   for (size_t i = 0; i < bp.coef.size(); ++i) {

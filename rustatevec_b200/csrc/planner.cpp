@@ -314,16 +314,15 @@ std::vector<Sweep> plan_sweeps(const std::vector<Gate>& in, uint32_t n, const qs
   qsvb_plan_opts o = o0;
   if (o.max_fused_qubits == 0) o.max_fused_qubits = 1;
   o.max_fused_qubits = std::min<uint32_t>(o.max_fused_qubits, std::min<uint32_t>(QSVB_MAX_GATE_QUBITS, n));
-  if (o.planner == QSVB_PLAN_TILE) return plan_with(in, n, o, dtype, true, TILE_ALWAYS);
+  // tile passes absorb diagonal runs themselves (per-tile phases outside the local set)
+  if (o.planner == QSVB_PLAN_TILE) return plan_with(in, n, o, dtype, false, TILE_ALWAYS);
   if (o.planner != QSVB_PLAN_LEARNED) return plan_with(in, n, o, dtype, false, TILE_NO);
   // learned: merging long diagonal runs into phase-polynomial sweeps, and running gate runs as
   // tile passes, are candidate choices weighed by predicted time
   std::vector<Sweep> best;
   double best_t = 1e300;
-  for (int c = 0; c < 3; ++c) {
-    std::vector<Sweep> cand = c == 0   ? plan_with(in, n, o, dtype, true, TILE_NO)
-                              : c == 1 ? plan_with(in, n, o, dtype, false, TILE_NO)
-                                       : plan_with(in, n, o, dtype, true, TILE_CHOOSE);
+  for (int c = 0; c < 4; ++c) {
+    std::vector<Sweep> cand = plan_with(in, n, o, dtype, (c & 1) == 0, c < 2 ? TILE_NO : TILE_CHOOSE);
     const double t = predict_plan_seconds(cand, n, dtype);
     if (t < best_t) {
       best_t = t;
@@ -355,9 +354,9 @@ std::vector<Sweep> fused_sweeps(const std::vector<Gate>& seg, uint32_t n, const 
 }
 
 // Tile passes over a run of gates. Each pass takes a local set S (qubits 0..4 plus the qubits of
-// the first pending gates, up to the tile width) and every pending 1- or 2-qubit gate inside S
-// that commutes past the pending gates it skips (disjoint qubits, or both diagonal); wider gates
-// end the run and become fused sweeps. TILE_CHOOSE keeps a pass as a tile sweep only when it is
+// the first pending non-diagonal gates, up to the tile width) and every pending 1- or 2-qubit gate
+// inside S, or diagonal, that commutes past the pending gates it skips (disjoint qubits, or both
+// diagonal); wider gates end the run and become fused sweeps. TILE_CHOOSE keeps a pass as a tile sweep only when it is
 // predicted faster than the fused sweeps of the same gates.
 void tile_segment(const std::vector<Gate>& seg, uint32_t n, const qsvb_plan_opts& o, int dtype, TileMode mode,
                   std::vector<Sweep>& out) {
@@ -376,9 +375,11 @@ void tile_segment(const std::vector<Gate>& seg, uint32_t n, const qsvb_plan_opts
     while (true) {
       while (first < pend.size() && done[first]) ++first;
       if (first == pend.size()) break;
+      // diagonal gates never force a qubit into the tile (outside it their entries are fixed per
+      // tile), so the local set follows the pending non-diagonal gates
       uint64_t S = 31;
       for (size_t i = first; i < pend.size() && uint32_t(__builtin_popcountll(S)) < L; ++i) {
-        if (done[i]) continue;
+        if (done[i] || is_diag(pend[i])) continue;
         const uint64_t m = qmask(pend[i]);
         if (uint32_t(__builtin_popcountll(S | m)) <= L) S |= m;
       }
@@ -391,7 +392,7 @@ void tile_segment(const std::vector<Gate>& seg, uint32_t n, const qsvb_plan_opts
         if (done[i]) continue;
         const uint64_t m = qmask(pend[i]);
         const bool diag = is_diag(pend[i]);
-        if ((m & ~S) == 0 && (m & blocked) == 0 && (diag || (m & dblocked) == 0)) {
+        if ((diag || (m & ~S) == 0) && (m & blocked) == 0 && (diag || (m & dblocked) == 0)) {
           done[i] = 1;
           t.tile_gates.push_back(pend[i]);
         } else if (diag) {

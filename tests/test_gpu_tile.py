@@ -110,3 +110,30 @@ def test_small_states_use_ordinary_sweeps(be):
     got, st = run(be, c)
     assert "tile" not in st["by_kind"]
     assert max_abs_diff(ref_state(c), got) < TOL[be.precision]
+
+
+def test_diagonals_reaching_outside_the_tile(be):
+    """Diagonal gates whose qubits lie outside a pass's local set ride along as per-tile phases:
+    one qubit outside (either gate position), both outside, and 1-qubit phases outside."""
+    import math
+    n = 21
+    c = Circuit(n)
+    rng = np.random.default_rng(8)
+    for layer in range(3):
+        for q in range(n):
+            c.h(q) if (q + layer) % 3 else c.rx(q, 0.3 + q)
+        for _ in range(40):
+            a, b = rng.choice(n, size=2, replace=False)
+            kind = rng.integers(4)
+            if kind == 0:
+                c.cphase(int(a), int(b), float(rng.uniform(0, 2 * math.pi)))
+            elif kind == 1:
+                c.cz(int(a), int(b))
+            elif kind == 2:
+                c.rzz(int(a), int(b), float(rng.uniform(0, 2 * math.pi)))
+            else:
+                c.rz(int(a), float(rng.uniform(0, 2 * math.pi)))
+    psi = random_state(n, 21)
+    got, st = run(be, c, psi0=psi)
+    assert st["by_kind"].get("tile", 0) >= 1
+    assert max_abs_diff(ref_state(c, psi), got) < TOL[be.precision]
