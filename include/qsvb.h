@@ -164,6 +164,12 @@ int qsvb_plan_profile(qsvb_ctx* ctx, qsvb_plan* plan, qsvb_state* st, int reps, 
 int qsvb_fuse(const qsvb_circuit* circuit, const qsvb_plan_opts* opts, qsvb_gate* out_gates,
               size_t* n_out, double* out_mats, size_t out_mats_cap);
 
+/* Plans a circuit on the host without a device (no allocation, no upload): the statistics the
+ * plan would report (sweeps by kind, algorithmic bytes, flops, predicted seconds), e.g. to compare
+ * planners or check a plan before a 137 GB state exists. No trait counterpart. */
+int qsvb_plan_dry_run(const qsvb_circuit* circuit, int dtype, const qsvb_plan_opts* opts,
+                      qsvb_plan_stats* stats);
+
 /* ---------------------------------------------------------------- read-out */
 /* Backend::download (mod.rs:62; lib.rs:218-227): SoA copy into host buffers of the state's
  * precision. */

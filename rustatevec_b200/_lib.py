@@ -104,6 +104,7 @@ SIGNATURES = {
     "qsvb_plan_free": (_i, [_vp, _vp]),
     "qsvb_plan_sweep_info": (_i, [_vp, _sz, C.c_void_p]),
     "qsvb_plan_profile": (_i, [_vp, _vp, _vp, _i, _dp]),
+    "qsvb_plan_dry_run": (_i, [C.POINTER(CircuitS), _i, C.POINTER(PlanOpts), C.POINTER(PlanStats)]),
     "qsvb_fuse": (_i, [C.POINTER(CircuitS), C.POINTER(PlanOpts), C.POINTER(Gate), C.POINTER(_sz), _dp, _sz]),
     "qsvb_download": (_i, [_vp, _vp, _vp, _vp]),
     "qsvb_amplitude": (_i, [_vp, _vp, _u64, _dp]),

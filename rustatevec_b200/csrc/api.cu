@@ -477,6 +477,19 @@ int qsvb_execute(qsvb_ctx* c, qsvb_state* s, const qsvb_circuit* circ, const qsv
   });
 }
 
+int qsvb_plan_dry_run(const qsvb_circuit* circ, int dtype, const qsvb_plan_opts* opts, qsvb_plan_stats* stats) {
+  return guarded([&] {
+    validate_circuit(circ);
+    QSVB_REQUIRE(dtype == QSVB_C64 || dtype == QSVB_C128, "dtype must be QSVB_C64 or QSVB_C128");
+    QSVB_REQUIRE(stats != nullptr, "null output");
+    const qsvb_plan_opts o = opts ? *opts : default_opts();
+    const std::vector<Sweep> sw = plan_sweeps(gates_from_circuit(circ), circ->n_qubits, o, dtype);
+    *stats = qsvb_plan_stats{};
+    stats->n_gates_in = circ->n_gates;
+    sweep_costs(sw, circ->n_qubits, dtype, stats);
+  });
+}
+
 int qsvb_fuse(const qsvb_circuit* circ, const qsvb_plan_opts* opts, qsvb_gate* out_gates, size_t* n_out,
               double* out_mats, size_t cap) {
   return guarded([&] {

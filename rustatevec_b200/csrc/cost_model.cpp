@@ -4,6 +4,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <future>
 #include <mutex>
 
 namespace qsvb {
@@ -152,27 +153,36 @@ void select_engines(std::vector<Sweep>& sw, uint32_t n, const qsvb_plan_opts& o,
 }
 
 std::vector<Gate> learned_fuse(const std::vector<Gate>& seg, uint32_t n, const qsvb_plan_opts& o, int dtype) {
-  std::vector<Gate> best;
-  double best_t = 1e300;
   const uint32_t cap = std::max<uint32_t>(1, o.max_fused_qubits);
-  for (int strategy = 0; strategy < 2; ++strategy) {
-    for (uint32_t k = 1; k <= cap; ++k) {
-      std::vector<Gate> cand = strategy == 0 ? fuse_greedy_public(seg, k) : fuse_window_public(seg, k);
-      std::vector<Sweep> sw;
-      sw.reserve(cand.size());
-      for (const Gate& g : cand) {
-        Sweep s = classify_gate(g);
-        if (s.kind != SK_NONE) sw.push_back(std::move(s));
-      }
-      select_engines(sw, n, o, dtype);
-      const double t = predict_plan_seconds(sw, n, dtype);
-      if (t < best_t) {
-        best_t = t;
-        best = std::move(cand);
-      }
+  // every (strategy, width) candidate is fused, classified and costed independently: on long
+  // segments they run on separate host threads
+  auto candidate = [&](int strategy, uint32_t k, std::vector<Gate>* out) {
+    std::vector<Gate> cand = strategy == 0 ? fuse_greedy_public(seg, k) : fuse_window_public(seg, k);
+    std::vector<Sweep> sw;
+    sw.reserve(cand.size());
+    for (const Gate& g : cand) {
+      Sweep s = classify_gate(g);
+      if (s.kind != SK_NONE) sw.push_back(std::move(s));
     }
+    select_engines(sw, n, o, dtype);
+    *out = std::move(cand);
+    return predict_plan_seconds(sw, n, dtype);
+  };
+  const size_t ncand = 2 * size_t(cap);
+  std::vector<std::vector<Gate>> cands(ncand);
+  std::vector<double> secs(ncand, 1e300);
+  if (seg.size() >= 64) {
+    std::vector<std::future<double>> fut;
+    for (size_t c = 0; c < ncand; ++c)
+      fut.push_back(std::async(std::launch::async, candidate, int(c / cap), uint32_t(c % cap) + 1, &cands[c]));
+    for (size_t c = 0; c < ncand; ++c) secs[c] = fut[c].get();
+  } else {
+    for (size_t c = 0; c < ncand; ++c) secs[c] = candidate(int(c / cap), uint32_t(c % cap) + 1, &cands[c]);
   }
-  return best;
+  size_t best = 0;
+  for (size_t c = 1; c < ncand; ++c)
+    if (secs[c] < secs[best]) best = c;  // ties keep the earlier (greedy, narrower) candidate
+  return std::move(cands[best]);
 }
 
 }  // namespace qsvb

@@ -20,6 +20,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <future>
 #include <numeric>
 
 #include "cost_model.h"
@@ -319,10 +320,16 @@ std::vector<Sweep> plan_sweeps(const std::vector<Gate>& in, uint32_t n, const qs
   if (o.planner != QSVB_PLAN_LEARNED) return plan_with(in, n, o, dtype, false, TILE_NO);
   // learned: merging long diagonal runs into phase-polynomial sweeps, and running gate runs as
   // tile passes, are candidate choices weighed by predicted time
+  // the four candidates are independent: plan them on separate host threads
+  std::vector<std::future<std::vector<Sweep>>> fut;
+  for (int c = 0; c < 4; ++c)
+    fut.push_back(std::async(std::launch::async, [&, c] {
+      return plan_with(in, n, o, dtype, (c & 1) == 0, c < 2 ? TILE_NO : TILE_CHOOSE);
+    }));
   std::vector<Sweep> best;
   double best_t = 1e300;
   for (int c = 0; c < 4; ++c) {
-    std::vector<Sweep> cand = plan_with(in, n, o, dtype, (c & 1) == 0, c < 2 ? TILE_NO : TILE_CHOOSE);
+    std::vector<Sweep> cand = fut[size_t(c)].get();
     const double t = predict_plan_seconds(cand, n, dtype);
     if (t < best_t) {
       best_t = t;

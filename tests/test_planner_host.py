@@ -1,0 +1,59 @@
+"""Planner decisions on the host (no device): qsvb_plan_dry_run plans a circuit exactly as
+qsvb_execute would and reports the sweeps by kind."""
+import ctypes as C
+
+import pytest
+
+from rustatevec_b200 import _lib as L
+from rustatevec_b200 import tuning
+from rustatevec_b200.circuits import brickwork, ghz_chain, qaoa_maxcut, qft, random_circuit
+
+
+def dry(circ, planner, k=4, dtype=L.C64, engine=L.ENGINE_AUTO):
+    st = L.PlanStats()
+    L.check(L.lib().qsvb_plan_dry_run(L.PackedCircuit(circ).ref(), dtype, C.byref(L.make_opts(planner, k, engine)),
+                                      C.byref(st)))
+    return st.to_dict()
+
+
+def test_tile_planner_passes(built):
+    # QFT(32): the Hadamards of blocks of qubits plus every controlled phase (diagonals may reach
+    # outside the tile) in a handful of passes, then the final swaps
+    st = dry(qft(32), L.PLAN_TILE)
+    assert set(st["by_kind"]) == {"tile"} and st["n_sweeps"] <= 8
+    st = dry(ghz_chain(24), L.PLAN_TILE, dtype=L.C128)
+    assert set(st["by_kind"]) == {"tile"} and st["n_sweeps"] <= 4
+    # too small for tiles: ordinary sweeps
+    assert "tile" not in dry(random_circuit(12, 80, 1), L.PLAN_TILE)["by_kind"]
+
+
+def test_wide_gates_stay_fused_sweeps(built):
+    from rustatevec_b200 import DenseGate
+    import numpy as np
+    c = random_circuit(20, 60, 3)
+    c.push(DenseGate(3, np.eye(8, dtype=complex) * 1j), [1, 7, 19])
+    for op in random_circuit(20, 60, 4).ops():
+        c.push(op.gate, op.qubits)
+    st = dry(c, L.PLAN_TILE)
+    assert st["by_kind"].get("tile", 0) >= 2 and sum(v for k, v in st["by_kind"].items() if k != "tile") >= 1
+
+
+def test_learned_planner_choices_with_the_trained_model(built):
+    doc = tuning.load()
+    if doc is None:
+        pytest.skip("no trained model in the tree")
+    try:
+        st = dry(brickwork(30, 20, 0), L.PLAN_LEARNED, 6)
+        assert st["by_kind"].get("dense_tc", 0) >= 40  # k>=5 blocks on tensor cores
+        assert dry(brickwork(30, 20, 0), L.PLAN_LEARNED, 6, engine=L.ENGINE_CUDA_CORE)["by_kind"].get("dense_tc", 0) == 0
+        q = dry(qaoa_maxcut(33, 4, 0), L.PLAN_LEARNED, 6, dtype=L.C128)
+        g = dry(qaoa_maxcut(33, 4, 0), L.PLAN_GREEDY, 4, dtype=L.C128)
+        assert q["predicted_seconds"] < g["predicted_seconds"] and q["n_sweeps"] < g["n_sweeps"]
+    finally:
+        tuning.install(None)
+
+
+def test_dry_run_rejects_bad_input(built):
+    st = L.PlanStats()
+    assert L.lib().qsvb_plan_dry_run(None, 0, None, C.byref(st)) == L.QSVB_E_INVALID
+    assert L.lib().qsvb_plan_dry_run(L.PackedCircuit(qft(4)).ref(), 7, None, C.byref(st)) == L.QSVB_E_INVALID
