@@ -692,6 +692,8 @@ KERNEL_CASES = {
     "tc4": ("f32", lambda n: [("u4", [0, 1, 2, 3])]),
     "tc6": ("f32", lambda n: [("u6", list(range(6)))]),
     "tc6_high": ("f32", lambda n: [("u6", list(range(n - 6, n)))]),
+    "tc6_bit1": ("f32", lambda n: [("u6", [1, 2, 7, 8, 9, 10])]),
+    "tc6_bit0": ("f32", lambda n: [("u6", [0, 3, 4, 8, 9, 12])]),
     "phase15": ("f32", lambda n: [("cz", [i, i + 1]) for i in range(0, n - 1, 2)]),
     "tile_h_all": ("f32", lambda n: [("h", [q]) for q in range(13)]),
     "tile_h_all_c128": ("f64", lambda n: [("h", [q]) for q in range(12)]),

@@ -80,7 +80,8 @@ struct TcParams {
   uint16_t dstlo[64];      // (row << ncb | col) contribution of the low 6 state bits
   uint16_t trow[64];       // address-order tile index of gate row s
   uint16_t tcol[256];      // address-order tile index of column c
-  uint32_t bmode;          // 0: MN-major vector, 1: K-major vector, 2: scalar stores
+  uint32_t bmode;          // 0: MN-major vector, 1: K-major vector, 2: K-major row pairs
+  uint32_t b2_bit0;        // bmode 2: state bit 0 is the gate bit (else state bit 1 is)
   uint32_t tcl[16];        // tcol[q] for q < 16 (uniform; read straight from the parameter bank)
   uint32_t tm_rank;        // > 0: the producer uses one tensor-map TMA per component per tile
   uint32_t tm_start[5];    // first state bit of each tensor dimension
@@ -412,20 +413,30 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_dense(float* __restrict__ 
         const float vr[4] = {xr.x, xr.y, xr.z, xr.w};
         const float vi[4] = {xi.x, xi.y, xi.z, xi.w};
         if (p.bmode == 2) {
+          // exactly one of state bits 0, 1 is a gate bit (the gate's lowest, so row parity): the
+          // four amplitudes are two pairs of adjacent rows (K) in two columns, stored as bf16 pairs
+          const int step = p.b2_bit0 ? 1 : 2;  // element offset of a pair's second row
 #pragma unroll
-          for (int e = 0; e < 4; ++e) {
+          for (int q = 0; q < 2; ++q) {
+            const int e = p.b2_bit0 ? 2 * q : q;
             const uint32_t d = uint32_t(s_dlo[tlo + e]) + s_dhi[thi];
             const uint32_t s = d >> NCB, c = d & CMASK;
             const uint32_t kb = (c >> 6) * KR, cl = c & 63u;
-            const uint32_t o_re = b_mn ? mnmaj_off(kb + s, cl) : kmaj_off(cl, kb + s, 64);
-            const uint32_t o_im = b_mn ? mnmaj_off(kb + M2 + s, cl) : kmaj_off(cl, kb + M2 + s, 64);
-            __nv_bfloat16 h, l;
-            split_bf16(vr[e], h, l);
-            *reinterpret_cast<__nv_bfloat16*>(b_hi + o_re) = h;
-            *reinterpret_cast<__nv_bfloat16*>(b_lo + o_re) = l;
-            split_bf16(vi[e], h, l);
-            *reinterpret_cast<__nv_bfloat16*>(b_hi + o_im) = h;
-            *reinterpret_cast<__nv_bfloat16*>(b_lo + o_im) = l;
+            const uint32_t o_re = kmaj_off(cl, kb + s, 64);
+            const uint32_t o_im = kmaj_off(cl, kb + M2 + s, 64);
+            __nv_bfloat16 h0, l0, h1, l1;
+            split_bf16(vr[e], h0, l0);
+            split_bf16(vr[e + step], h1, l1);
+            *reinterpret_cast<uint32_t*>(b_hi + o_re) =
+                uint32_t(__bfloat16_as_ushort(h0)) | (uint32_t(__bfloat16_as_ushort(h1)) << 16);
+            *reinterpret_cast<uint32_t*>(b_lo + o_re) =
+                uint32_t(__bfloat16_as_ushort(l0)) | (uint32_t(__bfloat16_as_ushort(l1)) << 16);
+            split_bf16(vi[e], h0, l0);
+            split_bf16(vi[e + step], h1, l1);
+            *reinterpret_cast<uint32_t*>(b_hi + o_im) =
+                uint32_t(__bfloat16_as_ushort(h0)) | (uint32_t(__bfloat16_as_ushort(h1)) << 16);
+            *reinterpret_cast<uint32_t*>(b_lo + o_im) =
+                uint32_t(__bfloat16_as_ushort(l0)) | (uint32_t(__bfloat16_as_ushort(l1)) << 16);
           }
         } else {
           // four consecutive columns of row s (MN-major) or four consecutive rows of column c
@@ -736,6 +747,7 @@ static void launch_tc_k(const LaunchEnv& env, float* re, float* im, uint32_t n, 
   const bool low_cols = gate_rank[0] < 0 && gate_rank[1] < 0;
   const bool low_rows = gate_rank[0] == 0 && gate_rank[1] == 1;
   p.bmode = low_cols ? 0u : (low_rows ? 1u : 2u);
+  p.b2_bit0 = gate_rank[0] == 0 ? 1u : 0u;
 
   const uint64_t ntiles = 1ull << (n - kTileBits);
   QSVB_CK(cudaFuncSetAttribute(k_tc_dense<KQ>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kTcSmem)));

@@ -52,7 +52,7 @@ QSETS = {
     "high": lambda n, k: list(range(n - k, n)),           # B MN-major (state bits 0-1 are columns)
     "low": lambda n, k: list(range(k)),                   # B K-major (gate owns bits 0-1)
     "mid": lambda n, k: list(range(3, 3 + k)),
-    "mixed": lambda n, k: [0] + list(range(5, 4 + k)),    # scalar B stores (bit 0 gate, bit 1 column)
+    "mixed": lambda n, k: [0] + list(range(5, 4 + k)),    # B row pairs (bit 0 gate, bit 1 column)
     "mixed2": lambda n, k: [1] + list(range(7, 6 + k)),
     "spread": lambda n, k: [2, 4, 7, 9, 10, 11][:k],
     "unsorted": lambda n, k: list(reversed(range(n - k, n))),
