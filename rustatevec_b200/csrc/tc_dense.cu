@@ -69,7 +69,7 @@ constexpr uint32_t kBBytes = uint32_t(kMmaN) * kMmaK * 2u;    // one of Xhi / Xl
 constexpr uint32_t kIoBytes = kTileAmps * 8u;                 // re [4096] + im [4096] fp32
 constexpr long long kWaitBudget = 1ll << 31;                  // clock64 cycles (~1 s)
 constexpr size_t kTcSmem = 1024 + kBSlots * 2 * size_t(kBBytes) + kIoSlots * size_t(kIoBytes) +
-                           144 + 64 * 8 + 3 * 64 * 2 + 256 * 2;
+                           144 + 64 * 8 + 3 * 64 * 2 + 256 * 2 + 64 * 2;
 
 struct TcParams {
   uint32_t hibits[6];      // tile bits above the 6 lowest state bits (ascending)
@@ -82,6 +82,10 @@ struct TcParams {
   uint16_t tcol[256];      // address-order tile index of column c
   uint32_t bmode;          // 0: MN-major vector, 1: K-major vector, 2: K-major row pairs
   uint32_t b2_bit0;        // bmode 2: state bit 0 is the gate bit (else state bit 1 is)
+  // converter work order: float4 u (u = thread + j * converter threads) covers tile amplitudes
+  // 4 * (tplo[u & 31] | tphi[u >> 5]): a bit permutation chosen on the host so that a warp's
+  // K-major B stores fall in distinct banks (the identity for MN-major tiles)
+  uint16_t tplo[32], tphi[32];
   uint32_t tcl[16];        // tcol[q] for q < 16 (uniform; read straight from the parameter bank)
   uint32_t tm_rank;        // > 0: the producer uses one tensor-map TMA per component per tile
   uint32_t tm_start[5];    // first state bit of each tensor dimension
@@ -278,6 +282,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_dense(float* __restrict__ 
   uint16_t* s_dlo = s_dhi + 64;
   uint16_t* s_trow = s_dlo + 64;
   uint16_t* s_tcol = s_trow + 64;  // 256 entries
+  uint16_t* s_tperm = s_tcol + 256;  // tplo [32] then tphi [32]
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const long long t_start = clock64();
@@ -289,6 +294,10 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_dense(float* __restrict__ 
     s_trow[i] = p.trow[i];
   }
   for (int i = tid; i < 256; i += kTcThreads) s_tcol[i] = p.tcol[i];
+  for (int i = tid; i < 32; i += kTcThreads) {
+    s_tperm[i] = p.tplo[i];
+    s_tperm[32 + i] = p.tphi[i];
+  }
   if (warp == kMmaWarp) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
                  "r"(kTmemCols));
@@ -399,16 +408,19 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_dense(float* __restrict__ 
       // all shared-memory loads first (the B stores below could alias them for the compiler)
       float4 xra[kVC], xia[kVC];
       uint32_t dda[kVC];
+      int tt[kVC];
 #pragma unroll
       for (int j = 0; j < kVC; ++j) {
-        const int t = (tid + j * kCvtThreads) * 4;
+        const uint32_t u = uint32_t(tid + j * kCvtThreads);
+        const int t = int(uint32_t(s_tperm[u & 31u]) | uint32_t(s_tperm[32 + (u >> 5)])) * 4;
+        tt[j] = t;
         xra[j] = *reinterpret_cast<const float4*>(sre + t);
         xia[j] = *reinterpret_cast<const float4*>(sim + t);
         dda[j] = uint32_t(s_dlo[t & 63]) + s_dhi[t >> 6];
       }
 #pragma unroll
       for (int j = 0; j < kVC; ++j) {
-        const int t = (tid + j * kCvtThreads) * 4, tlo = t & 63, thi = t >> 6;
+        const int t = tt[j], tlo = t & 63, thi = t >> 6;
         const float4 xr = xra[j], xi = xia[j];
         const float vr[4] = {xr.x, xr.y, xr.z, xr.w};
         const float vi[4] = {xi.x, xi.y, xi.z, xi.w};
@@ -748,6 +760,60 @@ static void launch_tc_k(const LaunchEnv& env, float* re, float* im, uint32_t n, 
   const bool low_rows = gate_rank[0] == 0 && gate_rank[1] == 1;
   p.bmode = low_cols ? 0u : (low_rows ? 1u : 2u);
   p.b2_bit0 = gate_rank[0] == 0 ? 1u : 0u;
+  {
+    // converter work order: float4 index bits 0..2 stay (a quarter-warp's 16-byte loads stay
+    // conflict-free); for K-major tiles the lane bits 3 and 4 take the two float4 bits that make
+    // the warp's B stores hit the most distinct banks (found by trying every pair)
+    constexpr uint32_t CM = (1u << NCB) - 1u;
+    constexpr uint32_t KRr = 2u * M2;
+    auto perm_t4 = [](uint32_t u, const int (&pi)[10]) {
+      uint32_t t4 = 0;
+      for (int i = 0; i < 10; ++i)
+        if ((u >> i) & 1u) t4 |= 1u << pi[i];
+      return t4;
+    };
+    auto conflict = [&](const int (&pi)[10]) {
+      int worst = 0;
+      const int nst = p.bmode == 2 ? 2 : 1;
+      for (int q = 0; q < nst; ++q) {
+        int count[32] = {0};
+        for (uint32_t lane = 0; lane < 32; ++lane) {
+          const uint32_t t = perm_t4(lane, pi) * 4u;
+          const uint32_t e = p.bmode == 2 ? (p.b2_bit0 ? 2u * q : uint32_t(q)) : 0u;
+          const uint32_t tl = t + e;
+          const uint32_t d = uint32_t(p.dstlo[tl & 63u]) + p.dsthi[tl >> 6];
+          const uint32_t sr = d >> NCB, c = d & CM;
+          const uint32_t off = kmaj_off(c & 63u, (c >> 6) * KRr + sr, 64);
+          // 4-byte stores: 32 banks per warp; 8-byte stores: 16 bank pairs per half-warp
+          const uint32_t bank = p.bmode == 2 ? (off >> 2) & 31u : ((off >> 3) & 15u) + 16u * (lane >> 4);
+          worst = std::max(worst, ++count[bank]);
+        }
+      }
+      return worst;
+    };
+    int best[10];
+    for (int i = 0; i < 10; ++i) best[i] = i;
+    if (p.bmode != 0) {
+      int best_c = conflict(best);
+      for (int a = 3; a < 10; ++a)
+        for (int b = 3; b < 10; ++b) {
+          if (a == b) continue;
+          int pi[10] = {0, 1, 2, a, b, 0, 0, 0, 0, 0};
+          int nxt = 5;
+          for (int v = 3; v < 10; ++v)
+            if (v != a && v != b) pi[nxt++] = v;
+          const int cc = conflict(pi);
+          if (cc < best_c) {
+            best_c = cc;
+            std::copy(pi, pi + 10, best);
+          }
+        }
+    }
+    for (uint32_t u = 0; u < 32; ++u) {
+      p.tplo[u] = uint16_t(perm_t4(u, best));
+      p.tphi[u] = uint16_t(perm_t4(u << 5, best));
+    }
+  }
 
   const uint64_t ntiles = 1ull << (n - kTileBits);
   QSVB_CK(cudaFuncSetAttribute(k_tc_dense<KQ>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kTcSmem)));
