@@ -180,6 +180,8 @@ class PackedCircuit:
         self.struct = CircuitS(circuit.n_qubits(), n, C.cast(self.gates, C.POINTER(Gate)))
 
     def ref(self):
+        """By-reference argument for the C calls. The struct points into this object's gate array
+        and matrix buffer: keep the PackedCircuit alive until the call returns."""
         return C.byref(self.struct)
 
 
@@ -219,6 +221,7 @@ class PackedBatch:
         self.n_qubits = np.array([c.n_qubits() for c in circuits], dtype=np.int64)
 
     def ptr(self):
+        """Pointer argument for the C calls; keep the PackedBatch alive until the call returns."""
         return C.cast(self.circs.ctypes.data, C.POINTER(CircuitS))
 
 

@@ -6,6 +6,8 @@
 
 #include <algorithm>
 #include <cstring>
+#include <thread>
+#include <cstring>
 #include <memory>
 #include <new>
 #include <string>
@@ -239,6 +241,10 @@ int qsvb_destroy(qsvb_ctx* c) {
     if (c->d_mat_ring) cudaFree(c->d_mat_ring);
     if (c->d_prob) cudaFree(c->d_prob);
     if (c->d_err) cudaFree(c->d_err);
+    for (int i = 0; i < 2; ++i) {
+      if (c->h_pin[i]) cudaFreeHost(c->h_pin[i]);
+      if (c->pin_ev[i]) cudaEventDestroy(c->pin_ev[i]);
+    }
     cudaStreamDestroy(c->stream);
     delete c;
   });
@@ -557,6 +563,60 @@ int qsvb_amplitude(qsvb_ctx* c, const qsvb_state* s, uint64_t index, double out[
   });
 }
 
+}  // extern "C"
+
+namespace qsvb {
+namespace {
+void ensure_pinned(qsvb_ctx* c) {
+  for (int i = 0; i < 2; ++i) {
+    if (!c->h_pin[i]) QSVB_CK(cudaHostAlloc(&c->h_pin[i], kPinChunk, cudaHostAllocDefault));
+    if (!c->pin_ev[i]) QSVB_CK(cudaEventCreateWithFlags(&c->pin_ev[i], cudaEventDisableTiming));
+  }
+}
+
+// host copy of one staged chunk, split over a few threads (one thread moves ~10 GB/s)
+void host_copy(void* dst, const void* src, size_t bytes) {
+  constexpr int kThreads = 4;
+  if (bytes < (size_t(4) << 20)) {
+    std::memcpy(dst, src, bytes);
+    return;
+  }
+  std::thread th[kThreads - 1];
+  const size_t part = (bytes / kThreads + 63) & ~size_t(63);
+  for (int t = 1; t < kThreads; ++t) {
+    const size_t off = std::min(bytes, part * t), len = std::min(bytes - off, part);
+    th[t - 1] = std::thread([=] { std::memcpy(static_cast<char*>(dst) + off, static_cast<const char*>(src) + off, len); });
+  }
+  std::memcpy(dst, src, std::min(bytes, part));
+  for (auto& t : th) t.join();
+}
+}  // namespace
+
+void d2h_staged(qsvb_ctx* c, void* dst, const void* src, size_t bytes) {
+  if (bytes <= (size_t(4) << 20)) {
+    QSVB_CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, c->stream));
+    QSVB_CK(cudaStreamSynchronize(c->stream));
+    return;
+  }
+  ensure_pinned(c);
+  const size_t n = (bytes + kPinChunk - 1) / kPinChunk;
+  auto issue = [&](size_t k) {
+    const size_t off = k * kPinChunk, len = std::min(kPinChunk, bytes - off);
+    QSVB_CK(cudaMemcpyAsync(c->h_pin[k & 1], static_cast<const char*>(src) + off, len, cudaMemcpyDeviceToHost,
+                            c->stream));
+    QSVB_CK(cudaEventRecord(c->pin_ev[k & 1], c->stream));
+  };
+  issue(0);
+  for (size_t k = 0; k < n; ++k) {
+    if (k + 1 < n) issue(k + 1);  // its buffer held chunk k-1, copied out in the previous step
+    QSVB_CK(cudaEventSynchronize(c->pin_ev[k & 1]));
+    const size_t off = k * kPinChunk;
+    host_copy(static_cast<char*>(dst) + off, c->h_pin[k & 1], std::min(kPinChunk, bytes - off));
+  }
+}
+}  // namespace qsvb
+
+extern "C" {
 int qsvb_probabilities(qsvb_ctx* c, const qsvb_state* s, void* out, int out_dtype) {
   return guarded([&] {
     check_state(c, s);
@@ -565,25 +625,36 @@ int qsvb_probabilities(qsvb_ctx* c, const qsvb_state* s, void* out, int out_dtyp
     DeviceGuard dg(c->device);
     const uint64_t dim = uint64_t(1) << s->n_qubits;
     const size_t esz = out_dtype == QSVB_C128 ? 8 : 4;
-    const uint64_t chunk = std::min<uint64_t>(dim, uint64_t(1) << 25);
+    // chunks of one pinned buffer: chunk k is computed and crosses PCIe while the host copies
+    // chunk k-1 into `out`
+    const uint64_t chunk = std::min<uint64_t>(dim, kPinChunk / esz);
     if (c->prob_cap < chunk * esz) {
       QSVB_CK(cudaStreamSynchronize(c->stream));
       if (c->d_prob) QSVB_CK(cudaFree(c->d_prob));
       c->d_prob = nullptr;
-      QSVB_CK(cudaMalloc(&c->d_prob, chunk * 8));
-      c->prob_cap = chunk * 8;
+      QSVB_CK(cudaMalloc(&c->d_prob, chunk * esz));
+      c->prob_cap = chunk * esz;
     }
-    for (uint64_t off = 0; off < dim; off += chunk) {
-      const uint64_t cnt = std::min(chunk, dim - off);
-      by_dtype(s->dtype, [&](auto r) {
-        using R = decltype(r);
-        launch_probabilities<R>(c->env(), static_cast<const R*>(s->re), static_cast<const R*>(s->im), off, cnt,
-                                c->d_prob, out_dtype == QSVB_C128);
-      });
-      QSVB_CK(cudaMemcpyAsync(static_cast<char*>(out) + off * esz, c->d_prob, cnt * esz, cudaMemcpyDeviceToHost,
-                              c->stream));
-      QSVB_CK(cudaStreamSynchronize(c->stream));
+    ensure_pinned(c);
+    const uint64_t nchunk = (dim + chunk - 1) / chunk;
+    for (uint64_t k = 0; k <= nchunk; ++k) {
+      if (k < nchunk) {
+        const uint64_t off = k * chunk, cnt = std::min(chunk, dim - off);
+        by_dtype(s->dtype, [&](auto r) {
+          using R = decltype(r);
+          launch_probabilities<R>(c->env(), static_cast<const R*>(s->re), static_cast<const R*>(s->im), off, cnt,
+                                  c->d_prob, out_dtype == QSVB_C128);
+        });
+        QSVB_CK(cudaMemcpyAsync(c->h_pin[k & 1], c->d_prob, cnt * esz, cudaMemcpyDeviceToHost, c->stream));
+        QSVB_CK(cudaEventRecord(c->pin_ev[k & 1], c->stream));
+      }
+      if (k >= 1) {
+        const uint64_t j = k - 1, off = j * chunk, cnt = std::min(chunk, dim - off);
+        QSVB_CK(cudaEventSynchronize(c->pin_ev[j & 1]));
+        host_copy(static_cast<char*>(out) + off * esz, c->h_pin[j & 1], cnt * esz);
+      }
     }
+    sync_and_check(c);
   });
 }
 

@@ -1467,10 +1467,10 @@ void batch_run(qsvb_ctx* c, qsvb_batch* b, double* z0_out, double* probs_out, co
       for (size_t i = 0; i < bp.ncirc; ++i)
         QSVB_CK(cudaMemcpyAsync(probs_out + probs_offset[i], b->d_probs + bp.prob_off[i],
                                 (size_t(1) << bp.nq[i]) * 8, cudaMemcpyDeviceToHost, s));
+      QSVB_CK(cudaStreamSynchronize(s));
     } else {
-      QSVB_CK(cudaMemcpyAsync(probs_out, b->d_probs, bp.prob_total * 8, cudaMemcpyDeviceToHost, s));
+      d2h_staged(c, probs_out, b->d_probs, bp.prob_total * 8);
     }
-    QSVB_CK(cudaStreamSynchronize(s));
   }
   if (b->d_prof) {
     std::vector<long long> h(5 * size_t(b->grid));

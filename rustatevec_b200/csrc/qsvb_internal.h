@@ -160,8 +160,19 @@ struct qsvb_ctx {
   void* d_prob = nullptr;         // probability staging chunk
   size_t prob_cap = 0;
   int* d_err = nullptr;           // device error flag (bounded waits)
+  void* h_pin[2] = {nullptr, nullptr};      // pinned host ring for large device -> host copies
+  cudaEvent_t pin_ev[2] = {nullptr, nullptr};
   qsvb::LaunchEnv env() const { return {stream, num_sms, d_err}; }
 };
+
+namespace qsvb {
+// Large device -> host copy through the context's pinned ring: chunk k+1 crosses PCIe while the
+// host copies chunk k into `dst` (pageable). `produce(k, off, len, dev_dst)` may enqueue work that
+// fills a device chunk first (it returns the device pointer to copy from); pass nullptr to copy
+// straight from `src`.
+constexpr size_t kPinChunk = size_t(32) << 20;
+void d2h_staged(qsvb_ctx* c, void* dst, const void* src, size_t bytes);
+}  // namespace qsvb
 
 void run_batch(qsvb_ctx* c, const qsvb_circuit* circuits, size_t n_circuits, int dtype, uint32_t local_qubits,
                uint32_t register_qubits, double* z0_out, double* probs_out, const uint64_t* probs_offset,

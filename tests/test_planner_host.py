@@ -11,8 +11,8 @@ from rustatevec_b200.circuits import brickwork, ghz_chain, qaoa_maxcut, qft, ran
 
 def dry(circ, planner, k=4, dtype=L.C64, engine=L.ENGINE_AUTO):
     st = L.PlanStats()
-    L.check(L.lib().qsvb_plan_dry_run(L.PackedCircuit(circ).ref(), dtype, C.byref(L.make_opts(planner, k, engine)),
-                                      C.byref(st)))
+    pc = L.PackedCircuit(circ)  # owns the gate structs and matrices for the duration of the call
+    L.check(L.lib().qsvb_plan_dry_run(pc.ref(), dtype, C.byref(L.make_opts(planner, k, engine)), C.byref(st)))
     return st.to_dict()
 
 
@@ -56,4 +56,5 @@ def test_learned_planner_choices_with_the_trained_model(built):
 def test_dry_run_rejects_bad_input(built):
     st = L.PlanStats()
     assert L.lib().qsvb_plan_dry_run(None, 0, None, C.byref(st)) == L.QSVB_E_INVALID
-    assert L.lib().qsvb_plan_dry_run(L.PackedCircuit(qft(4)).ref(), 7, None, C.byref(st)) == L.QSVB_E_INVALID
+    pc = L.PackedCircuit(qft(4))
+    assert L.lib().qsvb_plan_dry_run(pc.ref(), 7, None, C.byref(st)) == L.QSVB_E_INVALID
