@@ -61,7 +61,8 @@ constexpr uint32_t kTileStageBytes = 16384;   // the same for tile sweeps (four 
 // OP_D1P / OP_DTP: the same as OP_D1 / OP_DT with coefficients computed once per tile from a
 // phase sum over tile bits (tile sweeps merge runs of diagonal gates into them).
 enum BatchOp : uint32_t {
-  OP_PHASE = 0, OP_1Q = 1, OP_D1 = 2, OP_CX = 3, OP_2Q = 4, OP_D2 = 5, OP_D1T = 6, OP_DT = 7, OP_D1P = 8, OP_DTP = 9
+  OP_PHASE = 0, OP_1Q = 1, OP_D1 = 2, OP_CX = 3, OP_2Q = 4, OP_D2 = 5, OP_D1T = 6, OP_DT = 7, OP_D1P = 8, OP_DTP = 9,
+  OP_DTAB = 10  // the product of a phase's diagonal gates: one factor per register slot
 };
 constexpr uint32_t kTphSlots = 32;  // per-tile phase operations per pass (tile sweeps)
 constexpr uint32_t kTphSlotR = 12;  // reals per slot (the OP_D1 coefficient block of either precision)
@@ -336,6 +337,31 @@ __device__ __forceinline__ void gd2(Regs<R, RB>& v, const R* __restrict__ c) {
   }
 }
 
+// One factor per register slot (a phase's diagonal gates multiplied out on the host). complex64:
+// per float2 pair h the factors of slots 2h and 2h+1 as (re), (im), (-im) pairs; complex128: one
+// complex per slot.
+template <class R, int RB>
+__device__ __forceinline__ void gtab(Regs<R, RB>& v, const R* __restrict__ c) {
+  if constexpr (std::is_same<R, float>::value) {
+    const float2* cc = reinterpret_cast<const float2*>(c);
+#pragma unroll
+    for (int h = 0; h < (1 << RB) / 2; ++h) {
+      const float2 pr = cc[3 * h], pi = cc[3 * h + 1], npi = cc[3 * h + 2];
+      const float2 xr = v.r[h], xi = v.i[h];
+      v.r[h] = __ffma2_rn(pr, xr, __fmul2_rn(npi, xi));
+      v.i[h] = __ffma2_rn(pr, xi, __fmul2_rn(pi, xr));
+    }
+  } else {
+#pragma unroll
+    for (int s = 0; s < (1 << RB); ++s) {
+      const R pr = c[2 * s], pi = c[2 * s + 1];
+      const R xr = v.re(s), xi = v.im(s);
+      v.re(s) = fma(pr, xr, -pi * xi);
+      v.im(s) = fma(pr, xi, pi * xr);
+    }
+  }
+}
+
 #define QSVB_PAIR_CASES(F, ...)                       \
   case 0 * 8 + 1: F<0, 1, R, RB>(__VA_ARGS__); break; \
   case 0 * 8 + 2: F<0, 2, R, RB>(__VA_ARGS__); break; \
@@ -355,6 +381,9 @@ __device__ __forceinline__ void apply_instr(const Instr& in, Regs<R, RB>* v, con
                                             const R* tcoef) {
   const R* c = coef + 2 * size_t(in.coef);
   switch (in.op) {
+    case OP_DTAB:
+      for (int g = 0; g < G; ++g) gtab<R, RB>(v[g], c);
+      break;
     case OP_D1P: {
       c = tcoef + kTphSlotR * in.coef;
       switch (in.a) {
@@ -1024,11 +1053,66 @@ void emit_phases(BatchPlan& bp, const std::vector<LGate>& G, uint32_t nlocal, st
       D.lo[g] = uint16_t(lo);
       D.hi[g] = uint16_t(hi);
     }
-    D.ninstr = uint32_t(taken.size());
+    const size_t phase_idx = bp.phases.size(), phase_pc = bp.prog.size();
     bp.prog.push_back(Instr{OP_PHASE, 0, 0, uint32_t(bp.phases.size() - phase_base)});
     bp.phases.push_back(D);
+    // diagonal gates on register bits (LK_D1, LK_D2) are multiplied into a table that sits at the
+    // first of them; a later one joins it unless a non-diagonal gate on one of its bits came in
+    // between (it would have to move past that gate)
+    const uint32_t nslot = 1u << bp.rb;
+    std::vector<cd> table;
+    size_t table_coef = 0;  // complex index of the open table's coefficients
+    uint32_t nd_since = 0;  // register bits touched by non-diagonal gates since the table opened
+    bool open_table = false;
+    auto close_table = [&] {
+      if (!open_table) return;
+      if (bp.dtype == QSVB_C64) {
+        for (uint32_t h = 0; h < nslot / 2; ++h) {
+          const cd a0 = table[2 * h], a1 = table[2 * h + 1];
+          bp.coef[2 * (table_coef + 3 * h)] = a0.real();
+          bp.coef[2 * (table_coef + 3 * h) + 1] = a1.real();
+          bp.coef[2 * (table_coef + 3 * h + 1)] = a0.imag();
+          bp.coef[2 * (table_coef + 3 * h + 1) + 1] = a1.imag();
+          bp.coef[2 * (table_coef + 3 * h + 2)] = -a0.imag();
+          bp.coef[2 * (table_coef + 3 * h + 2) + 1] = -a1.imag();
+        }
+      } else {
+        for (uint32_t s2 = 0; s2 < nslot; ++s2) {
+          bp.coef[2 * (table_coef + s2)] = table[s2].real();
+          bp.coef[2 * (table_coef + s2) + 1] = table[s2].imag();
+        }
+      }
+      open_table = false;
+    };
     for (size_t i : taken) {
       const LGate& g = G[i];
+      if (g.kind == LK_D1 || g.kind == LK_D2) {
+        const uint32_t rb0 = uint32_t(regbit[g.p[0]]), rb1 = g.kind == LK_D2 ? uint32_t(regbit[g.p[1]]) : 0u;
+        const uint32_t m = (1u << rb0) | (g.kind == LK_D2 ? (1u << rb1) : 0u);
+        if (!open_table || (m & nd_since) != 0) {
+          close_table();
+          open_table = true;
+          nd_since = 0;
+          table.assign(nslot, cd(1, 0));
+          table_coef = bp.coef.size() / 2;
+          const size_t slots = bp.dtype == QSVB_C64 ? size_t(3) * nslot / 2 : nslot;
+          bp.coef.resize(bp.coef.size() + 2 * slots, 0.0);
+          bp.prog.push_back(Instr{OP_DTAB, 0, 0, uint32_t(table_coef - coef_base)});
+        }
+        const std::vector<cd>& a = g.g->a;
+        const size_t d = size_t(1) << g.g->m;
+        for (uint32_t s2 = 0; s2 < nslot; ++s2) {
+          size_t e = (s2 >> rb0) & 1u;
+          if (g.kind == LK_D2) e |= size_t((s2 >> rb1) & 1u) << 1;
+          table[s2] *= a[e * d + e];
+        }
+        continue;
+      }
+      if (!lgate_diag(g)) {
+        const uint32_t lm = lgate_mask(g);
+        for (uint32_t p = 0; p < nlocal; ++p)
+          if (((lm >> p) & 1u) && regbit[p] >= 0) nd_since |= 1u << regbit[p];
+      }
       Instr in{g.kind, uint32_t(regbit[g.p[0]]), 0, uint32_t(bp.coef.size() / 2 - coef_base)};
       const std::vector<cd>& a = g.g->a;
       switch (g.kind) {
@@ -1126,6 +1210,8 @@ void emit_phases(BatchPlan& bp, const std::vector<LGate>& G, uint32_t nlocal, st
       }
       bp.prog.push_back(in);
     }
+    close_table();
+    bp.phases[phase_idx].ninstr = uint32_t(bp.prog.size() - phase_pc - 1);
   }
 }
 
