@@ -62,7 +62,8 @@ constexpr uint32_t kTileStageBytes = 16384;   // the same for tile sweeps (four 
 // phase sum over tile bits (tile sweeps merge runs of diagonal gates into them).
 enum BatchOp : uint32_t {
   OP_PHASE = 0, OP_1Q = 1, OP_D1 = 2, OP_CX = 3, OP_2Q = 4, OP_D2 = 5, OP_D1T = 6, OP_DT = 7, OP_D1P = 8, OP_DTP = 9,
-  OP_DTAB = 10  // the product of a phase's diagonal gates: one factor per register slot
+  OP_DTAB = 10,  // the product of a phase's diagonal gates: one factor per register slot
+  OP_1QR = 11    // a real rotation [[C, -S], [S, C]] (the middle factor of a 1-qubit gate)
 };
 constexpr uint32_t kTphSlots = 32;  // per-tile phase operations per pass (tile sweeps)
 constexpr uint32_t kTphSlotR = 12;  // reals per slot (the OP_D1 coefficient block of either precision)
@@ -337,6 +338,51 @@ __device__ __forceinline__ void gd2(Regs<R, RB>& v, const R* __restrict__ c) {
   }
 }
 
+// Real rotation [[C, -S], [S, C]] on register bit J: complex64 coefficients (C, C), (S, S), (-S, -S)
+// as float2 pairs; complex128 (C, S).
+template <int J, class R, int RB>
+__device__ __forceinline__ void g1qr(Regs<R, RB>& v, const R* __restrict__ c) {
+  if constexpr (J < RB) {
+    if constexpr (std::is_same<R, float>::value) {
+      const float2* cc = reinterpret_cast<const float2*>(c);
+      if constexpr (J >= 1) {
+        constexpr int HJ = 1 << (J - 1);
+        const float2 Cc = cc[0], Sc = cc[1], NS = cc[2];
+#pragma unroll
+        for (int h = 0; h < (1 << RB) / 2; ++h) {
+          if (h & HJ) continue;
+          const int t = h | HJ;
+          const float2 xr0 = v.r[h], xi0 = v.i[h], xr1 = v.r[t], xi1 = v.i[t];
+          v.r[h] = __ffma2_rn(NS, xr1, __fmul2_rn(Cc, xr0));
+          v.i[h] = __ffma2_rn(NS, xi1, __fmul2_rn(Cc, xi0));
+          v.r[t] = __ffma2_rn(Cc, xr1, __fmul2_rn(Sc, xr0));
+          v.i[t] = __ffma2_rn(Cc, xi1, __fmul2_rn(Sc, xi0));
+        }
+      } else {
+        const float Cs = cc[0].x, Ss = cc[1].x;
+#pragma unroll
+        for (int h = 0; h < (1 << RB) / 2; ++h) {
+          const float xr0 = v.r[h].x, xi0 = v.i[h].x, xr1 = v.r[h].y, xi1 = v.i[h].y;
+          v.r[h] = make_float2(fmaf(-Ss, xr1, Cs * xr0), fmaf(Cs, xr1, Ss * xr0));
+          v.i[h] = make_float2(fmaf(-Ss, xi1, Cs * xi0), fmaf(Cs, xi1, Ss * xi0));
+        }
+      }
+    } else {
+      const R Cs = c[0], Ss = c[1];
+#pragma unroll
+      for (int s = 0; s < (1 << RB); ++s) {
+        if (s & (1 << J)) continue;
+        const int t = s | (1 << J);
+        const R xr0 = v.re(s), xi0 = v.im(s), xr1 = v.re(t), xi1 = v.im(t);
+        v.re(s) = fma(-Ss, xr1, Cs * xr0);
+        v.im(s) = fma(-Ss, xi1, Cs * xi0);
+        v.re(t) = fma(Cs, xr1, Ss * xr0);
+        v.im(t) = fma(Cs, xi1, Ss * xi0);
+      }
+    }
+  }
+}
+
 // One factor per register slot (a phase's diagonal gates multiplied out on the host). complex64:
 // per float2 pair h the factors of slots 2h and 2h+1 as (re), (im), (-im) pairs; complex128: one
 // complex per slot.
@@ -383,6 +429,15 @@ __device__ __forceinline__ void apply_instr(const Instr& in, Regs<R, RB>* v, con
   switch (in.op) {
     case OP_DTAB:
       for (int g = 0; g < G; ++g) gtab<R, RB>(v[g], c);
+      break;
+    case OP_1QR:
+      switch (in.a) {
+        case 0: for (int g = 0; g < G; ++g) g1qr<0, R, RB>(v[g], c); break;
+        case 1: for (int g = 0; g < G; ++g) g1qr<1, R, RB>(v[g], c); break;
+        case 2: for (int g = 0; g < G; ++g) g1qr<2, R, RB>(v[g], c); break;
+        case 3: for (int g = 0; g < G; ++g) g1qr<3, R, RB>(v[g], c); break;
+        case 4: for (int g = 0; g < G; ++g) g1qr<4, R, RB>(v[g], c); break;
+      }
       break;
     case OP_D1P: {
       c = tcoef + kTphSlotR * in.coef;
@@ -961,6 +1016,34 @@ void push_coef(BatchPlan& bp, const cd& v) {
   bp.coef.push_back(v.imag());
 }
 
+// A unitary 2x2 as Dl R Dr: Dl = diag(l0, l1), R = [[C, -S], [S, C]] with C, S >= 0, Dr =
+// diag(1, r1). False when the matrix is not of that form to 1e-12 (then it stays a general gate).
+bool real_rotation(const std::vector<cd>& a, cd& l0, cd& l1, cd& r1, double& C, double& S) {
+  const cd u00 = a[0], u01 = a[1], u10 = a[2], u11 = a[3];
+  C = std::abs(u00);
+  S = std::abs(u10);
+  constexpr double tol = 1e-14;
+  if (C > tol && S > tol) {
+    l0 = u00 / C;
+    l1 = u10 / S;
+    r1 = u11 / (l1 * C);
+  } else if (S > tol) {  // off-diagonal: u00 = u11 = 0
+    l1 = u10 / S;
+    r1 = cd(1, 0);
+    l0 = -u01 / S;
+  } else if (C > tol) {  // diagonal
+    l0 = u00 / C;
+    r1 = cd(1, 0);
+    l1 = u11 / C;
+  } else {
+    return false;
+  }
+  const double err = std::max({std::abs(l0 * C - u00), std::abs(-l0 * S * r1 - u01), std::abs(l1 * S - u10),
+                               std::abs(l1 * C * r1 - u11), std::abs(std::abs(l0) - 1.0), std::abs(std::abs(l1) - 1.0),
+                               std::abs(std::abs(r1) - 1.0)});
+  return err <= 1e-12;
+}
+
 // Splits a pass's gates into register phases and appends them to the plan's program.
 void emit_phases(BatchPlan& bp, const std::vector<LGate>& G, uint32_t nlocal, std::vector<TphOp>* tph = nullptr) {
   // phase and coefficient indices are relative to the pass (its program is staged as one block)
@@ -1056,109 +1139,145 @@ void emit_phases(BatchPlan& bp, const std::vector<LGate>& G, uint32_t nlocal, st
     const size_t phase_idx = bp.phases.size(), phase_pc = bp.prog.size();
     bp.prog.push_back(Instr{OP_PHASE, 0, 0, uint32_t(bp.phases.size() - phase_base)});
     bp.phases.push_back(D);
-    // diagonal gates on register bits (LK_D1, LK_D2) are multiplied into a table that sits at the
-    // first of them; a later one joins it unless a non-diagonal gate on one of its bits came in
-    // between (it would have to move past that gate)
+    // Emission. Non-diagonal operations keep their order (1-qubit real rotations as OP_1QR).
+    // Diagonal factors on register bits (LK_D1, LK_D2) are multiplied into per-slot tables: a factor
+    // may sit anywhere between the last non-diagonal operation on its bits before it and the first
+    // one after it, and the tables go where the fewest points cover every factor's range (interval
+    // stabbing, ends first).
     const uint32_t nslot = 1u << bp.rb;
-    std::vector<cd> table;
-    size_t table_coef = 0;  // complex index of the open table's coefficients
-    uint32_t nd_since = 0;  // register bits touched by non-diagonal gates since the table opened
-    bool open_table = false;
-    auto close_table = [&] {
-      if (!open_table) return;
-      if (bp.dtype == QSVB_C64) {
-        for (uint32_t h = 0; h < nslot / 2; ++h) {
-          const cd a0 = table[2 * h], a1 = table[2 * h + 1];
-          bp.coef[2 * (table_coef + 3 * h)] = a0.real();
-          bp.coef[2 * (table_coef + 3 * h) + 1] = a1.real();
-          bp.coef[2 * (table_coef + 3 * h + 1)] = a0.imag();
-          bp.coef[2 * (table_coef + 3 * h + 1) + 1] = a1.imag();
-          bp.coef[2 * (table_coef + 3 * h + 2)] = -a0.imag();
-          bp.coef[2 * (table_coef + 3 * h + 2) + 1] = -a1.imag();
-        }
-      } else {
-        for (uint32_t s2 = 0; s2 < nslot; ++s2) {
-          bp.coef[2 * (table_coef + s2)] = table[s2].real();
-          bp.coef[2 * (table_coef + s2) + 1] = table[s2].imag();
-        }
+    struct Op {
+      const LGate* g;  // nullptr: a real rotation (kind LK_1QR) on register bit rbit
+      uint32_t rbit;
+      double C, S;
+    };
+    struct Fac {
+      uint32_t rb0, rb1, nb;  // register bits (nb = 1 or 2)
+      cd d[4];                // diagonal entries, index bit 0 <-> rb0, bit 1 <-> rb1
+      size_t lo, hi;          // allowed slots: before ops[j], lo <= j <= hi
+    };
+    std::vector<Op> ops;
+    std::vector<Fac> facs;
+    int last_nd[8] = {-1, -1, -1, -1, -1, -1, -1, -1};  // per register bit: last non-diagonal op
+    std::vector<size_t> open_facs;                      // factors whose upper end is not known yet
+    auto add_fac = [&](uint32_t rb0, uint32_t rb1, uint32_t nb, const cd* d) {
+      Fac f{};
+      f.rb0 = rb0;
+      f.rb1 = rb1;
+      f.nb = nb;
+      for (uint32_t e = 0; e < (1u << nb); ++e) f.d[e] = d[e];
+      int lo = last_nd[rb0];
+      if (nb == 2) lo = std::max(lo, last_nd[rb1]);
+      f.lo = size_t(lo + 1);
+      f.hi = SIZE_MAX;
+      open_facs.push_back(facs.size());
+      facs.push_back(f);
+    };
+    auto add_nondiag = [&](const Op& op, uint32_t bits) {
+      const size_t idx = ops.size();
+      ops.push_back(op);
+      for (size_t fi : open_facs) {
+        Fac& f = facs[fi];
+        const uint32_t fm = (1u << f.rb0) | (f.nb == 2 ? (1u << f.rb1) : 0u);
+        if (f.hi == SIZE_MAX && (fm & bits)) f.hi = idx;
       }
-      open_table = false;
+      for (uint32_t b = 0; b < 8; ++b)
+        if ((bits >> b) & 1u) last_nd[b] = int(idx);
     };
     for (size_t i : taken) {
       const LGate& g = G[i];
-      if (g.kind == LK_D1 || g.kind == LK_D2) {
-        const uint32_t rb0 = uint32_t(regbit[g.p[0]]), rb1 = g.kind == LK_D2 ? uint32_t(regbit[g.p[1]]) : 0u;
-        const uint32_t m = (1u << rb0) | (g.kind == LK_D2 ? (1u << rb1) : 0u);
-        if (!open_table || (m & nd_since) != 0) {
-          close_table();
-          open_table = true;
-          nd_since = 0;
-          table.assign(nslot, cd(1, 0));
-          table_coef = bp.coef.size() / 2;
-          const size_t slots = bp.dtype == QSVB_C64 ? size_t(3) * nslot / 2 : nslot;
-          bp.coef.resize(bp.coef.size() + 2 * slots, 0.0);
-          bp.prog.push_back(Instr{OP_DTAB, 0, 0, uint32_t(table_coef - coef_base)});
-        }
-        const std::vector<cd>& a = g.g->a;
-        const size_t d = size_t(1) << g.g->m;
-        for (uint32_t s2 = 0; s2 < nslot; ++s2) {
-          size_t e = (s2 >> rb0) & 1u;
-          if (g.kind == LK_D2) e |= size_t((s2 >> rb1) & 1u) << 1;
-          table[s2] *= a[e * d + e];
-        }
+      const std::vector<cd>& a = g.g->a;
+      if (g.kind == LK_D1) {
+        const cd d[2] = {a[0], a[3]};
+        add_fac(uint32_t(regbit[g.p[0]]), 0, 1, d);
         continue;
       }
+      if (g.kind == LK_D2) {
+        const cd d[4] = {a[0], a[5], a[10], a[15]};
+        add_fac(uint32_t(regbit[g.p[0]]), uint32_t(regbit[g.p[1]]), 2, d);
+        continue;
+      }
+      if (g.kind == LK_1Q) {
+        // a real rotation (Dl = Dr = identity, e.g. RY) costs half a general 1-qubit gate; with
+        // phase factors the extra table work measured more than it saved, so those stay general
+        cd l0, l1, r1;
+        double C, S;
+        if (real_rotation(a, l0, l1, r1, C, S) && std::abs(l0 - 1.0) + std::abs(l1 - 1.0) + std::abs(r1 - 1.0) < 1e-15) {
+          const uint32_t rbit = uint32_t(regbit[g.p[0]]);
+          add_nondiag(Op{nullptr, rbit, C, S}, 1u << rbit);
+          continue;
+        }
+      }
+      uint32_t bits = 0;
       if (!lgate_diag(g)) {
         const uint32_t lm = lgate_mask(g);
         for (uint32_t p = 0; p < nlocal; ++p)
-          if (((lm >> p) & 1u) && regbit[p] >= 0) nd_since |= 1u << regbit[p];
+          if (((lm >> p) & 1u) && regbit[p] >= 0) bits |= 1u << regbit[p];
       }
-      Instr in{g.kind, uint32_t(regbit[g.p[0]]), 0, uint32_t(bp.coef.size() / 2 - coef_base)};
-      const std::vector<cd>& a = g.g->a;
-      switch (g.kind) {
-        case LK_1Q:
-          if (bp.dtype == QSVB_C64) {  // pre-broadcast pairs (re, re), (im, im), (-im, -im) per entry
-            for (int k = 0; k < 4; ++k) {
-              const cd e = a[size_t(k)];
-              push_coef(bp, cd(e.real(), e.real()));
-              push_coef(bp, cd(e.imag(), e.imag()));
-              push_coef(bp, cd(-e.imag(), -e.imag()));
-            }
-          } else {
-            for (int k = 0; k < 4; ++k) push_coef(bp, a[size_t(k)]);
-          }
-          break;
-        case LK_D1:
-          if (bp.dtype == QSVB_C64) {
-            const cd p0 = a[0], p1 = a[3];
-            if (in.a == 0) {  // lanes of a float2 pair are the two sides of the gate's bit
-              for (int rep = 0; rep < 2; ++rep) {
-                push_coef(bp, cd(p0.real(), p1.real()));
-                push_coef(bp, cd(p0.imag(), p1.imag()));
-                push_coef(bp, cd(-p0.imag(), -p1.imag()));
-              }
-            } else {
-              for (const cd& e : {p0, p1}) {
+      add_nondiag(Op{&g, 0, 0, 0}, bits);  // diagonal kinds outside tables constrain nothing
+    }
+    for (Fac& f : facs)
+      if (f.hi == SIZE_MAX) f.hi = ops.size();
+    std::vector<size_t> order(facs.size());
+    std::iota(order.begin(), order.end(), size_t(0));
+    std::stable_sort(order.begin(), order.end(), [&](size_t x, size_t y) { return facs[x].hi < facs[y].hi; });
+    std::vector<std::vector<cd>> tables(ops.size() + 1);
+    size_t point = SIZE_MAX;
+    for (size_t fi : order) {
+      const Fac& f = facs[fi];
+      if (point == SIZE_MAX || point < f.lo) point = f.hi;
+      std::vector<cd>& t = tables[point];
+      if (t.empty()) t.assign(nslot, cd(1, 0));
+      for (uint32_t s2 = 0; s2 < nslot; ++s2) {
+        size_t e = (s2 >> f.rb0) & 1u;
+        if (f.nb == 2) e |= size_t((s2 >> f.rb1) & 1u) << 1;
+        t[s2] *= f.d[e];
+      }
+    }
+    auto emit_table = [&](const std::vector<cd>& t) {
+      const size_t base = bp.coef.size() / 2;
+      if (bp.dtype == QSVB_C64) {
+        for (uint32_t h = 0; h < nslot / 2; ++h) {
+          const cd a0 = t[2 * h], a1 = t[2 * h + 1];
+          push_coef(bp, cd(a0.real(), a1.real()));
+          push_coef(bp, cd(a0.imag(), a1.imag()));
+          push_coef(bp, cd(-a0.imag(), -a1.imag()));
+        }
+      } else {
+        for (uint32_t s2 = 0; s2 < nslot; ++s2) push_coef(bp, t[s2]);
+      }
+      bp.prog.push_back(Instr{OP_DTAB, 0, 0, uint32_t(base - coef_base)});
+    };
+    auto emit_rotation = [&](const Op& op) {
+      Instr in{OP_1QR, op.rbit, 0, uint32_t(bp.coef.size() / 2 - coef_base)};
+      if (bp.dtype == QSVB_C64) {  // pre-broadcast (C, C), (S, S), (-S, -S)
+        push_coef(bp, cd(op.C, op.C));
+        push_coef(bp, cd(op.S, op.S));
+        push_coef(bp, cd(-op.S, -op.S));
+      } else {
+        push_coef(bp, cd(op.C, op.S));
+      }
+      bp.prog.push_back(in);
+    };
+    auto emit_one = [&](const LGate& g) {
+        Instr in{g.kind, uint32_t(regbit[g.p[0]]), 0, uint32_t(bp.coef.size() / 2 - coef_base)};
+        const std::vector<cd>& a = g.g->a;
+        switch (g.kind) {
+          case LK_1Q:
+            if (bp.dtype == QSVB_C64) {  // pre-broadcast pairs (re, re), (im, im), (-im, -im) per entry
+              for (int k = 0; k < 4; ++k) {
+                const cd e = a[size_t(k)];
                 push_coef(bp, cd(e.real(), e.real()));
                 push_coef(bp, cd(e.imag(), e.imag()));
                 push_coef(bp, cd(-e.imag(), -e.imag()));
               }
+            } else {
+              for (int k = 0; k < 4; ++k) push_coef(bp, a[size_t(k)]);
             }
-          } else {
-            push_coef(bp, a[0]);
-            push_coef(bp, a[3]);
-          }
-          break;
-        case LK_CX:
-          in.b = uint32_t(regbit[g.p[1]]);
-          break;
-        case LK_D1T: {
-          in.b = g.t[0];
-          for (uint32_t v = 0; v < 2; ++v) {  // the D1 block for tile bit v
-            const cd p0 = g.swapq ? a[size_t((v) * 5)] : a[size_t((2 * v) * 5)];
-            const cd p1 = g.swapq ? a[size_t((v + 2) * 5)] : a[size_t((1 + 2 * v) * 5)];
+            break;
+          case LK_D1:
             if (bp.dtype == QSVB_C64) {
-              if (in.a == 0) {
+              const cd p0 = a[0], p1 = a[3];
+              if (in.a == 0) {  // lanes of a float2 pair are the two sides of the gate's bit
                 for (int rep = 0; rep < 2; ++rep) {
                   push_coef(bp, cd(p0.real(), p1.real()));
                   push_coef(bp, cd(p0.imag(), p1.imag()));
@@ -1172,45 +1291,82 @@ void emit_phases(BatchPlan& bp, const std::vector<LGate>& G, uint32_t nlocal, st
                 }
               }
             } else {
-              push_coef(bp, p0);
-              push_coef(bp, p1);
+              push_coef(bp, a[0]);
+              push_coef(bp, a[3]);
             }
+            break;
+          case LK_CX:
+            in.b = uint32_t(regbit[g.p[1]]);
+            break;
+          case LK_D1T: {
+            in.b = g.t[0];
+            for (uint32_t v = 0; v < 2; ++v) {  // the D1 block for tile bit v
+              const cd p0 = g.swapq ? a[size_t((v) * 5)] : a[size_t((2 * v) * 5)];
+              const cd p1 = g.swapq ? a[size_t((v + 2) * 5)] : a[size_t((1 + 2 * v) * 5)];
+              if (bp.dtype == QSVB_C64) {
+                if (in.a == 0) {
+                  for (int rep = 0; rep < 2; ++rep) {
+                    push_coef(bp, cd(p0.real(), p1.real()));
+                    push_coef(bp, cd(p0.imag(), p1.imag()));
+                    push_coef(bp, cd(-p0.imag(), -p1.imag()));
+                  }
+                } else {
+                  for (const cd& e : {p0, p1}) {
+                    push_coef(bp, cd(e.real(), e.real()));
+                    push_coef(bp, cd(e.imag(), e.imag()));
+                    push_coef(bp, cd(-e.imag(), -e.imag()));
+                  }
+                }
+              } else {
+                push_coef(bp, p0);
+                push_coef(bp, p1);
+              }
+            }
+            break;
           }
-          break;
-        }
-        case LK_D1P:
-          in.coef = g.t[0];
-          (*tph)[g.t[0]].j0 = in.a == 0;
-          break;
-        case LK_DTP:
-          in.a = 0;
-          in.coef = g.t[0];
-          break;
-        case LK_DT: {
-          in.a = 0;
-          in.b = g.t[0] | (g.t[1] << 8) | (g.nt << 16);
-          const size_t d = size_t(1) << g.g->m;
-          for (size_t e = 0; e < d; ++e) push_coef(bp, a[e * d + e]);
-          break;
-        }
-        default: {  // LK_2Q / LK_D2: the kernel wants matrix bit 0 on the lower register bit
-          const uint32_t ra = uint32_t(regbit[g.p[0]]), rbit = uint32_t(regbit[g.p[1]]);
-          const bool swap = ra > rbit;
-          in.a = std::min(ra, rbit);
-          in.b = std::max(ra, rbit);
-          auto perm = [&](int s) { return swap ? (((s & 1) << 1) | ((s >> 1) & 1)) : s; };
-          if (g.kind == LK_2Q) {
-            for (int r = 0; r < 4; ++r)
-              for (int c = 0; c < 4; ++c) push_coef(bp, a[size_t(perm(r) * 4 + perm(c))]);
-          } else {
-            for (int r = 0; r < 4; ++r) push_coef(bp, a[size_t(perm(r) * 4 + perm(r))]);
+          case LK_D1P:
+            in.coef = g.t[0];
+            (*tph)[g.t[0]].j0 = in.a == 0;
+            break;
+          case LK_DTP:
+            in.a = 0;
+            in.coef = g.t[0];
+            break;
+          case LK_DT: {
+            in.a = 0;
+            in.b = g.t[0] | (g.t[1] << 8) | (g.nt << 16);
+            const size_t d = size_t(1) << g.g->m;
+            for (size_t e = 0; e < d; ++e) push_coef(bp, a[e * d + e]);
+            break;
           }
-          break;
+          default: {  // LK_2Q / LK_D2: the kernel wants matrix bit 0 on the lower register bit
+            const uint32_t ra = uint32_t(regbit[g.p[0]]), rbit = uint32_t(regbit[g.p[1]]);
+            const bool swap = ra > rbit;
+            in.a = std::min(ra, rbit);
+            in.b = std::max(ra, rbit);
+            auto perm = [&](int s) { return swap ? (((s & 1) << 1) | ((s >> 1) & 1)) : s; };
+            if (g.kind == LK_2Q) {
+              for (int r = 0; r < 4; ++r)
+                for (int c = 0; c < 4; ++c) push_coef(bp, a[size_t(perm(r) * 4 + perm(c))]);
+            } else {
+              for (int r = 0; r < 4; ++r) push_coef(bp, a[size_t(perm(r) * 4 + perm(r))]);
+            }
+            break;
+          }
         }
-      }
-      bp.prog.push_back(in);
+        bp.prog.push_back(in);
+    };
+    auto identity = [](const std::vector<cd>& t) {
+      for (const cd& z : t)
+        if (z != cd(1, 0)) return false;
+      return true;
+    };
+    for (size_t j = 0; j <= ops.size(); ++j) {
+      if (!tables[j].empty() && !identity(tables[j])) emit_table(tables[j]);
+      if (j == ops.size()) break;
+      if (ops[j].g) emit_one(*ops[j].g);
+      else emit_rotation(ops[j]);
     }
-    close_table();
     bp.phases[phase_idx].ninstr = uint32_t(bp.prog.size() - phase_pc - 1);
   }
 }

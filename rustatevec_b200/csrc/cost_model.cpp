@@ -20,7 +20,7 @@ constexpr double kFp64FmaFlops = 25.0e12;
 constexpr double kTcFlops = 1.2e15;         // bf16 tcgen05, achieved
 constexpr double kLaunchSeconds = 2.5e-6;
 constexpr double kTileFp32Flops = 31.0e12;  // tile-sweep gate arithmetic, achieved (register tiles)
-constexpr double kTileFp64Flops = 20.0e12;
+constexpr double kTileFp64Flops = 13.0e12;
 constexpr double kTileMemFactor = 1.25;     // tile fill / write-back against a plain streaming sweep
 
 int lowest_bit(const Sweep& s) {
