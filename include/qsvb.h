@@ -181,6 +181,11 @@ int qsvb_amplitude(qsvb_ctx* ctx, const qsvb_state* st, uint64_t index, double o
 int qsvb_probabilities(qsvb_ctx* ctx, const qsvb_state* st, void* out, int out_dtype);
 /* Backend::expectation_z (mod.rs:57-59; sample.rs:177-200), FP64 on device. */
 int qsvb_expectation_z(qsvb_ctx* ctx, const qsvb_state* st, uint64_t mask, double* out);
+/* `shots` measurement outcomes drawn on the device (no probability download): shot k returns the
+ * outcome whose FP64 cumulative-probability interval holds u_k * total, u_k the k-th unit() value
+ * of SplitMix64(seed) (crates/qsv-core/src/circuits.rs:22-46). Same distribution as the trait's
+ * sample (crates/qsv-core/src/sample.rs:84-97, alias method), not the same draws. shots <= 2^30. */
+int qsvb_sample(qsvb_ctx* ctx, const qsvb_state* st, uint64_t shots, uint64_t seed, uint64_t* out);
 /* StateVector::norm_sqr (crates/qsv-core/src/state/mod.rs:112-118), FP64 on device. */
 int qsvb_norm_sqr(qsvb_ctx* ctx, const qsvb_state* st, double* out);
 /* <a|b> in FP64 (no trait counterpart). a and b may differ in precision (complex64 vs complex128),

@@ -110,6 +110,7 @@ SIGNATURES = {
     "qsvb_amplitude": (_i, [_vp, _vp, _u64, _dp]),
     "qsvb_probabilities": (_i, [_vp, _vp, _vp, _i]),
     "qsvb_expectation_z": (_i, [_vp, _vp, _u64, _dp]),
+    "qsvb_sample": (_i, [_vp, _vp, _u64, _u64, C.POINTER(_u64)]),
     "qsvb_norm_sqr": (_i, [_vp, _vp, _dp]),
     "qsvb_inner_product": (_i, [_vp, _vp, _vp, _dp]),
     "qsvb_fidelity": (_i, [_vp, _vp, _vp, _dp]),

@@ -142,6 +142,14 @@ class B200Backend:
         from .sample import alias_sample
         return alias_sample(self.probabilities(state, fp64=True), shots, rng)
 
+    def sample_device(self, state: DeviceState, shots: int, seed: int) -> np.ndarray:
+        """``shots`` outcomes drawn on the device by inverse-CDF sampling (qsvb_sample): shot k uses
+        the k-th ``unit()`` of ``SplitMix64(seed)``; no probability download."""
+        out = np.empty(shots, dtype=np.uint64)
+        L.check(L.lib().qsvb_sample(self.ctx, state.handle, shots, seed,
+                                    out.ctypes.data_as(C.POINTER(C.c_uint64))))
+        return out
+
     def expectation_z(self, state: DeviceState, mask: int) -> float:
         out = C.c_double()
         L.check(L.lib().qsvb_expectation_z(self.ctx, state.handle, mask, C.byref(out)))

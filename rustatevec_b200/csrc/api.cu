@@ -658,6 +658,14 @@ int qsvb_probabilities(qsvb_ctx* c, const qsvb_state* s, void* out, int out_dtyp
   });
 }
 
+int qsvb_sample(qsvb_ctx* c, const qsvb_state* s, uint64_t shots, uint64_t seed, uint64_t* out) {
+  return guarded([&] {
+    check_state(c, s);
+    DeviceGuard dg(c->device);
+    sample_shots(c, s, shots, seed, out);
+  });
+}
+
 int qsvb_expectation_z(qsvb_ctx* c, const qsvb_state* s, uint64_t mask, double* out) {
   return guarded([&] {
     check_state(c, s);

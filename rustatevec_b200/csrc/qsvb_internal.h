@@ -172,6 +172,7 @@ namespace qsvb {
 // straight from `src`.
 constexpr size_t kPinChunk = size_t(32) << 20;
 void d2h_staged(qsvb_ctx* c, void* dst, const void* src, size_t bytes);
+void sample_shots(qsvb_ctx* c, const qsvb_state* st, uint64_t shots, uint64_t seed, uint64_t* out);
 }  // namespace qsvb
 
 void run_batch(qsvb_ctx* c, const qsvb_circuit* circuits, size_t n_circuits, int dtype, uint32_t local_qubits,
