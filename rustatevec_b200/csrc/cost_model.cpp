@@ -119,10 +119,54 @@ float mlp_forward_host(const MlpModel& m, const float* feat) {
   return y * m.y_scale + m.y_mean;
 }
 
+namespace {
+// Largest state the installed model has seen (its records span 22..30 qubits). A ReLU network
+// extrapolates linearly in its inputs, which for larger states put some predictions below the
+// memory floor; larger states are predicted as the same sweep on a kModelMaxQubits state times
+// the amplitude ratio.
+constexpr uint32_t kModelMaxQubits = 30;
+
+// The sweep with d = n - kModelMaxQubits state bits removed: the d highest bits >= 12 that no
+// qubit of the sweep uses, the others renumbered below them (low bits, which set the access
+// pattern, keep their positions).
+Sweep shrink_sweep(const Sweep& s, uint32_t n) {
+  const uint32_t d = n - kModelMaxQubits;
+  bool used[64] = {false};
+  for (uint32_t j = 0; j < s.m; ++j) used[s.q[j]] = true;
+  for (uint32_t j = 0; j < s.nctrl; ++j) used[s.ctrl[j]] = true;
+  if (s.kind == SK_1Q || s.kind == SK_CTRL) used[s.target] = true;
+  bool drop[64] = {false};
+  uint32_t dropped = 0;
+  for (int b = int(n) - 1; b >= 12 && dropped < d; --b)
+    if (!used[b]) drop[b] = true, ++dropped;
+  uint32_t to[64];
+  for (uint32_t b = 0, below = 0; b < n; ++b) {
+    to[b] = b - below;
+    below += drop[b];
+  }
+  Sweep t;
+  t.kind = s.kind;
+  t.m = s.m;
+  t.target = to[s.target];
+  t.nctrl = s.nctrl;
+  for (uint32_t j = 0; j < 6; ++j) {
+    t.q[j] = j < s.m ? to[s.q[j]] : 0;
+    t.ctrl[j] = j < s.nctrl ? to[s.ctrl[j]] : 0;
+  }
+  t.terms.resize(s.terms.size());
+  t.n_gates = s.n_gates;
+  return t;
+}
+}  // namespace
+
 double predict_sweep_seconds(const Sweep& s, uint32_t n, int dtype) {
   const MlpModel& m = g_model;
   if (m.hidden > 0 && s.kind != SK_TILE) {  // the model has not been trained on tile sweeps
     float f[kNumFeatures];
+    if (n > kModelMaxQubits && n - kModelMaxQubits <= 20) {
+      sweep_features(shrink_sweep(s, n), kModelMaxQubits, dtype, f);
+      return std::ldexp(std::exp2(double(mlp_forward_host(m, f))), int(n - kModelMaxQubits));
+    }
     sweep_features(s, n, dtype, f);
     return std::exp2(double(mlp_forward_host(m, f)));
   }
