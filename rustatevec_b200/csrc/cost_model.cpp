@@ -3,15 +3,19 @@
 #include "cost_model.h"
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
+#include <cstring>
 #include <future>
 #include <mutex>
+#include <unordered_map>
 
 namespace qsvb {
 
 namespace {
 std::mutex g_model_mu;
 MlpModel g_model;
+std::atomic<uint64_t> g_model_generation{0};  // bumped by install_model; keys the prediction memo
 
 // Roofline constants for one B200 (measured copy bandwidth ~6.5 TB/s; sustained fractions).
 constexpr double kHbmBytesPerSec = 6.0e12;
@@ -98,11 +102,23 @@ const MlpModel& installed_model() { return g_model; }
 void install_model(const MlpModel& m) {
   std::lock_guard<std::mutex> lk(g_model_mu);
   g_model = m;
+  g_model_generation.fetch_add(1);
 }
 
 float mlp_forward_host(const MlpModel& m, const float* feat) {
   const int H = m.hidden;
-  std::vector<float> x(kNumFeatures), h1(H), h2(H);
+  constexpr int kStackH = 128;  // widest model the trainer accepts
+  float xs[kNumFeatures], h1s[kStackH], h2s[kStackH];
+  std::vector<float> h1v, h2v;
+  float* x = xs;
+  float* h1 = h1s;
+  float* h2 = h2s;
+  if (H > kStackH) {
+    h1v.resize(H);
+    h2v.resize(H);
+    h1 = h1v.data();
+    h2 = h2v.data();
+  }
   for (int i = 0; i < kNumFeatures; ++i) x[i] = (feat[i] - m.mean[i]) * m.scale[i];
   for (int j = 0; j < H; ++j) {
     float a = m.b1[j];
@@ -120,6 +136,38 @@ float mlp_forward_host(const MlpModel& m, const float* feat) {
 }
 
 namespace {
+// The planner predicts the same sweeps many times (the same shapes recur across layers and
+// fusion candidates): each thread memoises predictions by feature vector for the installed model.
+struct FeatKey {
+  float f[kNumFeatures];
+  bool operator==(const FeatKey& o) const { return std::memcmp(f, o.f, sizeof(f)) == 0; }
+};
+struct FeatHash {
+  size_t operator()(const FeatKey& k) const {
+    uint64_t h = 1469598103934665603ull;
+    const unsigned char* p = reinterpret_cast<const unsigned char*>(k.f);
+    for (size_t i = 0; i < sizeof(k.f); ++i) h = (h ^ p[i]) * 1099511628211ull;
+    return size_t(h);
+  }
+};
+
+float mlp_forward_host_memo(const MlpModel& m, const float* feat) {
+  thread_local std::unordered_map<FeatKey, float, FeatHash> memo;
+  thread_local uint64_t memo_gen = ~uint64_t(0);
+  const uint64_t gen = g_model_generation.load();
+  if (gen != memo_gen || memo.size() > (1u << 16)) {
+    memo.clear();
+    memo_gen = gen;
+  }
+  FeatKey k;
+  std::memcpy(k.f, feat, sizeof(k.f));
+  auto it = memo.find(k);
+  if (it != memo.end()) return it->second;
+  const float y = mlp_forward_host(m, feat);
+  memo.emplace(k, y);
+  return y;
+}
+
 // Largest state the installed model has seen (its records span 22..30 qubits). A ReLU network
 // extrapolates linearly in its inputs, which for larger states put some predictions below the
 // memory floor; larger states are predicted as the same sweep on a kModelMaxQubits state times
@@ -165,10 +213,10 @@ double predict_sweep_seconds(const Sweep& s, uint32_t n, int dtype) {
     float f[kNumFeatures];
     if (n > kModelMaxQubits && n - kModelMaxQubits <= 20) {
       sweep_features(shrink_sweep(s, n), kModelMaxQubits, dtype, f);
-      return std::ldexp(std::exp2(double(mlp_forward_host(m, f))), int(n - kModelMaxQubits));
+      return std::ldexp(std::exp2(double(mlp_forward_host_memo(m, f))), int(n - kModelMaxQubits));
     }
     sweep_features(s, n, dtype, f);
-    return std::exp2(double(mlp_forward_host(m, f)));
+    return std::exp2(double(mlp_forward_host_memo(m, f)));
   }
   return analytic_sweep_seconds(s, n, dtype);
 }
@@ -198,35 +246,44 @@ void select_engines(std::vector<Sweep>& sw, uint32_t n, const qsvb_plan_opts& o,
 
 std::vector<Gate> learned_fuse(const std::vector<Gate>& seg, uint32_t n, const qsvb_plan_opts& o, int dtype) {
   const uint32_t cap = std::max<uint32_t>(1, o.max_fused_qubits);
-  // every (strategy, width) candidate is fused, classified and costed independently: on long
-  // segments they run on separate host threads
-  auto candidate = [&](int strategy, uint32_t k, std::vector<Gate>* out) {
-    std::vector<Gate> cand = strategy == 0 ? fuse_greedy_public(seg, k) : fuse_window_public(seg, k);
+  // every (strategy, width) candidate is grouped, classified and costed independently (on long
+  // segments on separate host threads), without composing the matrices of groups whose sweep
+  // kind does not depend on them; only the chosen candidate is composed
+  auto candidate = [&](int strategy, uint32_t k) {
+    const std::vector<Gate> cand = strategy == 0 ? fuse_greedy_public(seg, k, true) : fuse_window_public(seg, k, true);
     std::vector<Sweep> sw;
     sw.reserve(cand.size());
     for (const Gate& g : cand) {
-      Sweep s = classify_gate(g);
+      Sweep s;
+      if (g.a.empty()) {  // uncomposed group of >= 3 qubits: a dense sweep on its sorted qubits
+        s.kind = SK_DENSE;
+        s.m = g.m;
+        for (uint32_t j = 0; j < g.m; ++j) s.q[j] = g.q[j];
+        std::sort(s.q, s.q + g.m);
+        s.n_gates = 1;
+      } else {
+        s = classify_gate(g);
+      }
       if (s.kind != SK_NONE) sw.push_back(std::move(s));
     }
     select_engines(sw, n, o, dtype);
-    *out = std::move(cand);
     return predict_plan_seconds(sw, n, dtype);
   };
   const size_t ncand = 2 * size_t(cap);
-  std::vector<std::vector<Gate>> cands(ncand);
   std::vector<double> secs(ncand, 1e300);
   if (seg.size() >= 64) {
     std::vector<std::future<double>> fut;
     for (size_t c = 0; c < ncand; ++c)
-      fut.push_back(std::async(std::launch::async, candidate, int(c / cap), uint32_t(c % cap) + 1, &cands[c]));
+      fut.push_back(std::async(std::launch::async, candidate, int(c / cap), uint32_t(c % cap) + 1));
     for (size_t c = 0; c < ncand; ++c) secs[c] = fut[c].get();
   } else {
-    for (size_t c = 0; c < ncand; ++c) secs[c] = candidate(int(c / cap), uint32_t(c % cap) + 1, &cands[c]);
+    for (size_t c = 0; c < ncand; ++c) secs[c] = candidate(int(c / cap), uint32_t(c % cap) + 1);
   }
   size_t best = 0;
   for (size_t c = 1; c < ncand; ++c)
     if (secs[c] < secs[best]) best = c;  // ties keep the earlier (greedy, narrower) candidate
-  return std::move(cands[best]);
+  const uint32_t k = uint32_t(best % cap) + 1;
+  return best / cap == 0 ? fuse_greedy_public(seg, k) : fuse_window_public(seg, k);
 }
 
 }  // namespace qsvb

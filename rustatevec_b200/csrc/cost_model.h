@@ -26,8 +26,10 @@ void select_engines(std::vector<Sweep>& sw, uint32_t n, const qsvb_plan_opts& o,
 std::vector<Gate> learned_fuse(const std::vector<Gate>& seg, uint32_t n, const qsvb_plan_opts& o, int dtype);
 
 // Fusion strategies (planner.cpp).
-std::vector<Gate> fuse_greedy_public(const std::vector<Gate>& in, uint32_t maxq);
-std::vector<Gate> fuse_window_public(const std::vector<Gate>& in, uint32_t maxq);
+// cost_only: groups whose sweep kind does not depend on their entries are left uncomposed (no
+// matrix), for costing candidates; the chosen candidate is fused again with cost_only false.
+std::vector<Gate> fuse_greedy_public(const std::vector<Gate>& in, uint32_t maxq, bool cost_only = false);
+std::vector<Gate> fuse_window_public(const std::vector<Gate>& in, uint32_t maxq, bool cost_only = false);
 
 // Installed MLP (weights are host copies; mlp.cu trains them on the device).
 struct MlpModel {

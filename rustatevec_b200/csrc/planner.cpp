@@ -88,62 +88,126 @@ bool is_diag(const Gate& g) {
 }
 
 // Compose `ops` (applied in order) onto the sorted qubit list `q` in FP64: new = E(g) * mat, the
-// embedding qsv's build_fused uses (fusion.rs:102-140).
+// embedding qsv's build_fused uses (fusion.rs:102-140). Each gate updates, in place, the 2^m rows
+// it mixes (rows whose indices differ only in the gate's bits), with real and imaginary parts in
+// separate arrays so the column loops vectorise; every product is summed in gate-column order
+// from zero, skipping zero entries.
 Gate compose(const std::vector<uint32_t>& q, const std::vector<const Gate*>& ops) {
   const size_t m = q.size(), dim = size_t(1) << m;
-  std::vector<cd> mat(dim * dim, cd(0, 0)), nw(dim * dim);
-  for (size_t i = 0; i < dim; ++i) mat[i * dim + i] = cd(1, 0);
+  std::vector<double> re(dim * dim, 0.0), im(dim * dim, 0.0);  // row-major
+  for (size_t i = 0; i < dim; ++i) re[i * dim + i] = 1.0;
+  std::vector<double> ore, oim;  // the old values of the rows one gate block mixes
   for (const Gate* g : ops) {
+    const size_t nsub = size_t(1) << g->m;
+    size_t off[64], gmask = 0;
     uint32_t local[6];
-    for (uint32_t j = 0; j < g->m; ++j)
+    for (uint32_t j = 0; j < g->m; ++j) {
       local[j] = uint32_t(std::find(q.begin(), q.end(), g->q[j]) - q.begin());
-    const size_t nsub = size_t(1) << g->m, gd = nsub;
-    std::fill(nw.begin(), nw.end(), cd(0, 0));
-    for (size_t r = 0; r < dim; ++r) {
-      size_t rs = 0;
-      for (uint32_t j = 0; j < g->m; ++j) rs |= ((r >> local[j]) & 1u) << j;
+      gmask |= size_t(1) << local[j];
+    }
+    for (size_t ks = 0; ks < nsub; ++ks) {
+      size_t o = 0;
+      for (uint32_t j = 0; j < g->m; ++j) o |= ((ks >> j) & 1u) << local[j];
+      off[ks] = o;
+    }
+    ore.resize(nsub * dim);
+    oim.resize(nsub * dim);
+    for (size_t b = 0; b < dim; ++b) {
+      if (b & gmask) continue;
       for (size_t ks = 0; ks < nsub; ++ks) {
-        const cd e = g->a[rs * gd + ks];
-        if (e == cd(0, 0)) continue;
-        size_t k = r;
-        for (uint32_t j = 0; j < g->m; ++j) k = (k & ~(size_t(1) << local[j])) | (((ks >> j) & 1u) << local[j]);
-        const cd* src = &mat[k * dim];
-        cd* dst = &nw[r * dim];
-        for (size_t c = 0; c < dim; ++c) dst[c] += e * src[c];
+        std::copy_n(&re[(b | off[ks]) * dim], dim, &ore[ks * dim]);
+        std::copy_n(&im[(b | off[ks]) * dim], dim, &oim[ks * dim]);
+      }
+      for (size_t rs = 0; rs < nsub; ++rs) {
+        double* __restrict__ dr = &re[(b | off[rs]) * dim];
+        double* __restrict__ di = &im[(b | off[rs]) * dim];
+        std::fill_n(dr, dim, 0.0);
+        std::fill_n(di, dim, 0.0);
+        for (size_t ks = 0; ks < nsub; ++ks) {
+          const cd e = g->a[rs * nsub + ks];
+          if (e == cd(0, 0)) continue;
+          const double er = e.real(), ei = e.imag();
+          const double* __restrict__ sr = &ore[ks * dim];
+          const double* __restrict__ si = &oim[ks * dim];
+          for (size_t c = 0; c < dim; ++c) {
+            dr[c] += er * sr[c] - ei * si[c];
+            di[c] += er * si[c] + ei * sr[c];
+          }
+        }
       }
     }
-    mat.swap(nw);
   }
   Gate out;
   out.m = uint32_t(m);
   for (size_t j = 0; j < m; ++j) out.q[j] = q[j];
-  out.a = std::move(mat);
+  out.a.resize(dim * dim);
+  for (size_t i = 0; i < dim * dim; ++i) out.a[i] = cd(re[i], im[i]);
   return out;
 }
 
-void emit_group(std::vector<Gate>& out, const std::vector<const Gate*>& grp) {
+// A group of diagonal gates composed as the product of their diagonals (O(2^m) per gate).
+Gate compose_diag(const std::vector<uint32_t>& q, const std::vector<const Gate*>& ops) {
+  const size_t m = q.size(), dim = size_t(1) << m;
+  std::vector<cd> d(dim, cd(1, 0));
+  for (const Gate* g : ops) {
+    uint32_t local[6];
+    for (uint32_t j = 0; j < g->m; ++j)
+      local[j] = uint32_t(std::find(q.begin(), q.end(), g->q[j]) - q.begin());
+    const size_t gd = size_t(1) << g->m;
+    for (size_t r = 0; r < dim; ++r) {
+      size_t rs = 0;
+      for (uint32_t j = 0; j < g->m; ++j) rs |= ((r >> local[j]) & 1u) << j;
+      d[r] = g->a[rs * gd + rs] * d[r];
+    }
+  }
+  Gate out;
+  out.m = uint32_t(m);
+  for (size_t j = 0; j < m; ++j) out.q[j] = q[j];
+  out.a.assign(dim * dim, cd(0, 0));
+  for (size_t r = 0; r < dim; ++r) out.a[r * dim + r] = d[r];
+  return out;
+}
+
+// Emits one fused group. With `cost_only` (candidate costing in the learned planner) a group of
+// three or more qubits that holds a non-diagonal gate becomes a placeholder with no matrix (it
+// classifies as a dense sweep, whose cost does not depend on the entries); groups whose kind the
+// entries decide (diagonal, or at most two qubits) are still composed.
+void emit_group(std::vector<Gate>& out, const std::vector<const Gate*>& grp, bool cost_only) {
   if (grp.empty()) return;
   if (grp.size() == 1) {
     out.push_back(*grp[0]);
     return;
   }
   uint64_t mask = 0;
-  for (const Gate* g : grp) mask |= qmask(*g);
+  bool all_diag = true;
+  for (const Gate* g : grp) {
+    mask |= qmask(*g);
+    all_diag = all_diag && is_diag(*g);
+  }
   std::vector<uint32_t> q;
   for (uint32_t b = 0; b < 64; ++b)
     if ((mask >> b) & 1) q.push_back(b);
-  out.push_back(compose(q, grp));
+  if (cost_only && all_diag) {
+    out.push_back(compose_diag(q, grp));
+  } else if (cost_only && q.size() > 2) {
+    Gate ph;
+    ph.m = uint32_t(q.size());
+    for (size_t j = 0; j < q.size(); ++j) ph.q[j] = q[j];
+    out.push_back(std::move(ph));
+  } else {
+    out.push_back(compose(q, grp));
+  }
 }
 
 // fusion.rs:39-77 — consecutive-only greedy.
-std::vector<Gate> fuse_greedy(const std::vector<Gate>& in, uint32_t maxq) {
+std::vector<Gate> fuse_greedy(const std::vector<Gate>& in, uint32_t maxq, bool cost_only = false) {
   maxq = std::max<uint32_t>(maxq, 1);
   std::vector<Gate> out;
   std::vector<const Gate*> grp;
   std::vector<uint32_t> gq;  // insertion order, as the reference keeps it
   for (const Gate& g : in) {
     if (g.m > maxq) {
-      emit_group(out, grp);
+      emit_group(out, grp, cost_only);
       grp.clear();
       gq.clear();
       out.push_back(g);
@@ -159,19 +223,20 @@ std::vector<Gate> fuse_greedy(const std::vector<Gate>& in, uint32_t maxq) {
       gq = uni;
       grp.push_back(&g);
     } else {
-      emit_group(out, grp);
+      emit_group(out, grp, cost_only);
       grp.clear();
       gq.assign(g.q, g.q + g.m);
       grp.push_back(&g);
     }
   }
-  emit_group(out, grp);
+  emit_group(out, grp, cost_only);
   return out;
 }
 
 // Commutation-aware window fusion: a later gate may join the open group when its qubits are
 // disjoint from every not-yet-emitted gate it would jump over.
-std::vector<Gate> fuse_window(const std::vector<Gate>& in, uint32_t maxq, size_t lookahead = 1024) {
+std::vector<Gate> fuse_window(const std::vector<Gate>& in, uint32_t maxq, bool cost_only = false,
+                              size_t lookahead = 1024) {
   maxq = std::max<uint32_t>(maxq, 1);
   std::vector<char> done(in.size(), 0);
   std::vector<Gate> out;
@@ -203,7 +268,7 @@ std::vector<Gate> fuse_window(const std::vector<Gate>& in, uint32_t maxq, size_t
         if (uint32_t(__builtin_popcountll(gmask)) == maxq && (gmask & ~blocked) == 0) break;
       }
     }
-    emit_group(out, grp);
+    emit_group(out, grp, cost_only);
   }
   return out;
 }
@@ -218,8 +283,12 @@ bool phase_representable(const Gate& g) {
 
 }  // namespace
 
-std::vector<Gate> fuse_greedy_public(const std::vector<Gate>& in, uint32_t maxq) { return fuse_greedy(in, maxq); }
-std::vector<Gate> fuse_window_public(const std::vector<Gate>& in, uint32_t maxq) { return fuse_window(in, maxq); }
+std::vector<Gate> fuse_greedy_public(const std::vector<Gate>& in, uint32_t maxq, bool cost_only) {
+  return fuse_greedy(in, maxq, cost_only);
+}
+std::vector<Gate> fuse_window_public(const std::vector<Gate>& in, uint32_t maxq, bool cost_only) {
+  return fuse_window(in, maxq, cost_only);
+}
 
 std::vector<Gate> fuse_gates(const std::vector<Gate>& in, uint32_t n, const qsvb_plan_opts& o, int dtype) {
   (void)n;
