@@ -198,27 +198,28 @@ class PackedBatch:
 
     def __init__(self, circuits):
         assert C.sizeof(Gate) == _GATE_DT.itemsize and C.sizeof(CircuitS) == _CIRC_DT.itemsize
-        flats = [c.flatten() for c in circuits]
-        arity = np.concatenate([f[0] for f in flats]) if flats else np.zeros(0, np.uint32)
-        self.mats = np.ascontiguousarray(np.concatenate([f[2] for f in flats]) if flats else np.zeros(1))
+        from itertools import chain
+        from .circuit import flatten_ops
+        counts = np.array([len(c) for c in circuits], dtype=np.int64)
+        arity, allq, mats = flatten_ops(list(chain.from_iterable(c.ops() for c in circuits)))
+        self.mats = mats if len(mats) else np.zeros(1)
         ng = len(arity)
         self.gates = np.zeros(max(ng, 1), dtype=_GATE_DT)
         self.gates["n"][:ng] = arity
         a64 = arity.astype(np.int64)
         qoff = np.concatenate([[0], np.cumsum(a64)])
-        allq = np.concatenate([f[1] for f in flats]) if flats else np.zeros(0, np.uint32)
         for j in range(int(a64.max()) if ng else 0):
             sel = a64 > j
             self.gates["q"][:ng][sel, j] = allq[qoff[:-1][sel] + j]
         moff = np.concatenate([[0], np.cumsum(2 * (1 << (2 * a64)))])[:-1]
         self.gates["mat"][:ng] = self.mats.ctypes.data + 8 * moff
-        counts = np.array([len(f[0]) for f in flats], dtype=np.int64)
+        nc = len(circuits)
         goff = np.concatenate([[0], np.cumsum(counts)])[:-1]
-        self.circs = np.zeros(max(len(flats), 1), dtype=_CIRC_DT)
-        self.circs["n"][:len(flats)] = [c.n_qubits() for c in circuits]
-        self.circs["ngates"][:len(flats)] = counts
-        self.circs["gates"][:len(flats)] = self.gates.ctypes.data + _GATE_DT.itemsize * goff
-        self.count = len(flats)
+        self.circs = np.zeros(max(nc, 1), dtype=_CIRC_DT)
+        self.circs["n"][:nc] = [c.n_qubits() for c in circuits]
+        self.circs["ngates"][:nc] = counts
+        self.circs["gates"][:nc] = self.gates.ctypes.data + _GATE_DT.itemsize * goff
+        self.count = nc
         self.n_qubits = np.array([c.n_qubits() for c in circuits], dtype=np.int64)
 
     def ptr(self):

@@ -11,11 +11,30 @@ per-op arity, concatenated qubits, and concatenated row-major interleaved FP64 m
 from __future__ import annotations
 
 from dataclasses import dataclass
+from itertools import chain
+from operator import attrgetter
 
 import numpy as np
 
 from . import gate as G
 from .gate import DenseGate, MAX_GATE_QUBITS
+
+
+_QUBITS = attrgetter("qubits")
+_MATRIX = attrgetter("gate.matrix")
+
+
+def flatten_ops(ops):
+    """``(arity u32[nops], qubits u32[sum m], mats f64[sum 2*4^m])`` of a list of ``GateOp``; the
+    per-op work runs in C (``map`` + ``attrgetter``, and one ``bytes.join`` over the matrices'
+    buffers, which ``DenseGate`` keeps C-contiguous complex128). The matrix array is read-only."""
+    if not ops:
+        return np.zeros(0, np.uint32), np.zeros(0, np.uint32), np.zeros(0, np.float64)
+    qs = list(map(_QUBITS, ops))
+    arity = np.fromiter(map(len, qs), dtype=np.uint32, count=len(qs))
+    qubits = np.fromiter(chain.from_iterable(qs), dtype=np.uint32)
+    mats = np.frombuffer(b"".join(map(_MATRIX, ops)), dtype=np.float64)
+    return arity, qubits, mats
 
 
 @dataclass
@@ -78,15 +97,7 @@ class Circuit:
     # ---- packing for the C ABI / oracle
     def flatten(self):
         """Return ``(arity u32[nops], qubits u32[sum m], mats f64[sum 2*4^m])``."""
-        arity = np.fromiter((len(op.qubits) for op in self._ops), dtype=np.uint32,
-                            count=len(self._ops))
-        qubits = np.fromiter((q for op in self._ops for q in op.qubits), dtype=np.uint32)
-        if self._ops:
-            mats = np.concatenate([op.gate.matrix.reshape(-1).view(np.float64)
-                                   for op in self._ops])
-        else:
-            mats = np.zeros(0, dtype=np.float64)
-        return arity, qubits, np.ascontiguousarray(mats)
+        return flatten_ops(self._ops)
 
     @classmethod
     def from_flat(cls, n_qubits, arity, qubits, mats) -> "Circuit":

@@ -37,11 +37,13 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <future>
 #include <memory>
 #include <mutex>
 #include <numeric>
 #include <type_traits>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "qsvb_internal.h"
@@ -1373,22 +1375,26 @@ void emit_phases(BatchPlan& bp, const std::vector<LGate>& G, uint32_t nlocal, st
 
 }  // namespace
 
-std::unique_ptr<BatchPlan> build_batch(const qsvb_circuit* circuits, size_t ncirc, int dtype, uint32_t local_bits,
-                                       uint32_t reg_bits) {
-  QSVB_REQUIRE(circuits != nullptr && ncirc > 0, "empty batch");
-  QSVB_REQUIRE(ncirc <= (1u << 20), "at most 2^20 circuits per batch");
-  QSVB_REQUIRE(dtype == QSVB_C64 || dtype == QSVB_C128, "dtype must be QSVB_C64 or QSVB_C128");
-  QSVB_REQUIRE(local_bits >= 7 && local_bits <= uint32_t(kMaxLocal), "local qubits must be 7..14");
-  auto bp = std::make_unique<BatchPlan>();
-  bp->dtype = dtype;
-  bp->local_bits = local_bits;
-  bp->rb = reg_bits;
-  bp->swz_w = dtype == QSVB_C128 ? 4u : 5u;
-  bp->ncirc = uint32_t(ncirc);
-  std::vector<std::vector<uint32_t>> circuit_passes(ncirc);
-  std::vector<double> cost(ncirc);
-  const double eb = dtype == QSVB_C128 ? 16.0 : 8.0;
+// Passes of circuits[0..ncirc) appended to `bp` (circuit numbers, pass, state, probability and
+// <Z_0> offsets all counted from zero within `bp`).
+struct BatchPart {
+  BatchPlan bp;
+  std::vector<std::vector<uint32_t>> circuit_passes;
+  std::vector<double> cost;
   double bytes = 0, flops = 0;
+};
+
+void plan_batch_part(BatchPart& part, const qsvb_circuit* circuits, size_t ncirc) {
+  BatchPlan* bp = &part.bp;
+  const int dtype = bp->dtype;
+  const uint32_t local_bits = bp->local_bits;
+  auto& circuit_passes = part.circuit_passes;
+  auto& cost = part.cost;
+  circuit_passes.assign(ncirc, {});
+  cost.assign(ncirc, 0.0);
+  const double eb = dtype == QSVB_C128 ? 16.0 : 8.0;
+  double& bytes = part.bytes;
+  double& flops = part.flops;
   for (size_t ci = 0; ci < ncirc; ++ci) {
     const qsvb_circuit& c = circuits[ci];
     validate_circuit(&c);
@@ -1491,6 +1497,85 @@ std::unique_ptr<BatchPlan> build_batch(const qsvb_circuit* circuits, size_t ncir
     const size_t np = circuit_passes[ci].size();
     bytes += amps * 8.0 + double(np - 1) * 2.0 * amps * eb;
     cost[ci] = double(np) * amps + double(gates.size()) * amps / 16.0;
+  }
+}
+
+std::unique_ptr<BatchPlan> build_batch(const qsvb_circuit* circuits, size_t ncirc, int dtype, uint32_t local_bits,
+                                       uint32_t reg_bits) {
+  QSVB_REQUIRE(circuits != nullptr && ncirc > 0, "empty batch");
+  QSVB_REQUIRE(ncirc <= (1u << 20), "at most 2^20 circuits per batch");
+  QSVB_REQUIRE(dtype == QSVB_C64 || dtype == QSVB_C128, "dtype must be QSVB_C64 or QSVB_C128");
+  QSVB_REQUIRE(local_bits >= 7 && local_bits <= uint32_t(kMaxLocal), "local qubits must be 7..14");
+  auto bp = std::make_unique<BatchPlan>();
+  bp->dtype = dtype;
+  bp->local_bits = local_bits;
+  bp->rb = reg_bits;
+  bp->swz_w = dtype == QSVB_C128 ? 4u : 5u;
+  bp->ncirc = uint32_t(ncirc);
+  // circuits are planned independently: contiguous chunks on host threads, then concatenated with
+  // their offsets shifted (the result does not depend on the number of chunks)
+  size_t nthreads = std::max<size_t>(1, std::thread::hardware_concurrency());
+  if (const char* e = std::getenv("QSVB_BATCH_PLAN_THREADS")) nthreads = std::max(1, std::atoi(e));
+  const size_t nchunks = std::min<size_t>({nthreads, ncirc, 32});
+  std::vector<BatchPart> parts(nchunks);
+  std::vector<size_t> lo(nchunks + 1);
+  for (size_t k = 0; k <= nchunks; ++k) lo[k] = ncirc * k / nchunks;
+  for (BatchPart& pt : parts) {
+    pt.bp.dtype = dtype;
+    pt.bp.local_bits = local_bits;
+    pt.bp.rb = reg_bits;
+    pt.bp.swz_w = bp->swz_w;
+  }
+  if (nchunks == 1) {
+    plan_batch_part(parts[0], circuits, ncirc);
+  } else {
+    std::vector<std::future<void>> fut;
+    for (size_t k = 0; k < nchunks; ++k)
+      fut.push_back(std::async(std::launch::async, plan_batch_part, std::ref(parts[k]), circuits + lo[k],
+                               lo[k + 1] - lo[k]));
+    for (auto& f : fut) f.get();
+  }
+  std::vector<std::vector<uint32_t>> circuit_passes;
+  std::vector<double> cost;
+  circuit_passes.reserve(ncirc);
+  cost.reserve(ncirc);
+  double bytes = 0, flops = 0;
+  for (size_t k = 0; k < nchunks; ++k) {
+    BatchPart& pt = parts[k];
+    const BatchPlan& q = pt.bp;
+    const uint32_t pass_base = uint32_t(bp->passes.size());
+    const uint32_t prog_base = uint32_t(bp->prog.size()), phase_base = uint32_t(bp->phases.size());
+    const uint32_t coef_base = uint32_t(bp->coef.size() / 2);
+    const uint64_t state_base = bp->state_amps, prob_base = bp->prob_total, z_base = bp->zslots;
+    for (PassDev P : q.passes) {
+      const bool single = q.nq[P.circuit] <= local_bits;  // whole in shared memory: no state block
+      P.circuit += uint32_t(lo[k]);
+      if (!single) P.state_off += state_base;
+      P.prob_off += prob_base;
+      P.prog_off += prog_base;
+      P.phase_off += phase_base;
+      P.coef_off += coef_base;
+      if (P.prev != ~0u) P.prev += pass_base;
+      if (P.last) P.zslot += z_base;
+      bp->passes.push_back(P);
+    }
+    bp->phases.insert(bp->phases.end(), q.phases.begin(), q.phases.end());
+    bp->prog.insert(bp->prog.end(), q.prog.begin(), q.prog.end());
+    bp->coef.insert(bp->coef.end(), q.coef.begin(), q.coef.end());
+    bp->nq.insert(bp->nq.end(), q.nq.begin(), q.nq.end());
+    for (uint64_t v : q.prob_off) bp->prob_off.push_back(v + prob_base);
+    for (uint64_t v : q.zoff) bp->zoff.push_back(v + z_base);
+    bp->zcnt.insert(bp->zcnt.end(), q.zcnt.begin(), q.zcnt.end());
+    bp->state_amps += q.state_amps;
+    bp->prob_total += q.prob_total;
+    bp->zslots += q.zslots;
+    for (auto& v : pt.circuit_passes) {
+      for (uint32_t& pi : v) pi += pass_base;
+      circuit_passes.push_back(std::move(v));
+    }
+    cost.insert(cost.end(), pt.cost.begin(), pt.cost.end());
+    bytes += pt.bytes;
+    flops += pt.flops;
   }
   // work items: level by level, costliest circuits first within a level
   std::vector<uint32_t> order(ncirc);

@@ -134,6 +134,27 @@ def test_reusable_batch_object_and_autotune(be):
     assert np.min(secs[:6]) == secs[2 * (best_l.value - (top - 2)) + register_widths(be).index(best_r.value)]
 
 
+def test_planning_on_several_host_threads_gives_the_same_batch(be, monkeypatch):
+    """Circuits are planned in chunks on host threads and concatenated; the device results are
+    bit-identical whatever the number of chunks."""
+    rng = SplitMix64(77)
+    circuits = ansatz_batch(40, 9, n_lo=2, n_hi=12, d_lo=1, d_hi=5)
+    circuits += [ansatz_circuit(n, 4, rng) for n in (13, 15, 17)] + [random_circuit(n, 25 * n, n) for n in (14, 16)]
+    rng2 = np.random.default_rng(0)
+    order = rng2.permutation(len(circuits))
+    circuits = [circuits[i] for i in order]
+    out = []
+    for threads in ("1", "3", "7", "64"):
+        monkeypatch.setenv("QSVB_BATCH_PLAN_THREADS", threads)
+        z0, probs, st = be.execute_batch(circuits, local_qubits=10)
+        out.append((z0, np.concatenate(probs), st["n_sweeps"], st["algorithmic_bytes"]))
+    for z0, p, n, b in out[1:]:
+        assert np.array_equal(z0, out[0][0]) and np.array_equal(p, out[0][1])
+        assert n == out[0][2] and b == pytest.approx(out[0][3], rel=1e-12)
+    monkeypatch.delenv("QSVB_BATCH_PLAN_THREADS")
+    check_batch(be, circuits, 10)
+
+
 def test_backend_execute_batch_matches_single_circuit_path(be):
     circuits = ansatz_batch(6, 3, n_lo=10, n_hi=16, d_lo=2, d_hi=4)
     z0, probs, st = be.execute_batch(circuits)
