@@ -574,9 +574,10 @@ void ensure_pinned(qsvb_ctx* c) {
   }
 }
 
-// host copy of one staged chunk, split over a few threads (one thread moves ~10 GB/s)
+// host copy of one staged chunk, split over a few threads (one thread moves ~10 GB/s, less while
+// it first touches fresh pages of the destination)
 void host_copy(void* dst, const void* src, size_t bytes) {
-  constexpr int kThreads = 4;
+  constexpr int kThreads = 8;
   if (bytes < (size_t(4) << 20)) {
     std::memcpy(dst, src, bytes);
     return;

@@ -170,7 +170,7 @@ namespace qsvb {
 // host copies chunk k into `dst` (pageable). `produce(k, off, len, dev_dst)` may enqueue work that
 // fills a device chunk first (it returns the device pointer to copy from); pass nullptr to copy
 // straight from `src`.
-constexpr size_t kPinChunk = size_t(32) << 20;
+constexpr size_t kPinChunk = size_t(64) << 20;
 void d2h_staged(qsvb_ctx* c, void* dst, const void* src, size_t bytes);
 void sample_shots(qsvb_ctx* c, const qsvb_state* st, uint64_t shots, uint64_t seed, uint64_t* out);
 }  // namespace qsvb
