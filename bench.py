@@ -728,7 +728,12 @@ def run_kernel_case(args):
         planner = L.PLAN_TILE
     be = B200Backend(0, precision=prec)
     st = be.alloc(n)
-    be.init_basis(st, 0)
+    # a dense random state by default: a basis state leaves almost every streamed amplitude zero,
+    # which draws less power and times optimistically
+    if args.input == "basis":
+        be.init_basis(st, 0)
+    else:
+        be.init_gaussian(st, 7)
     p = Plan(be, c, L.make_opts(planner, 2, engine, use_graph=False))
     info = p.sweeps()
     stream = torch.cuda.ExternalStream(be.stream())
@@ -744,7 +749,7 @@ def run_kernel_case(args):
     t = e0.elapsed_time(e1) * 1e-3 / args.reps
     nbytes = sum(s["algorithmic_bytes"] for s in info)
     peak, kind = peaks()
-    print(json.dumps({"kernel_case": args.kernel_case, "qubits": n, "precision": prec,
+    print(json.dumps({"kernel_case": args.kernel_case, "qubits": n, "precision": prec, "input": args.input,
                       "sweeps": [s["kind"] for s in info], "us_per_launch": round(t * 1e6, 2),
                       "algorithmic_bytes": nbytes, "GB/s": round(nbytes / t / 1e9, 1),
                       "frac_of_peak": round(nbytes / t / 1e9 / peak, 4), "peak": f"{peak} ({kind})"}))
@@ -754,6 +759,8 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--kernel-case", choices=sorted(KERNEL_CASES))
     ap.add_argument("--qubits", type=int, default=30)
+    ap.add_argument("--input", default="gaussian", choices=["gaussian", "basis"],
+                    help="kernel cases: initial state (dense random, or |0..0>)")
     ap.add_argument("--reps", type=int, default=10)
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
