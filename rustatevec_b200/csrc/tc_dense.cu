@@ -80,8 +80,10 @@ struct TcParams {
   uint16_t dstlo[64];      // (row << ncb | col) contribution of the low 6 state bits
   uint16_t trow[64];       // address-order tile index of gate row s
   uint16_t tcol[256];      // address-order tile index of column c
-  uint32_t bmode;          // 0: MN-major vector, 1: K-major vector, 2: K-major row pairs
+  uint32_t bmode;          // 0: MN-major vector, 1: K-major vector, 2: K-major row pairs,
+                           // 3: K-major vector assembled from a lane pair
   uint32_t b2_bit0;        // bmode 2: state bit 0 is the gate bit (else state bit 1 is)
+  uint32_t pair_shift;     // bmode 3: the gate's second row bit is state bit pair_shift + 2
   // converter work order: float4 u (u = thread + j * converter threads) covers tile amplitudes
   // 4 * (tplo[u & 31] | tphi[u >> 5]): a bit permutation chosen on the host so that a warp's
   // K-major B stores fall in distinct banks (the identity for MN-major tiles)
@@ -255,7 +257,9 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
       : "memory");
 }
 
-template <int KQ>
+// BM: the B-operand layout mode (TcParams::bmode), fixed at compile time so that each
+// instantiation's converter loop holds only its own path.
+template <int KQ, int BM>
 __global__ void __launch_bounds__(kTcThreads, 1) k_tc_dense(float* __restrict__ re, float* __restrict__ im,
                                                             uint64_t ntiles, const uint4* __restrict__ wpack,
                                                             TcParams p, int* err, long long* prof,
@@ -321,7 +325,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_dense(float* __restrict__ 
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = *tmem_slot;
-  const uint32_t b_mn = p.bmode == 0 ? 1u : 0u;
+  constexpr uint32_t b_mn = BM == 0 ? 1u : 0u;
   if (warp >= kEpiWarp0) {
     // A (Whi, Wlo) into tensor memory: the thread owning TMEM lane m writes row m of each, 64
     // 32-bit columns of packed bf16 pairs (element 2j in the low half).
@@ -397,7 +401,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_dense(float* __restrict__ 
     for (uint64_t i = 0; i < my_tiles; ++i) {
       const uint32_t slot = uint32_t(i % kIoSlots), par = uint32_t((i / kIoSlots) & 1);
       const uint32_t bs = uint32_t(i & 1), bpar = uint32_t((i >> 1) & 1);
-      if (!mbar_wait_t(&iofull[slot], par, w0) || !mbar_wait_t(&bfree[bs], bpar ^ 1u, w1)) {
+      const bool ready = mbar_wait_t(&iofull[slot], par, w0) && mbar_wait_t(&bfree[bs], bpar ^ 1u, w1);
+      if (!__all_sync(0xffffffffu, ready)) {  // warp-uniform exit: the lane-pair mode shuffles
         atomicExch(err, 1);
         break;
       }
@@ -424,7 +429,38 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_dense(float* __restrict__ 
         const float4 xr = xra[j], xi = xia[j];
         const float vr[4] = {xr.x, xr.y, xr.z, xr.w};
         const float vi[4] = {xi.x, xi.y, xi.z, xi.w};
-        if (p.bmode == 2) {
+        if constexpr (BM == 3) {
+          // state bit 0 is a column, bit 1 the gate's row bit 0 and state bit 2 + pair_shift its
+          // row bit 1, which is lane bit pair_shift (the work order keeps float4 index bits 0..2
+          // as lane bits 0..2). The lane pair differing in it holds rows 0-3 of two columns: each
+          // lane gives its partner the two values of the partner's column and keeps four
+          // consecutive rows of its own, stored like bmode 1.
+          const uint32_t sh = p.pair_shift;
+          const bool odd = ((uint32_t(lane) >> sh) & 1u) != 0;
+          const int pm = 1 << sh;
+          const float rr0 = __shfl_xor_sync(0xffffffffu, odd ? xr.x : xr.y, pm);
+          const float rr1 = __shfl_xor_sync(0xffffffffu, odd ? xr.z : xr.w, pm);
+          const float ri0 = __shfl_xor_sync(0xffffffffu, odd ? xi.x : xi.y, pm);
+          const float ri1 = __shfl_xor_sync(0xffffffffu, odd ? xi.z : xi.w, pm);
+          const float wr[4] = {odd ? rr0 : xr.x, odd ? rr1 : xr.z, odd ? xr.y : rr0, odd ? xr.w : rr1};
+          const float wi[4] = {odd ? ri0 : xi.x, odd ? ri1 : xi.z, odd ? xi.y : ri0, odd ? xi.w : ri1};
+          const int tg = (t & ~(4 << sh)) | (odd ? 1 : 0);  // the group's row-0 element of this column
+          const uint32_t d = uint32_t(s_dlo[tg & 63]) + s_dhi[tg >> 6];
+          const uint32_t s = d >> NCB, c = d & CMASK;
+          const uint32_t kb = (c >> 6) * KR, cl = c & 63u;
+          const uint32_t o_re = kmaj_off(cl, kb + s, 64);
+          const uint32_t o_im = kmaj_off(cl, kb + M2 + s, 64);
+          __nv_bfloat16 hr[4], lr[4], hm[4], lm[4];
+#pragma unroll
+          for (int e = 0; e < 4; ++e) {
+            split_bf16(wr[e], hr[e], lr[e]);
+            split_bf16(wi[e], hm[e], lm[e]);
+          }
+          *reinterpret_cast<uint2*>(b_hi + o_re) = pack4(hr);
+          *reinterpret_cast<uint2*>(b_lo + o_re) = pack4(lr);
+          *reinterpret_cast<uint2*>(b_hi + o_im) = pack4(hm);
+          *reinterpret_cast<uint2*>(b_lo + o_im) = pack4(lm);
+        } else if constexpr (BM == 2) {
           // exactly one of state bits 0, 1 is a gate bit (the gate's lowest, so row parity): the
           // four amplitudes are two pairs of adjacent rows (K) in two columns, stored as bf16 pairs
           const int step = p.b2_bit0 ? 1 : 2;  // element offset of a pair's second row
@@ -534,7 +570,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_dense(float* __restrict__ 
       w2 += tb - ta;
       // the converters finished reading this slot before the MMAs that produced v were issued
       float* st = io + slot * 2 * kTileAmps + part * kTileAmps;
-      if (p.bmode == 0) {
+      if constexpr (BM == 0) {
 #pragma unroll
         for (int cb = 0; cb < 4; ++cb)
 #pragma unroll
@@ -758,8 +794,14 @@ static void launch_tc_k(const LaunchEnv& env, float* re, float* im, uint32_t n, 
   }
   const bool low_cols = gate_rank[0] < 0 && gate_rank[1] < 0;
   const bool low_rows = gate_rank[0] == 0 && gate_rank[1] == 1;
-  p.bmode = low_cols ? 0u : (low_rows ? 1u : 2u);
+  // bit 0 a column, bit 1 the gate's lowest qubit and its next qubit among state bits 2..4
+  int row1_bit = -1;
+  for (uint32_t b = 0; b < n; ++b)
+    if (gate_rank[b] == 1) row1_bit = int(b);
+  const bool lane_pair = gate_rank[0] < 0 && gate_rank[1] == 0 && row1_bit >= 2 && row1_bit <= 4;
+  p.bmode = low_cols ? 0u : (low_rows ? 1u : (lane_pair ? 3u : 2u));
   p.b2_bit0 = gate_rank[0] == 0 ? 1u : 0u;
+  p.pair_shift = lane_pair ? uint32_t(row1_bit - 2) : 0u;
   {
     // converter work order: float4 index bits 0..2 stay (a quarter-warp's 16-byte loads stay
     // conflict-free); for K-major tiles the lane bits 3 and 4 take the two float4 bits that make
@@ -780,7 +822,8 @@ static void launch_tc_k(const LaunchEnv& env, float* re, float* im, uint32_t n, 
         for (uint32_t lane = 0; lane < 32; ++lane) {
           const uint32_t t = perm_t4(lane, pi) * 4u;
           const uint32_t e = p.bmode == 2 ? (p.b2_bit0 ? 2u * q : uint32_t(q)) : 0u;
-          const uint32_t tl = t + e;
+          uint32_t tl = t + e;
+          if (p.bmode == 3) tl = (t & ~(4u << p.pair_shift)) | ((lane >> p.pair_shift) & 1u);
           const uint32_t d = uint32_t(p.dstlo[tl & 63u]) + p.dsthi[tl >> 6];
           const uint32_t sr = d >> NCB, c = d & CM;
           const uint32_t off = kmaj_off(c & 63u, (c >> 6) * KRr + sr, 64);
@@ -816,8 +859,10 @@ static void launch_tc_k(const LaunchEnv& env, float* re, float* im, uint32_t n, 
   }
 
   const uint64_t ntiles = 1ull << (n - kTileBits);
-  QSVB_CK(cudaFuncSetAttribute(k_tc_dense<KQ>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kTcSmem)));
-  QSVB_CK(cudaFuncSetAttribute(k_tc_dense<KQ>, cudaFuncAttributePreferredSharedMemoryCarveout,
+  auto kern = p.bmode == 0 ? k_tc_dense<KQ, 0> : p.bmode == 1 ? k_tc_dense<KQ, 1>
+             : p.bmode == 2 ? k_tc_dense<KQ, 2> : k_tc_dense<KQ, 3>;
+  QSVB_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kTcSmem)));
+  QSVB_CK(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
                                int(cudaSharedmemCarveoutMaxShared)));
   // one persistent CTA per SM (the tensor-memory allocation assumes it)
   const unsigned grid = unsigned(std::max<uint64_t>(1, std::min<uint64_t>(ntiles, uint64_t(env.num_sms))));
@@ -826,8 +871,8 @@ static void launch_tc_k(const LaunchEnv& env, float* re, float* im, uint32_t n, 
   long long* prof = nullptr;
   if (profile) QSVB_CK(cudaMalloc(&prof, sizeof(long long) * 12 * grid));
   if (prof) QSVB_CK(cudaMemsetAsync(prof, 0, sizeof(long long) * 12 * grid, env.stream));
-  k_tc_dense<KQ><<<grid, kTcThreads, kTcSmem, env.stream>>>(re, im, ntiles, static_cast<const uint4*>(dev_mat), p,
-                                                            env.err_flag, prof, maps[0], maps[1]);
+  kern<<<grid, kTcThreads, kTcSmem, env.stream>>>(re, im, ntiles, static_cast<const uint4*>(dev_mat), p, env.err_flag,
+                                                  prof, maps[0], maps[1]);
   QSVB_CK(cudaGetLastError());
   if (prof) {
     std::vector<long long> h(12 * size_t(grid));

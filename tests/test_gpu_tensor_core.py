@@ -54,6 +54,10 @@ QSETS = {
     "mid": lambda n, k: list(range(3, 3 + k)),
     "mixed": lambda n, k: [0] + list(range(5, 4 + k)),    # B row pairs (bit 0 gate, bit 1 column)
     "mixed2": lambda n, k: [1] + list(range(7, 6 + k)),
+    # bit 0 a column, bit 1 the gate's lowest qubit, its next qubit state bit 2, 3 or 4 (lane pairs)
+    "pair2": lambda n, k: [1, 2] + list(range(8, 6 + k)),
+    "pair3": lambda n, k: [1, 3] + list(range(7, 5 + k)),
+    "pair4": lambda n, k: [4, 1] + list(range(n - k + 2, n)),
     "spread": lambda n, k: [2, 4, 7, 9, 10, 11][:k],
     "unsorted": lambda n, k: list(reversed(range(n - k, n))),
 }
@@ -84,6 +88,10 @@ def test_single_tc_sweep(be, k, qset, n):
     [0, 2, 9, 10, 16, 19],       # bit 0 in the gate, bit 1 a column (scalar B stores)
     [2, 3, 4, 5],                # k = 4, one contiguous tile
     [1, 6, 7, 12, 19],           # k = 5, bit 1 in the gate
+    [1, 2, 7, 8, 9, 10],         # brickwork window with bit 1: lane-pair B stores
+    [1, 2, 3, 4, 18, 19],        # lane pairs, bits 2-4 all in the gate
+    [1, 4, 9, 10, 16],           # k = 5, lane pairs across lane bit 2
+    [3, 1, 6, 11],               # k = 4, lane pairs across lane bit 1
 ])
 def test_tc_tile_shapes_n20(be, qs):
     n = 20
