@@ -88,7 +88,7 @@ struct TcParams {
   // 4 * (tplo[u & 31] | tphi[u >> 5]): a bit permutation chosen on the host so that a warp's
   // K-major B stores fall in distinct banks (the identity for MN-major tiles)
   uint16_t tplo[32], tphi[32];
-  uint32_t tcl[16];        // tcol[q] for q < 16 (uniform; read straight from the parameter bank)
+  uint32_t tcl[16];        // stage_idx(tcol[q]) for q < 16 (uniform; read straight from the parameter bank)
   uint32_t tm_rank;        // > 0: the producer uses one tensor-map TMA per component per tile
   uint32_t tm_start[5];    // first state bit of each tensor dimension
   uint32_t tm_len[5];      // bits of that dimension (a run of tile bits plus the run of non-tile bits above it)
@@ -213,7 +213,9 @@ __device__ __forceinline__ uint32_t mnmaj_off(uint32_t kk, uint32_t col) {
   return (kk >> 3) * 1024u + (kk & 7u) * 128u + ((((col >> 3) ^ (kk & 7u))) << 4) + (col & 7u) * 2u;
 }
 // Output staging (fp32, address order) with a 16-byte XOR swizzle against bank conflicts.
-__device__ __forceinline__ uint32_t stage_idx(uint32_t t) { return t ^ (((t >> 7) & 7u) << 2); }
+// XOR-linear: stage_idx(a ^ b) = stage_idx(a) ^ stage_idx(b), so an index assembled from disjoint
+// row and column bits can be swizzled part by part.
+__host__ __device__ __forceinline__ uint32_t stage_idx(uint32_t t) { return t ^ (((t >> 7) & 7u) << 2); }
 
 __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
@@ -544,12 +546,13 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_dense(float* __restrict__ 
     const uint32_t m = uint32_t(quad * 32 + lane);  // accumulator row = TMEM lane
     const uint32_t blk = m / KR, r = m % KR;
     const uint32_t s = r & uint32_t(M2 - 1), part = r >> KQ;
-    // address-order index of (row s, column blk*64 + cb*16 + q) = tr + tch[cb] + tcl[q]: the column
-    // map is a bit deposit, so it splits additively into the low 4 column bits and the rest
+    // address-order index of (row s, column blk*64 + cb*16 + q) = tr + tch[cb] + tcl[q]: the row
+    // and column maps are bit deposits onto disjoint bits, so the sum is an XOR and its staging
+    // index is stage_idx(tr ^ tch[cb]) ^ stage_idx(tcol[q]) (the latter precomputed in p.tcl)
     const uint32_t tr = s_trow[s];
-    uint32_t tch[4];
+    uint32_t sch[4];
 #pragma unroll
-    for (int cb = 0; cb < 4; ++cb) tch[cb] = s_tcol[blk * 64 + cb * 16];
+    for (int cb = 0; cb < 4; ++cb) sch[cb] = stage_idx(tr ^ uint32_t(s_tcol[blk * 64 + cb * 16]));
     for (uint64_t i = 0; i < my_tiles; ++i) {
       const uint32_t slot = uint32_t(i % kIoSlots);
       const uint32_t ds = uint32_t(i & 1), dpar = uint32_t((i >> 1) & 1);
@@ -575,8 +578,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_dense(float* __restrict__ 
         for (int cb = 0; cb < 4; ++cb)
 #pragma unroll
           for (int q = 0; q < 4; ++q) {
-            const uint32_t t = tr + tch[cb] + p.tcl[q * 4];
-            *reinterpret_cast<float4*>(st + stage_idx(t)) =
+            *reinterpret_cast<float4*>(st + (sch[cb] ^ p.tcl[q * 4])) =
                 make_float4(__uint_as_float(v[cb][4 * q]), __uint_as_float(v[cb][4 * q + 1]),
                             __uint_as_float(v[cb][4 * q + 2]), __uint_as_float(v[cb][4 * q + 3]));
           }
@@ -584,7 +586,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_dense(float* __restrict__ 
 #pragma unroll
         for (int cb = 0; cb < 4; ++cb)
 #pragma unroll
-          for (int q = 0; q < 16; ++q) st[stage_idx(tr + tch[cb] + p.tcl[q])] = __uint_as_float(v[cb][q]);
+          for (int q = 0; q < 16; ++q) st[sch[cb] ^ p.tcl[q]] = __uint_as_float(v[cb][q]);
       }
       const long long tc0 = clock64();
       w3 += tc0 - tb;
@@ -734,7 +736,7 @@ static void launch_tc_k(const LaunchEnv& env, float* re, float* im, uint32_t n, 
     for (uint32_t b = 0; b < n; ++b)
       if (col_rank[b] >= 0 && ((c >> col_rank[b]) & 1)) t |= 1u << rank_of(b);
     p.tcol[c] = uint16_t(t);
-    if (c < 16) p.tcl[c] = t;
+    if (c < 16) p.tcl[c] = stage_idx(t);
   }
   uint32_t rb = 0;
   while (rb < uint32_t(kTileBits) && tbits[rb] == rb) ++rb;
