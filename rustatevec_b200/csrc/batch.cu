@@ -65,7 +65,8 @@ constexpr uint32_t kTileStageBytes = 16384;   // the same for tile sweeps (four 
 enum BatchOp : uint32_t {
   OP_PHASE = 0, OP_1Q = 1, OP_D1 = 2, OP_CX = 3, OP_2Q = 4, OP_D2 = 5, OP_D1T = 6, OP_DT = 7, OP_D1P = 8, OP_DTP = 9,
   OP_DTAB = 10,  // the product of a phase's diagonal gates: one factor per register slot
-  OP_1QR = 11    // a real rotation [[C, -S], [S, C]] (the middle factor of a 1-qubit gate)
+  OP_1QR = 11,   // a real 1-qubit gate [[a, b], [c, d]] (RY, H, X): half the work of a general one
+  OP_1QX = 12    // [[a, i b], [i c, d]] with a..d real (RX, Y): half the work as well
 };
 constexpr uint32_t kTphSlots = 32;  // per-tile phase operations per pass (tile sweeps)
 constexpr uint32_t kTphSlotR = 12;  // reals per slot (the OP_D1 coefficient block of either precision)
@@ -340,46 +341,68 @@ __device__ __forceinline__ void gd2(Regs<R, RB>& v, const R* __restrict__ c) {
   }
 }
 
-// Real rotation [[C, -S], [S, C]] on register bit J: complex64 coefficients (C, C), (S, S), (-S, -S)
-// as float2 pairs; complex128 (C, S).
-template <int J, class R, int RB>
-__device__ __forceinline__ void g1qr(Regs<R, RB>& v, const R* __restrict__ c) {
+// A 1-qubit gate whose entries are each real or imaginary, on register bit J: X false, the real
+// matrix [[a, b], [c, d]]; X true, [[a, i b], [i c, d]]. Four real multiplies per amplitude instead
+// of eight. Coefficients: complex128 (a, b), (c, d); complex64 float2 pairs broadcast on the host,
+// (a, a), (b, b), (c, c), (d, d) and, for X, (-b, -b), (-c, -c) after them.
+template <int J, class R, int RB, bool X>
+__device__ __forceinline__ void g1qs(Regs<R, RB>& v, const R* __restrict__ c) {
   if constexpr (J < RB) {
     if constexpr (std::is_same<R, float>::value) {
       const float2* cc = reinterpret_cast<const float2*>(c);
+      const float2 A = cc[0], B = cc[1], Cc = cc[2], D = cc[3];
       if constexpr (J >= 1) {
         constexpr int HJ = 1 << (J - 1);
-        const float2 Cc = cc[0], Sc = cc[1], NS = cc[2];
 #pragma unroll
         for (int h = 0; h < (1 << RB) / 2; ++h) {
           if (h & HJ) continue;
           const int t = h | HJ;
           const float2 xr0 = v.r[h], xi0 = v.i[h], xr1 = v.r[t], xi1 = v.i[t];
-          v.r[h] = __ffma2_rn(NS, xr1, __fmul2_rn(Cc, xr0));
-          v.i[h] = __ffma2_rn(NS, xi1, __fmul2_rn(Cc, xi0));
-          v.r[t] = __ffma2_rn(Cc, xr1, __fmul2_rn(Sc, xr0));
-          v.i[t] = __ffma2_rn(Cc, xi1, __fmul2_rn(Sc, xi0));
+          if constexpr (X) {
+            const float2 NB = cc[4], NC = cc[5];
+            v.r[h] = __ffma2_rn(NB, xi1, __fmul2_rn(A, xr0));
+            v.i[h] = __ffma2_rn(B, xr1, __fmul2_rn(A, xi0));
+            v.r[t] = __ffma2_rn(D, xr1, __fmul2_rn(NC, xi0));
+            v.i[t] = __ffma2_rn(D, xi1, __fmul2_rn(Cc, xr0));
+          } else {
+            v.r[h] = __ffma2_rn(B, xr1, __fmul2_rn(A, xr0));
+            v.i[h] = __ffma2_rn(B, xi1, __fmul2_rn(A, xi0));
+            v.r[t] = __ffma2_rn(D, xr1, __fmul2_rn(Cc, xr0));
+            v.i[t] = __ffma2_rn(D, xi1, __fmul2_rn(Cc, xi0));
+          }
         }
       } else {
-        const float Cs = cc[0].x, Ss = cc[1].x;
+        const float a = A.x, b = B.x, cs = Cc.x, d = D.x;
 #pragma unroll
         for (int h = 0; h < (1 << RB) / 2; ++h) {
           const float xr0 = v.r[h].x, xi0 = v.i[h].x, xr1 = v.r[h].y, xi1 = v.i[h].y;
-          v.r[h] = make_float2(fmaf(-Ss, xr1, Cs * xr0), fmaf(Cs, xr1, Ss * xr0));
-          v.i[h] = make_float2(fmaf(-Ss, xi1, Cs * xi0), fmaf(Cs, xi1, Ss * xi0));
+          if constexpr (X) {
+            v.r[h] = make_float2(fmaf(-b, xi1, a * xr0), fmaf(d, xr1, -cs * xi0));
+            v.i[h] = make_float2(fmaf(b, xr1, a * xi0), fmaf(d, xi1, cs * xr0));
+          } else {
+            v.r[h] = make_float2(fmaf(b, xr1, a * xr0), fmaf(d, xr1, cs * xr0));
+            v.i[h] = make_float2(fmaf(b, xi1, a * xi0), fmaf(d, xi1, cs * xi0));
+          }
         }
       }
     } else {
-      const R Cs = c[0], Ss = c[1];
+      const R a = c[0], b = c[1], cs = c[2], d = c[3];
 #pragma unroll
       for (int s = 0; s < (1 << RB); ++s) {
         if (s & (1 << J)) continue;
         const int t = s | (1 << J);
         const R xr0 = v.re(s), xi0 = v.im(s), xr1 = v.re(t), xi1 = v.im(t);
-        v.re(s) = fma(-Ss, xr1, Cs * xr0);
-        v.im(s) = fma(-Ss, xi1, Cs * xi0);
-        v.re(t) = fma(Cs, xr1, Ss * xr0);
-        v.im(t) = fma(Cs, xi1, Ss * xi0);
+        if constexpr (X) {
+          v.re(s) = fma(-b, xi1, a * xr0);
+          v.im(s) = fma(b, xr1, a * xi0);
+          v.re(t) = fma(d, xr1, -cs * xi0);
+          v.im(t) = fma(d, xi1, cs * xr0);
+        } else {
+          v.re(s) = fma(b, xr1, a * xr0);
+          v.im(s) = fma(b, xi1, a * xi0);
+          v.re(t) = fma(d, xr1, cs * xr0);
+          v.im(t) = fma(d, xi1, cs * xi0);
+        }
       }
     }
   }
@@ -434,11 +457,20 @@ __device__ __forceinline__ void apply_instr(const Instr& in, Regs<R, RB>* v, con
       break;
     case OP_1QR:
       switch (in.a) {
-        case 0: for (int g = 0; g < G; ++g) g1qr<0, R, RB>(v[g], c); break;
-        case 1: for (int g = 0; g < G; ++g) g1qr<1, R, RB>(v[g], c); break;
-        case 2: for (int g = 0; g < G; ++g) g1qr<2, R, RB>(v[g], c); break;
-        case 3: for (int g = 0; g < G; ++g) g1qr<3, R, RB>(v[g], c); break;
-        case 4: for (int g = 0; g < G; ++g) g1qr<4, R, RB>(v[g], c); break;
+        case 0: for (int g = 0; g < G; ++g) g1qs<0, R, RB, false>(v[g], c); break;
+        case 1: for (int g = 0; g < G; ++g) g1qs<1, R, RB, false>(v[g], c); break;
+        case 2: for (int g = 0; g < G; ++g) g1qs<2, R, RB, false>(v[g], c); break;
+        case 3: for (int g = 0; g < G; ++g) g1qs<3, R, RB, false>(v[g], c); break;
+        case 4: for (int g = 0; g < G; ++g) g1qs<4, R, RB, false>(v[g], c); break;
+      }
+      break;
+    case OP_1QX:
+      switch (in.a) {
+        case 0: for (int g = 0; g < G; ++g) g1qs<0, R, RB, true>(v[g], c); break;
+        case 1: for (int g = 0; g < G; ++g) g1qs<1, R, RB, true>(v[g], c); break;
+        case 2: for (int g = 0; g < G; ++g) g1qs<2, R, RB, true>(v[g], c); break;
+        case 3: for (int g = 0; g < G; ++g) g1qs<3, R, RB, true>(v[g], c); break;
+        case 4: for (int g = 0; g < G; ++g) g1qs<4, R, RB, true>(v[g], c); break;
       }
       break;
     case OP_D1P: {
@@ -1018,32 +1050,26 @@ void push_coef(BatchPlan& bp, const cd& v) {
   bp.coef.push_back(v.imag());
 }
 
-// A unitary 2x2 as Dl R Dr: Dl = diag(l0, l1), R = [[C, -S], [S, C]] with C, S >= 0, Dr =
-// diag(1, r1). False when the matrix is not of that form to 1e-12 (then it stays a general gate).
-bool real_rotation(const std::vector<cd>& a, cd& l0, cd& l1, cd& r1, double& C, double& S) {
-  const cd u00 = a[0], u01 = a[1], u10 = a[2], u11 = a[3];
-  C = std::abs(u00);
-  S = std::abs(u10);
-  constexpr double tol = 1e-14;
-  if (C > tol && S > tol) {
-    l0 = u00 / C;
-    l1 = u10 / S;
-    r1 = u11 / (l1 * C);
-  } else if (S > tol) {  // off-diagonal: u00 = u11 = 0
-    l1 = u10 / S;
-    r1 = cd(1, 0);
-    l0 = -u01 / S;
-  } else if (C > tol) {  // diagonal
-    l0 = u00 / C;
-    r1 = cd(1, 0);
-    l1 = u11 / C;
-  } else {
-    return false;
+// A 2x2 gate whose entries are each real or imaginary: 1 for a real matrix [[a, b], [c, d]], 2 for
+// [[a, i b], [i c, d]] with a..d real (k = a, b, c, d), 0 otherwise. Parts within 1e-15 of the
+// largest entry's magnitude count as zero.
+int split_form(const std::vector<cd>& u, double k[4]) {
+  double mx = 0;
+  for (int e = 0; e < 4; ++e) mx = std::max(mx, std::abs(u[e]));
+  const double tol = 1e-15 * mx;
+  auto z = [&](double x) { return std::abs(x) <= tol; };
+  if (z(u[0].imag()) && z(u[1].imag()) && z(u[2].imag()) && z(u[3].imag())) {
+    for (int e = 0; e < 4; ++e) k[e] = u[e].real();
+    return 1;
   }
-  const double err = std::max({std::abs(l0 * C - u00), std::abs(-l0 * S * r1 - u01), std::abs(l1 * S - u10),
-                               std::abs(l1 * C * r1 - u11), std::abs(std::abs(l0) - 1.0), std::abs(std::abs(l1) - 1.0),
-                               std::abs(std::abs(r1) - 1.0)});
-  return err <= 1e-12;
+  if (z(u[0].imag()) && z(u[3].imag()) && z(u[1].real()) && z(u[2].real())) {
+    k[0] = u[0].real();
+    k[1] = u[1].imag();
+    k[2] = u[2].imag();
+    k[3] = u[3].real();
+    return 2;
+  }
+  return 0;
 }
 
 // Splits a pass's gates into register phases and appends them to the plan's program.
@@ -1141,16 +1167,18 @@ void emit_phases(BatchPlan& bp, const std::vector<LGate>& G, uint32_t nlocal, st
     const size_t phase_idx = bp.phases.size(), phase_pc = bp.prog.size();
     bp.prog.push_back(Instr{OP_PHASE, 0, 0, uint32_t(bp.phases.size() - phase_base)});
     bp.phases.push_back(D);
-    // Emission. Non-diagonal operations keep their order (1-qubit real rotations as OP_1QR).
+    // Emission. Non-diagonal operations keep their order (1-qubit gates of split form as OP_1QR /
+    // OP_1QX).
     // Diagonal factors on register bits (LK_D1, LK_D2) are multiplied into per-slot tables: a factor
     // may sit anywhere between the last non-diagonal operation on its bits before it and the first
     // one after it, and the tables go where the fewest points cover every factor's range (interval
     // stabbing, ends first).
     const uint32_t nslot = 1u << bp.rb;
     struct Op {
-      const LGate* g;  // nullptr: a real rotation (kind LK_1QR) on register bit rbit
+      const LGate* g;  // nullptr: a split-form 1-qubit gate on register bit rbit
       uint32_t rbit;
-      double C, S;
+      int form;        // split_form: 1 real, 2 imaginary off-diagonal
+      double k[4];
     };
     struct Fac {
       uint32_t rb0, rb1, nb;  // register bits (nb = 1 or 2)
@@ -1199,13 +1227,12 @@ void emit_phases(BatchPlan& bp, const std::vector<LGate>& G, uint32_t nlocal, st
         continue;
       }
       if (g.kind == LK_1Q) {
-        // a real rotation (Dl = Dr = identity, e.g. RY) costs half a general 1-qubit gate; with
-        // phase factors the extra table work measured more than it saved, so those stay general
-        cd l0, l1, r1;
-        double C, S;
-        if (real_rotation(a, l0, l1, r1, C, S) && std::abs(l0 - 1.0) + std::abs(l1 - 1.0) + std::abs(r1 - 1.0) < 1e-15) {
-          const uint32_t rbit = uint32_t(regbit[g.p[0]]);
-          add_nondiag(Op{nullptr, rbit, C, S}, 1u << rbit);
+        // entries each real or imaginary (RY, H, X; RX, Y): half the work of a general 1-qubit gate
+        Op op{nullptr, 0, 0, {0, 0, 0, 0}};
+        op.form = split_form(a, op.k);
+        if (op.form != 0) {
+          op.rbit = uint32_t(regbit[g.p[0]]);
+          add_nondiag(op, 1u << op.rbit);
           continue;
         }
       }
@@ -1215,7 +1242,7 @@ void emit_phases(BatchPlan& bp, const std::vector<LGate>& G, uint32_t nlocal, st
         for (uint32_t p = 0; p < nlocal; ++p)
           if (((lm >> p) & 1u) && regbit[p] >= 0) bits |= 1u << regbit[p];
       }
-      add_nondiag(Op{&g, 0, 0, 0}, bits);  // diagonal kinds outside tables constrain nothing
+      add_nondiag(Op{&g, 0, 0, {0, 0, 0, 0}}, bits);  // diagonal kinds outside tables constrain nothing
     }
     for (Fac& f : facs)
       if (f.hi == SIZE_MAX) f.hi = ops.size();
@@ -1249,14 +1276,18 @@ void emit_phases(BatchPlan& bp, const std::vector<LGate>& G, uint32_t nlocal, st
       }
       bp.prog.push_back(Instr{OP_DTAB, 0, 0, uint32_t(base - coef_base)});
     };
-    auto emit_rotation = [&](const Op& op) {
-      Instr in{OP_1QR, op.rbit, 0, uint32_t(bp.coef.size() / 2 - coef_base)};
-      if (bp.dtype == QSVB_C64) {  // pre-broadcast (C, C), (S, S), (-S, -S)
-        push_coef(bp, cd(op.C, op.C));
-        push_coef(bp, cd(op.S, op.S));
-        push_coef(bp, cd(-op.S, -op.S));
+    auto emit_split = [&](const Op& op) {
+      Instr in{op.form == 2 ? uint32_t(OP_1QX) : uint32_t(OP_1QR), op.rbit, 0,
+               uint32_t(bp.coef.size() / 2 - coef_base)};
+      if (bp.dtype == QSVB_C64) {  // pre-broadcast pairs (a, a), (b, b), (c, c), (d, d) [, (-b, -b), (-c, -c)]
+        for (int e = 0; e < 4; ++e) push_coef(bp, cd(op.k[e], op.k[e]));
+        if (op.form == 2) {
+          push_coef(bp, cd(-op.k[1], -op.k[1]));
+          push_coef(bp, cd(-op.k[2], -op.k[2]));
+        }
       } else {
-        push_coef(bp, cd(op.C, op.S));
+        push_coef(bp, cd(op.k[0], op.k[1]));
+        push_coef(bp, cd(op.k[2], op.k[3]));
       }
       bp.prog.push_back(in);
     };
@@ -1367,7 +1398,7 @@ void emit_phases(BatchPlan& bp, const std::vector<LGate>& G, uint32_t nlocal, st
       if (!tables[j].empty() && !identity(tables[j])) emit_table(tables[j]);
       if (j == ops.size()) break;
       if (ops[j].g) emit_one(*ops[j].g);
-      else emit_rotation(ops[j]);
+      else emit_split(ops[j]);
     }
     bp.phases[phase_idx].ninstr = uint32_t(bp.prog.size() - phase_pc - 1);
   }
@@ -1946,7 +1977,9 @@ void tile_prepare(Sweep& s, uint32_t n, int dtype) {
     };
     if (nout == 0) {
       G.push_back(LGate{kind, {uint32_t(pos[g.q[0]]), g.m == 2 ? uint32_t(pos[g.q[1]]) : 0u}, &hg[i]});
-      flops += dim * (kind == LK_1Q ? 16.0 : kind == LK_2Q ? 32.0 : kind == LK_CX ? 0.0 : 6.0);
+      double k[4];
+      const double f1q = split_form(g.a, k) != 0 ? 8.0 : 16.0;
+      flops += dim * (kind == LK_1Q ? f1q : kind == LK_2Q ? 32.0 : kind == LK_CX ? 0.0 : 6.0);
     } else {
       QSVB_REQUIRE(kind == LK_D1 || kind == LK_D2, "only diagonal gates may reach qubits outside the tile");
       LGate lg{};
