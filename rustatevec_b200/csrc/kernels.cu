@@ -308,9 +308,12 @@ __global__ void __launch_bounds__(kThreads) k_phase(R* __restrict__ re, R* __res
 // Phase polynomial in Ising form for states of >= 12 qubits. Any product of <= 2-qubit diagonal
 // phases is exp(i theta(x)) with theta = C + sum_q h_q z_q + sum_(a<b) J_ab z_a z_b, z_q = 1 - 2 x_q.
 // A CTA walks chunks of 4096 consecutive amplitudes. The edge terms inside the low 12 bits are
-// tabulated once per CTA (32 KB); per chunk, the high bits are constant, so the high-high terms fold
-// into one scalar and the high-low edges into the linear coefficients of the low bits, kept as two
-// 64-entry tables. Each amplitude then costs three shared loads, three adds and one FP64 sincos.
+// tabulated once per CTA; per chunk, the high bits are constant, so the high-high terms fold into one
+// scalar and the high-low edges into the linear coefficients of the low bits, kept as two 64-entry
+// tables. All three tables hold unit complex factors exp(i angle) (the chunk scalar folded into the
+// first 64-entry one), so an amplitude's factor is a product of three shared loads: two complex
+// multiplies in FP64 instead of one sincos per amplitude. The low-bit table is 64 KB of dynamic
+// shared memory.
 constexpr int kIsingMaxEdges = 160;
 constexpr int kIsingChunkBits = 12;
 struct IsingP {
@@ -327,15 +330,18 @@ template <class R>
 __global__ void __launch_bounds__(kThreads) k_ising(R* __restrict__ re, R* __restrict__ im, uint64_t nchunks,
                                                     IsingP p) {
   constexpr int CB = kIsingChunkBits, CH = 1 << CB, N = VecT<R>::N;
-  __shared__ double tll[CH];
-  __shared__ double l1[64], l2[64], hp[CB];
+  extern __shared__ double2 tll[];  // CH entries: (cos, sin) of the low-bit edge phases
+  __shared__ double2 l1[64], l2[64];
+  __shared__ double hp[CB];
   __shared__ double thh;
   const int tid = threadIdx.x;
   for (int l = tid; l < CH; l += kThreads) {
     double s = 0.0;
     for (uint32_t e = 0; e < p.nedges; ++e)
       if (p.eb[e] < CB) s += p.J[e] * zsign(uint64_t(l), p.ea[e]) * zsign(uint64_t(l), p.eb[e]);
-    tll[l] = s;
+    double sn, cs;
+    sincos(s, &sn, &cs);
+    tll[l] = make_double2(cs, sn);
   }
   for (uint64_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
     const uint64_t base = ch << CB;
@@ -355,16 +361,19 @@ __global__ void __launch_bounds__(kThreads) k_ising(R* __restrict__ re, R* __res
     }
     __syncthreads();
     if (tid < 64) {
-      double v = 0.0;
+      double v = thh;
       for (int q = 0; q < 6; ++q) v += hp[q] * zsign(uint64_t(tid), q);
-      l1[tid] = v;
+      double sn, cs;
+      sincos(v, &sn, &cs);
+      l1[tid] = make_double2(cs, sn);
     } else if (tid < 128) {
       double v = 0.0;
       for (int q = 0; q < 6; ++q) v += hp[6 + q] * zsign(uint64_t(tid - 64), q);
-      l2[tid - 64] = v;
+      double sn, cs;
+      sincos(v, &sn, &cs);
+      l2[tid - 64] = make_double2(cs, sn);
     }
     __syncthreads();
-    const double t0 = thh;
     for (int v = tid; v < CH / N; v += kThreads) {
       const uint32_t l = uint32_t(v * N);
       R xr[N], xi[N];
@@ -373,9 +382,9 @@ __global__ void __launch_bounds__(kThreads) k_ising(R* __restrict__ re, R* __res
 #pragma unroll
       for (int e = 0; e < N; ++e) {
         const uint32_t x = l + e;
-        const double th = t0 + tll[x] + l1[x & 63u] + l2[x >> 6];
-        double sn, cs;
-        sincos(th, &sn, &cs);
+        const double2 f0 = tll[x], f1 = l1[x & 63u], f2 = l2[x >> 6];
+        const double ur = f0.x * f1.x - f0.y * f1.y, ui = f0.x * f1.y + f0.y * f1.x;
+        const double cs = ur * f2.x - ui * f2.y, sn = ur * f2.y + ui * f2.x;
         const double a = double(xr[e]), c = double(xi[e]);
         xr[e] = R(cs * a - sn * c);
         xi[e] = R(cs * c + sn * a);
@@ -947,7 +956,9 @@ void launch_phase(const LaunchEnv& env, R* re, R* im, uint32_t n, const Sweep& s
       p.J[e] = js[e];
     }
     const uint64_t nchunks = dim >> kIsingChunkBits;
-    k_ising<R><<<grid_for(nchunks, 1, env.num_sms, 4), kThreads, 0, env.stream>>>(re, im, nchunks, p);
+    const size_t tsm = sizeof(double2) << kIsingChunkBits;
+    QSVB_CK(cudaFuncSetAttribute(k_ising<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(tsm)));
+    k_ising<R><<<grid_for(nchunks, 1, env.num_sms, 3), kThreads, tsm, env.stream>>>(re, im, nchunks, p);
     check_launch();
     return;
   }
