@@ -698,6 +698,9 @@ KERNEL_CASES = {
     "tile_h_all": ("f32", lambda n: [("h", [q]) for q in range(13)]),
     "tile_h_all_c128": ("f64", lambda n: [("h", [q]) for q in range(12)]),
     "1q_low_c128": ("f64", lambda n: [("h", [1])]),
+    "dense3_c128_high": ("f64", lambda n: [("u3", [n - 16, n - 15, n - 14])]),
+    "dense4_c128": ("f64", lambda n: [("u4", [0, 1, 2, 3])]),
+    "dense5_c128": ("f64", lambda n: [("u5", [2, 3, 9, 10, 20])]),
     "dense4_c128": ("f64", lambda n: [("u4", [0, 1, 2, 3])]),
 }
 
