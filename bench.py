@@ -36,7 +36,7 @@ WORKLOAD = f"random brickwork {N_QUBITS}q depth {DEPTH}, complex64, Haar SU(2) +
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum, one ncu capture of one launch at 26
 # qubits, scaled by the amplitudes a launch processes) per algorithmic byte, for the kernels the
 # roofline object can name
-TRAFFIC_PER_ALGORITHMIC_BYTE = {"dense_tc": (537.137408 + 477.872384) / 1073.741824,
+TRAFFIC_PER_ALGORITHMIC_BYTE = {"dense_tc": (536.995584 + 477.506560) / 1073.741824,
                                 "1q": (536.916992 + 479.222272) / 1073.741824}
 
 
