@@ -103,10 +103,11 @@ class ClockSampler:
 # ------------------------------------------------------------------ CPU baseline (oracle CpuBackend)
 def cpu_baseline(circuit, budget_s: float = 15.0) -> dict:
     """Time the CpuBackend restatement (OpenMP, all host threads) on the reference-fused circuit
-    (FusionConfig default max_qubits=4, composed in f32 as qsv does for Circuit<f32>); run ops
-    until the time budget is spent and extrapolate to the whole circuit."""
+    (FusionConfig default max_qubits=4, composed in f32 as qsv does for Circuit<f32>). Ops are
+    sampled round-robin over their arities (a seeded order within each arity) until the time budget
+    is spent; the estimate is sum over arities of (ops of that arity) x (mean time of the sampled
+    ones), so it does not depend on which ops come first in the circuit."""
     import oracle
-    from rustatevec_b200.circuit import Circuit
     n = circuit.n_qubits()
     arity, qubits, mats = oracle.fuse(circuit, 4, oracle.F32)
     nops = len(arity)
@@ -124,19 +125,32 @@ def cpu_baseline(circuit, budget_s: float = 15.0) -> dict:
                     np.ascontiguousarray(mats[offs_m[i]:offs_m[i + 1]]),
                     np.ascontiguousarray(qubits[offs_q[i]:offs_q[i + 1]]), m)
 
-    run_op(0)  # first touch of the pages, untimed
+    rng = np.random.default_rng(SEED)
+    classes = {}
+    for i in rng.permutation(nops):
+        classes.setdefault(int(arity[i]), []).append(int(i))
+    order = []
+    for r in range(max(len(v) for v in classes.values())):
+        for m in sorted(classes):
+            if r < len(classes[m]):
+                order.append(classes[m][r])
+    run_op(order[0])  # first touch of the pages, untimed
+    times = {m: [] for m in classes}
     t0 = time.perf_counter()
-    done = 0
-    for i in range(1, nops):
+    for i in order:
+        t = time.perf_counter()
         run_op(i)
-        done += 1
+        times[int(arity[i])].append(time.perf_counter() - t)
         if time.perf_counter() - t0 > budget_s:
             break
     dt = time.perf_counter() - t0
-    per_op = dt / max(done, 1)
-    return {"value": per_op * nops, "unit": "s", "cores": cores, "kind": "port",
+    done = sum(len(v) for v in times.values())
+    mean_all = dt / max(done, 1)
+    est = sum(len(classes[m]) * (float(np.mean(times[m])) if times[m] else mean_all) for m in classes)
+    hist = ", ".join(f"{len(times[m])}/{len(classes[m])} of arity {m}" for m in sorted(classes))
+    return {"value": est, "unit": "s", "cores": cores, "kind": "port",
             "sample": f"{done} of {nops} fused ops (qsv fuse, max_qubits=4, f32) of the {n}q circuit timed "
-                      f"({dt:.1f} s, OpenMP x{cores}); value = mean per op x {nops} ops"}
+                      f"({hist}; {dt:.1f} s, OpenMP x{cores}); value = sum over arities of ops x mean time"}
 
 
 # ------------------------------------------------------------------ GPU
