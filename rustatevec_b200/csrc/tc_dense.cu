@@ -59,7 +59,8 @@ constexpr int kMmaWarp = kCvtWarps + 1;                       // warp 9
 constexpr int kEpiWarp0 = kCvtWarps + 2;                      // warps 10..13 (lane quadrants 2,3,0,1)
 constexpr int kTcThreads = (kCvtWarps + 2 + kEpiWarps) * 32;
 constexpr int kBSlots = 2;
-constexpr int kIoSlots = 4;
+constexpr int kIoSlots = 4;                 // input tiles in flight (released once converted)
+constexpr int kIoBufs = kIoSlots + 1;       // + the epilogue's output staging
 constexpr int kTmemCols = 256;                                // two 64-column accumulators + Whi + Wlo
 constexpr uint32_t kTmemAHi = 128, kTmemALo = 192;           // A operand columns (64 each)
 constexpr int kVC = kTileAmps / 4 / kCvtThreads;              // float4 per component per converter
@@ -68,8 +69,9 @@ constexpr uint32_t kABytes = 128u * kMmaK * 2u;               // one of Whi / Wl
 constexpr uint32_t kBBytes = uint32_t(kMmaN) * kMmaK * 2u;    // one of Xhi / Xlo
 constexpr uint32_t kIoBytes = kTileAmps * 8u;                 // re [4096] + im [4096] fp32
 constexpr long long kWaitBudget = 1ll << 31;                  // clock64 cycles (~1 s)
-constexpr size_t kTcSmem = 1024 + kBSlots * 2 * size_t(kBBytes) + kIoSlots * size_t(kIoBytes) +
+constexpr size_t kTcSmem = 1024 + kBSlots * 2 * size_t(kBBytes) + kIoBufs * size_t(kIoBytes) +
                            144 + 64 * 8 + 3 * 64 * 2 + 256 * 2 + 64 * 2;
+static_assert(kTcSmem <= 232448, "tensor-core sweep: shared memory above the 227 KB per-block limit");
 
 struct TcParams {
   uint32_t hibits[6];      // tile bits above the 6 lowest state bits (ascending)
@@ -189,6 +191,19 @@ __device__ __forceinline__ void tmem_st64(uint32_t addr, const uint32_t (&r)[64]
 __device__ __forceinline__ void named_sync(uint32_t id, uint32_t nthreads) {
   asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
 }
+// Named barrier that also returns whether `v` holds for every participating thread.
+__device__ __forceinline__ bool named_all(uint32_t id, uint32_t nthreads, bool v) {
+  uint32_t r;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\t"
+      "setp.ne.u32 p, %1, 0;\n\t"
+      "bar.red.and.pred q, %2, %3, p;\n\t"
+      "selp.u32 %0, 1, 0, q;\n\t}\n"
+      : "=r"(r)
+      : "r"(uint32_t(v)), "r"(id), "r"(nthreads)
+      : "memory");
+  return r != 0;
+}
 
 __device__ __forceinline__ void split_bf16(float x, __nv_bfloat16& hi, __nv_bfloat16& lo) {
   hi = __float2bfloat16_rn(x);
@@ -275,9 +290,10 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_dense(float* __restrict__ 
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint8_t* bbuf = smem;                            // slot s: hi at bbuf + s*2*B, lo right after
   float* io = reinterpret_cast<float*>(bbuf + kBSlots * 2 * kBBytes);  // slot s: re [4096], im [4096]
-  uint64_t* bars = reinterpret_cast<uint64_t*>(io + kIoSlots * 2 * kTileAmps);
+  float* ostage = io + kIoSlots * 2 * kTileAmps;  // the epilogue's result, re [4096] then im [4096]
+  uint64_t* bars = reinterpret_cast<uint64_t*>(io + kIoBufs * 2 * kTileAmps);
   uint64_t* iofull = bars;       // [4] TMA complete_tx -> converters
-  uint64_t* ioempty = bars + 4;  // [4] epilogue -> producer
+  uint64_t* ioempty = bars + 4;  // [4] converters -> producer
   uint64_t* bfull = bars + 8;    // [2] converters -> MMA
   uint64_t* bfree = bars + 10;   // [2] MMA commit -> converters
   uint64_t* dfull = bars + 12;   // [2] MMA commit -> epilogue
@@ -312,7 +328,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_dense(float* __restrict__ 
   if (tid == 0) {
     for (int s = 0; s < kIoSlots; ++s) {
       mbar_init(&iofull[s], 1);
-      mbar_init(&ioempty[s], kEpiThreads);
+      mbar_init(&ioempty[s], kCvtThreads);
     }
     for (int s = 0; s < 2; ++s) {
       mbar_init(&bfull[s], kCvtThreads);
@@ -509,6 +525,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_dense(float* __restrict__ 
       }
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       mbar_arrive(&bfull[bs]);
+      mbar_arrive(&ioempty[slot]);  // this thread's reads of the input slot are done (fenced above)
     }
   } else if (warp == kMmaWarp) {
     // ============================ MMA issue: one lane
@@ -554,9 +571,11 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_dense(float* __restrict__ 
 #pragma unroll
     for (int cb = 0; cb < 4; ++cb) sch[cb] = stage_idx(tr ^ uint32_t(s_tcol[blk * 64 + cb * 16]));
     for (uint64_t i = 0; i < my_tiles; ++i) {
-      const uint32_t slot = uint32_t(i % kIoSlots);
       const uint32_t ds = uint32_t(i & 1), dpar = uint32_t((i >> 1) & 1);
-      if (!mbar_wait_t(&dfull[ds], dpar, w0)) {
+      const bool ready = mbar_wait_t(&dfull[ds], dpar, w0);
+      // one decision for all epilogue threads (they meet at named barriers below); reaching this
+      // barrier also means every thread's reads of the previous tile's staging are done
+      if (!named_all(2, kEpiThreads, ready)) {
         atomicExch(err, 1);
         break;
       }
@@ -571,8 +590,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_dense(float* __restrict__ 
       mbar_arrive(&dfree[ds]);  // accumulator may be overwritten now
       const long long tb = clock64();
       w2 += tb - ta;
-      // the converters finished reading this slot before the MMAs that produced v were issued
-      float* st = io + slot * 2 * kTileAmps + part * kTileAmps;
+      float* st = ostage + part * kTileAmps;
       if constexpr (BM == 0) {
 #pragma unroll
         for (int cb = 0; cb < 4; ++cb)
@@ -593,7 +611,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_dense(float* __restrict__ 
       named_sync(1, kEpiThreads);  // the whole result is staged
       const long long ts = clock64();
       w4 += ts - tc0;
-      const float* sre = io + slot * 2 * kTileAmps;
+      const float* sre = ostage;
       const uint64_t base = tile_base(blockIdx.x + i * gridDim.x);
 #pragma unroll
       for (int j = 0; j < kVE; ++j) {
@@ -603,9 +621,6 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_dense(float* __restrict__ 
         __stcs(reinterpret_cast<float4*>(re + a), *reinterpret_cast<const float4*>(sre + si));
         __stcs(reinterpret_cast<float4*>(im + a), *reinterpret_cast<const float4*>(sre + kTileAmps + si));
       }
-      // this thread's reads of the slot are done; the producer may refill it once all 128 arrive
-      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      mbar_arrive(&ioempty[slot]);
       w1 += clock64() - ts;
     }
   }
