@@ -709,6 +709,7 @@ KERNEL_CASES = {
     "tc6_bit1": ("f32", lambda n: [("u6", [1, 2, 7, 8, 9, 10])]),
     "tc6_bit0": ("f32", lambda n: [("u6", [0, 3, 4, 8, 9, 12])]),
     "phase15": ("f32", lambda n: [("cz", [i, i + 1]) for i in range(0, n - 1, 2)]),
+    "phase15_c128": ("f64", lambda n: [("cz", [i, i + 1]) for i in range(0, n - 1, 2)]),
     "tile_h_all": ("f32", lambda n: [("h", [q]) for q in range(13)]),
     "tile_h_all_c128": ("f64", lambda n: [("h", [q]) for q in range(12)]),
     "1q_low_c128": ("f64", lambda n: [("h", [1])]),
