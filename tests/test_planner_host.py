@@ -53,6 +53,23 @@ def test_learned_planner_choices_with_the_trained_model(built):
         tuning.install(None)
 
 
+def test_predictions_above_the_trained_size_respect_the_memory_floor(built):
+    """The cost model is trained on states of at most 30 qubits; larger states are predicted as the
+    same sweep on a 30-qubit state times the amplitude ratio, so no plan is predicted faster than
+    its algorithmic bytes at the measured copy bandwidth (about 6.55 TB/s)."""
+    doc = tuning.load()
+    if doc is None:
+        pytest.skip("no trained model in the tree")
+    try:
+        for circ, dtype in ((qaoa_maxcut(33, 4, 0), L.C128), (qaoa_maxcut(31, 2, 0), L.C128),
+                            (qft(32), L.C64), (brickwork(32, 6, 0), L.C64)):
+            for planner, k in ((L.PLAN_GREEDY, 4), (L.PLAN_WINDOW, 5), (L.PLAN_LEARNED, 6)):
+                st = dry(circ, planner, k, dtype=dtype)
+                assert st["predicted_seconds"] >= st["algorithmic_bytes"] / 6.6e12, (circ.n_qubits(), planner)
+    finally:
+        tuning.install(None)
+
+
 def test_dry_run_rejects_bad_input(built):
     st = L.PlanStats()
     assert L.lib().qsvb_plan_dry_run(None, 0, None, C.byref(st)) == L.QSVB_E_INVALID
