@@ -14,20 +14,23 @@
 // contiguous run of >= 64 amplitudes) and all 128 accumulator lanes carry results.
 //
 // One persistent CTA per SM runs a warp-specialized pipeline over its tiles:
-//   producer warp (1 lane): TMA bulk copies (cp.async.bulk, one per contiguous run, no
-//     multicast) of the tile's re/im runs into one of three fp32 staging slots, completing on
-//     that slot's mbarrier;
+//   producer warp: one tiled TMA (a tensor map whose dimensions are the runs of tile bits) or
+//     bulk copies (cp.async.bulk, one per contiguous run; no multicast anywhere) of the tile's
+//     re/im into one of four fp32 input slots, completing on that slot's mbarrier;
 //   converter warps (8): split the staged tile into bf16 hi/lo and store it into one of two B
-//     buffers (128-byte swizzle; MN-major when state bits 0-1 are tile columns, K-major when
-//     they are the gate's two lowest qubits);
+//     buffers (128-byte swizzle; the layout is a template parameter: MN-major when state bits 0-1
+//     are tile columns, K-major when they are the gate's two lowest qubits, K-major assembled by
+//     lane-pair shuffles when bit 0 is a column and bit 1 the gate's lowest qubit, K-major row
+//     pairs otherwise), then release the input slot to the producer;
 //   MMA warp (1 lane): 24 tcgen05.mma per tile into one of two TMEM accumulators (128 lanes x
 //     64 fp32 columns); tcgen05.commit frees the B buffer and hands the accumulator on;
-//   epilogue warps (4, one per TMEM lane quadrant): tcgen05.ld the accumulator, write the result
-//     over the tile's own staging slot (address order, 16-byte XOR swizzle), release the
-//     accumulator, write the tile back with coalesced 16-byte streaming stores, release the slot.
+//   epilogue warps (4, one per TMEM lane quadrant): tcgen05.ld the accumulator, release it, write
+//     the result into the output staging buffer (address order, 16-byte XOR swizzle) and write
+//     the tile back with coalesced 16-byte streaming stores.
 // A (Whi, Wlo; K-major, 128-byte swizzle) is packed on the host in the exact shared-memory byte
 // layout and copied in once per CTA. Every mbarrier wait is bounded: a wait that runs out sets the
-// context error flag and that role stops; the host reports QSVB_E_TIMEOUT.
+// context error flag and that role stops (the epilogue threads vote before their named barriers,
+// so they stop together); the host reports QSVB_E_TIMEOUT.
 
 #include <cuda.h>
 #include <cudaTypedefs.h>
