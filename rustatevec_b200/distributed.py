@@ -264,7 +264,10 @@ class TorchComm:
         self.dist, self.torch, self.group = dist, torch, group
         self.rank = dist.get_rank(group)
         self.size = dist.get_world_size(group)
-        self.device = device if device is not None else torch.device("cpu")
+        if device is None:  # NCCL reduces device tensors only
+            nccl = dist.get_backend(group) == "nccl"
+            device = torch.device("cuda", torch.cuda.current_device()) if nccl else torch.device("cpu")
+        self.device = device
 
     def exchange(self, send, recv, peer: int):
         """Send the tensors ``send`` to ``peer`` and receive the same shapes into ``recv``."""
