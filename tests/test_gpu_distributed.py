@@ -10,7 +10,7 @@ from rustatevec_b200 import B200Backend
 from rustatevec_b200.circuit import Circuit
 from rustatevec_b200 import gate as G
 from rustatevec_b200.circuits import brickwork, ghz_chain, qaoa_maxcut, qft, random_circuit
-from rustatevec_b200.distributed import B200SliceEngine, DistributedState
+from rustatevec_b200.distributed import B200SliceEngine, DistributedState, TorchComm
 
 pytestmark = pytest.mark.gpu
 
@@ -67,3 +67,34 @@ def test_matches_the_single_state_engine(be):
     assert abs(np.vdot(want, got)) ** 2 > 1 - 10 * TOL[be.precision]
     assert abs(ds.norm_sqr() - 1) < 10 * TOL[be.precision]
     ds.free()
+
+
+def test_nccl_communicator_on_one_rank(be):
+    """TorchComm over a one-rank NCCL group (reductions and the gather run through NCCL on the
+    device); the block exchange itself needs two GPUs and is covered by the gloo tests."""
+    import datetime
+    import socket
+    import torch.distributed as dist
+    if dist.is_initialized():
+        pytest.skip("a process group already exists")
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1,
+                            timeout=datetime.timedelta(seconds=60))
+    try:
+        comm = TorchComm()
+        assert comm.device.type == "cuda" and comm.size == 1
+        n = 12
+        c = random_circuit(n, 80, 4)
+        ds = DistributedState(n, 0, B200SliceEngine(be), comm)
+        ds.init_basis(0)
+        ds.run(c)
+        re, im = oracle.run(c, oracle.REF, oracle.F64)
+        want = re + 1j * im
+        assert np.max(np.abs(ds.gather() - want)) < TOL[be.precision]
+        p = np.abs(want) ** 2
+        assert abs(ds.expectation_z(0b101) - oracle.expectation_z(p, 0b101)) < 10 * TOL[be.precision]
+        ds.free()
+    finally:
+        dist.destroy_process_group()
