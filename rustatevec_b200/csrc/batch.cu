@@ -66,7 +66,8 @@ enum BatchOp : uint32_t {
   OP_PHASE = 0, OP_1Q = 1, OP_D1 = 2, OP_CX = 3, OP_2Q = 4, OP_D2 = 5, OP_D1T = 6, OP_DT = 7, OP_D1P = 8, OP_DTP = 9,
   OP_DTAB = 10,  // the product of a phase's diagonal gates: one factor per register slot
   OP_1QR = 11,   // a real 1-qubit gate [[a, b], [c, d]] (RY, H, X): half the work of a general one
-  OP_1QX = 12    // [[a, i b], [i c, d]] with a..d real (RX, Y): half the work as well
+  OP_1QX = 12,   // [[a, i b], [i c, d]] with a..d real (RX, Y): half the work as well
+  OP_D1G = 13    // a diagonal on one register bit whose entries depend on bits of the group index
 };
 constexpr uint32_t kTphSlots = 32;  // per-tile phase operations per pass (tile sweeps)
 constexpr uint32_t kTphSlotR = 12;  // reals per slot (the OP_D1 coefficient block of either precision)
@@ -286,6 +287,53 @@ __device__ __forceinline__ void gd1(Regs<R, RB>& v, const R* __restrict__ c) {
   }
 }
 
+// Diagonal on register bit J whose entries depend on bits of this thread's group index gidx (local
+// qubits outside the phase's registers, constant per group): for each set bit k of mask, in
+// ascending order, c holds the four entries of one 2-qubit diagonal (index: register bit | group
+// bit k << 1, complex pairs). The thread multiplies the entries its group bits select, then applies
+// the resulting diag(f0, f1).
+template <int J, class R, int RB>
+__device__ __forceinline__ void gd1g(Regs<R, RB>& v, const R* __restrict__ c, uint32_t mask, uint32_t gidx) {
+  if constexpr (J < RB) {
+    R f0r = 1, f0i = 0, f1r = 1, f1i = 0;
+    for (uint32_t mm = mask; mm; mm &= mm - 1u, c += 8) {
+      const R* d = c + 4 * ((gidx >> (__ffs(mm) - 1)) & 1u);
+      const R a0r = d[0], a0i = d[1], a1r = d[2], a1i = d[3];
+      const R t0 = f0r * a0r - f0i * a0i, t1 = f1r * a1r - f1i * a1i;
+      f0i = f0r * a0i + f0i * a0r;
+      f1i = f1r * a1i + f1i * a1r;
+      f0r = t0;
+      f1r = t1;
+    }
+    if constexpr (std::is_same<R, float>::value) {
+#pragma unroll
+      for (int h = 0; h < (1 << RB) / 2; ++h) {
+        float2 pr, pi;
+        if constexpr (J == 0) {  // the pair (2h, 2h+1) straddles bit 0
+          pr = make_float2(f0r, f1r);
+          pi = make_float2(f0i, f1i);
+        } else {
+          const bool one = (h >> (J - 1)) & 1;
+          pr = one ? make_float2(f1r, f1r) : make_float2(f0r, f0r);
+          pi = one ? make_float2(f1i, f1i) : make_float2(f0i, f0i);
+        }
+        const float2 npi = make_float2(-pi.x, -pi.y);
+        const float2 xr = v.r[h], xi = v.i[h];
+        v.r[h] = __ffma2_rn(pr, xr, __fmul2_rn(npi, xi));
+        v.i[h] = __ffma2_rn(pr, xi, __fmul2_rn(pi, xr));
+      }
+    } else {
+#pragma unroll
+      for (int s = 0; s < (1 << RB); ++s) {
+        const R pr = (s & (1 << J)) ? f1r : f0r, pi = (s & (1 << J)) ? f1i : f0i;
+        const R xr = v.re(s), xi = v.im(s);
+        v.re(s) = fma(pr, xr, -pi * xi);
+        v.im(s) = fma(pr, xi, pi * xr);
+      }
+    }
+  }
+}
+
 template <int J, int K, class R, int RB>
 __device__ __forceinline__ void gcx(Regs<R, RB>& v) {
   if constexpr (J < RB && K < RB && J != K) {
@@ -449,9 +497,18 @@ __device__ __forceinline__ void gtab(Regs<R, RB>& v, const R* __restrict__ c) {
 // are shared; the G independent updates interleave).
 template <class R, int RB, int G>
 __device__ __forceinline__ void apply_instr(const Instr& in, Regs<R, RB>* v, const R* __restrict__ coef, uint32_t tile,
-                                            const R* tcoef) {
+                                            const R* tcoef, const uint32_t* grp) {
   const R* c = coef + 2 * size_t(in.coef);
   switch (in.op) {
+    case OP_D1G:
+      switch (in.a) {
+        case 0: for (int g = 0; g < G; ++g) gd1g<0, R, RB>(v[g], c, in.b, grp[g]); break;
+        case 1: for (int g = 0; g < G; ++g) gd1g<1, R, RB>(v[g], c, in.b, grp[g]); break;
+        case 2: for (int g = 0; g < G; ++g) gd1g<2, R, RB>(v[g], c, in.b, grp[g]); break;
+        case 3: for (int g = 0; g < G; ++g) gd1g<3, R, RB>(v[g], c, in.b, grp[g]); break;
+        case 4: for (int g = 0; g < G; ++g) gd1g<4, R, RB>(v[g], c, in.b, grp[g]); break;
+      }
+      break;
     case OP_DTAB:
       for (int g = 0; g < G; ++g) gtab<R, RB>(v[g], c);
       break;
@@ -612,7 +669,7 @@ __device__ __forceinline__ void phase_groups(const uint32_t* grp, const PhaseDev
         v[g].im(s) = xi[off];
       }
   }
-  for (uint32_t kk = kbeg; kk < kend; ++kk) apply_instr<R, RB, G>(pprog[kk], v, pcoef, tile, tcoef);
+  for (uint32_t kk = kbeg; kk < kend; ++kk) apply_instr<R, RB, G>(pprog[kk], v, pcoef, tile, tcoef, grp);
   if (r == uint32_t(RB)) {
 #pragma unroll
     for (int g = 0; g < G; ++g)
@@ -1098,6 +1155,11 @@ void emit_phases(BatchPlan& bp, const std::vector<LGate>& G, uint32_t nlocal, st
         Rm |= m;
         done[i] = 1;
         taken.push_back(i);
+      } else if (g.kind == LK_D2 && (m & blocked) == 0 && __builtin_popcount(m & Rm) == 1) {
+        // a 2-qubit diagonal with one qubit in the registers: the other is a group-index bit of
+        // this phase, so each thread applies the entries its group selects (OP_D1G)
+        done[i] = 1;
+        taken.push_back(i);
       } else if (diag) {
         dblocked |= m;
       } else {
@@ -1152,6 +1214,9 @@ void emit_phases(BatchPlan& bp, const std::vector<LGate>& G, uint32_t nlocal, st
       if (!used[i]) lanes.push_back(nonr[i]);
     D.nt = uint32_t(nonr.size());
     QSVB_REQUIRE(D.nt <= 10, "register phase with more than 2^10 groups");
+    int gbit_of[32];  // local position -> its bit in the group index (-1: a register bit)
+    for (int q = 0; q < 32; ++q) gbit_of[q] = -1;
+    for (size_t i = 0; i < lanes.size(); ++i) gbit_of[lanes[i]] = int(i);
     // group index bits -> local positions (lanes first), as swizzled offsets: the swizzle is
     // linear, so the offset of a group is the XOR of the offsets of its bits
     auto phys_of = [&](uint32_t pos) { return (1u << pos) ^ swz_col(int(pos), int(W)); };
@@ -1175,11 +1240,20 @@ void emit_phases(BatchPlan& bp, const std::vector<LGate>& G, uint32_t nlocal, st
     // stabbing, ends first).
     const uint32_t nslot = 1u << bp.rb;
     struct Op {
-      const LGate* g;  // nullptr: a split-form 1-qubit gate on register bit rbit
+      const LGate* g;  // nullptr: a split-form 1-qubit gate or group-dependent diagonal on rbit
       uint32_t rbit;
-      int form;        // split_form: 1 real, 2 imaginary off-diagonal
+      int form;        // split_form: 1 real, 2 imaginary off-diagonal; 3: OP_D1G (factors gf[gidx])
       double k[4];
+      int gidx;
     };
+    // group-dependent diagonals on a register bit: (group bit, the 4 entries indexed register bit |
+    // group bit << 1), merged per group bit, pending until the next non-diagonal op on that bit
+    struct GFac {
+      uint32_t gbit;
+      cd d[4];
+    };
+    std::vector<std::vector<GFac>> gfs;
+    std::vector<GFac> pend_g[8];
     struct Fac {
       uint32_t rb0, rb1, nb;  // register bits (nb = 1 or 2)
       cd d[4];                // diagonal entries, index bit 0 <-> rb0, bit 1 <-> rb1
@@ -1202,7 +1276,25 @@ void emit_phases(BatchPlan& bp, const std::vector<LGate>& G, uint32_t nlocal, st
       open_facs.push_back(facs.size());
       facs.push_back(f);
     };
+    auto flush_g = [&](uint32_t rbit) {
+      if (pend_g[rbit].empty()) return;
+      std::sort(pend_g[rbit].begin(), pend_g[rbit].end(), [](const GFac& x, const GFac& y) { return x.gbit < y.gbit; });
+      gfs.push_back(std::move(pend_g[rbit]));
+      pend_g[rbit].clear();
+      ops.push_back(Op{nullptr, rbit, 3, {0, 0, 0, 0}, int(gfs.size() - 1)});
+    };
+    auto add_gfac = [&](uint32_t rbit, uint32_t gbit, const cd* d) {
+      for (GFac& f : pend_g[rbit])
+        if (f.gbit == gbit) {
+          for (int e = 0; e < 4; ++e) f.d[e] *= d[e];
+          return;
+        }
+      GFac f{gbit, {d[0], d[1], d[2], d[3]}};
+      pend_g[rbit].push_back(f);
+    };
     auto add_nondiag = [&](const Op& op, uint32_t bits) {
+      for (uint32_t b = 0; b < 8; ++b)
+        if ((bits >> b) & 1u) flush_g(b);
       const size_t idx = ops.size();
       ops.push_back(op);
       for (size_t fi : open_facs) {
@@ -1221,6 +1313,15 @@ void emit_phases(BatchPlan& bp, const std::vector<LGate>& G, uint32_t nlocal, st
         add_fac(uint32_t(regbit[g.p[0]]), 0, 1, d);
         continue;
       }
+      if (g.kind == LK_D2 && (regbit[g.p[0]] < 0 || regbit[g.p[1]] < 0)) {
+        // entry index bit 0 <-> p[0], bit 1 <-> p[1]; OP_D1G wants register bit | group bit << 1
+        const bool in0 = regbit[g.p[0]] >= 0;
+        const uint32_t pout = in0 ? g.p[1] : g.p[0];
+        const cd d[4] = {a[0], a[in0 ? 5 : 10], a[in0 ? 10 : 5], a[15]};
+        QSVB_REQUIRE(gbit_of[pout] >= 0, "group-dependent diagonal outside the phase's group bits");
+        add_gfac(uint32_t(regbit[in0 ? g.p[0] : g.p[1]]), uint32_t(gbit_of[pout]), d);
+        continue;
+      }
       if (g.kind == LK_D2) {
         const cd d[4] = {a[0], a[5], a[10], a[15]};
         add_fac(uint32_t(regbit[g.p[0]]), uint32_t(regbit[g.p[1]]), 2, d);
@@ -1228,7 +1329,7 @@ void emit_phases(BatchPlan& bp, const std::vector<LGate>& G, uint32_t nlocal, st
       }
       if (g.kind == LK_1Q) {
         // entries each real or imaginary (RY, H, X; RX, Y): half the work of a general 1-qubit gate
-        Op op{nullptr, 0, 0, {0, 0, 0, 0}};
+        Op op{nullptr, 0, 0, {0, 0, 0, 0}, -1};
         op.form = split_form(a, op.k);
         if (op.form != 0) {
           op.rbit = uint32_t(regbit[g.p[0]]);
@@ -1242,8 +1343,9 @@ void emit_phases(BatchPlan& bp, const std::vector<LGate>& G, uint32_t nlocal, st
         for (uint32_t p = 0; p < nlocal; ++p)
           if (((lm >> p) & 1u) && regbit[p] >= 0) bits |= 1u << regbit[p];
       }
-      add_nondiag(Op{&g, 0, 0, {0, 0, 0, 0}}, bits);  // diagonal kinds outside tables constrain nothing
+      add_nondiag(Op{&g, 0, 0, {0, 0, 0, 0}, -1}, bits);  // diagonal kinds outside tables constrain nothing
     }
+    for (uint32_t b = 0; b < 8; ++b) flush_g(b);
     for (Fac& f : facs)
       if (f.hi == SIZE_MAX) f.hi = ops.size();
     std::vector<size_t> order(facs.size());
@@ -1275,6 +1377,15 @@ void emit_phases(BatchPlan& bp, const std::vector<LGate>& G, uint32_t nlocal, st
         for (uint32_t s2 = 0; s2 < nslot; ++s2) push_coef(bp, t[s2]);
       }
       bp.prog.push_back(Instr{OP_DTAB, 0, 0, uint32_t(base - coef_base)});
+    };
+    auto emit_group = [&](const Op& op) {
+      uint32_t mask = 0;
+      const uint32_t base = uint32_t(bp.coef.size() / 2 - coef_base);
+      for (const GFac& f : gfs[size_t(op.gidx)]) {
+        mask |= 1u << f.gbit;
+        for (int e = 0; e < 4; ++e) push_coef(bp, f.d[e]);
+      }
+      bp.prog.push_back(Instr{OP_D1G, op.rbit, mask, base});
     };
     auto emit_split = [&](const Op& op) {
       Instr in{op.form == 2 ? uint32_t(OP_1QX) : uint32_t(OP_1QR), op.rbit, 0,
@@ -1398,6 +1509,7 @@ void emit_phases(BatchPlan& bp, const std::vector<LGate>& G, uint32_t nlocal, st
       if (!tables[j].empty() && !identity(tables[j])) emit_table(tables[j]);
       if (j == ops.size()) break;
       if (ops[j].g) emit_one(*ops[j].g);
+      else if (ops[j].form == 3) emit_group(ops[j]);
       else emit_split(ops[j]);
     }
     bp.phases[phase_idx].ninstr = uint32_t(bp.prog.size() - phase_pc - 1);
