@@ -2089,9 +2089,6 @@ void tile_prepare(Sweep& s, uint32_t n, int dtype) {
     };
     if (nout == 0) {
       G.push_back(LGate{kind, {uint32_t(pos[g.q[0]]), g.m == 2 ? uint32_t(pos[g.q[1]]) : 0u}, &hg[i]});
-      double k[4];
-      const double f1q = split_form(g.a, k) != 0 ? 8.0 : 16.0;
-      flops += dim * (kind == LK_1Q ? f1q : kind == LK_2Q ? 32.0 : kind == LK_CX ? 0.0 : 6.0);
     } else {
       QSVB_REQUIRE(kind == LK_D1 || kind == LK_D2, "only diagonal gates may reach qubits outside the tile");
       LGate lg{};
@@ -2109,7 +2106,6 @@ void tile_prepare(Sweep& s, uint32_t n, int dtype) {
         lg.t[0] = tbit(qout);
       }
       G.push_back(lg);
-      flops += dim * 6.0;
     }
   }
   // merge diagonal gates into per-tile phase sums: per local qubit, every diagonal (local or
@@ -2200,6 +2196,23 @@ void tile_prepare(Sweep& s, uint32_t n, int dtype) {
     G.swap(out);
   }
   emit_phases(bp, G, P.nlocal, &tph);
+  // arithmetic per amplitude of the emitted program, in FP32/FP64 operations: general 1-qubit gates
+  // 16, split-form ones 8, 2-qubit dense 32, diagonal kinds 6 (one complex multiply), and each
+  // register phase kTilePhaseWork for its shared-memory round trip
+  constexpr double kTilePhaseWork = 8.0;
+  double work = 0;
+  for (const Instr& in : bp.prog) {
+    switch (in.op) {
+      case OP_PHASE: work += kTilePhaseWork; break;
+      case OP_1Q: work += 16.0; break;
+      case OP_1QR:
+      case OP_1QX: work += 8.0; break;
+      case OP_2Q: work += 32.0; break;
+      case OP_CX: break;
+      default: work += 6.0; break;
+    }
+  }
+  flops = dim * work;
   P.prog_len = uint32_t(bp.prog.size());
   P.nphase = uint32_t(bp.phases.size());
   P.ncoef = uint32_t(bp.coef.size() / 2);
