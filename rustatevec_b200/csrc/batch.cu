@@ -803,12 +803,12 @@ __global__ void __launch_bounds__(NT, MINB)
       }
       __syncthreads();
       if (tid == 0 && item.tile == 0) xr[0] = R(1);  // the swizzle maps 0 to 0
-    } else if (L >= 5 && !(fixed && sizeof(R) == 8)) {
+    } else if (L >= 5 && sizeof(R) != 8) {
       // 16-byte loads of contiguous amplitudes (a run of 32 shares its global offset), several in
       // flight per thread, then scattered through the swizzle (it only flips bits below W, so the
-      // VN amplitudes of a vector land at y ^ e). complex128 tile sweeps take the per-element
-      // cp.async path below instead: the whole tile in flight at once with no registers held
-      // (measured 3-4 % faster there; 1.5-4 % slower for complex64)
+      // VN amplitudes of a vector land at y ^ e). complex128 takes the per-element cp.async path
+      // below instead: the whole tile in flight at once with no registers held (measured 3-4 %
+      // faster for tile sweeps and 2 % for batches; 1.5-4 % slower for complex64)
       using VT = typename Vec16<R>::T;
       constexpr int VN = Vec16<R>::N, UNR = 4;
       for (uint32_t xb = tid * VN; xb < T; xb += NT * VN * UNR) {
