@@ -193,7 +193,7 @@ def run_gpu(args):
     from rustatevec_b200 import tuning
     world, rank, local = dist_setup()
     torch.cuda.set_device(local)
-    model_doc = tuning.load()  # the learned cost model trained on this pool's B200s (None: roofline model)
+    model_doc = tuning.load()  # the learned cost model trained on B200 measurements (None: roofline model)
     be = B200Backend(local, precision="f32")
     stream = torch.cuda.ExternalStream(be.stream(), device=torch.device("cuda", local))
     circuit = brickwork(N_QUBITS, DEPTH, SEED)
