@@ -19,7 +19,9 @@ Physical positions are not fixed per logical qubit: a map ``phys[q]`` moves as t
   lie in HBM, with no packing pass. Partners follow an XOR schedule (step s pairs ranks whose
   exchanged bits differ by s), so every step is a set of disjoint pairwise swaps and no rank waits
   on one that is busy elsewhere. A qubit of the gate that sits in that top region moves down first
-  by a local SWAP; the local qubits that leave are those whose next use lies furthest ahead.
+  by a local SWAP. The local qubits that leave are either those whose next use lies furthest ahead
+  (moved into the top positions by local SWAPs) or those already there; the planner keeps the
+  choice with less estimated data movement (``plan_cost``).
 
 The exchange goes through a communicator: ``TorchComm`` (torch.distributed; NCCL over
 NVLink/NVSwitch between GPUs, gloo on CPU) or none when one process owns every rank (the ranks are
@@ -45,10 +47,12 @@ from .gate import DenseGate
 @dataclass
 class LocalOp:
     """A gate in physical positions. ``glob`` lists (gate bit j, global bit index) of qubits that
-    stay global: each rank applies the block its own bits select."""
+    stay global: each rank applies the block its own bits select. ``moved``: a SWAP the planner
+    inserted to bring a leaving qubit into the top positions."""
     matrix: np.ndarray
     local: tuple            # (gate bit j, physical position) of the local qubits
     glob: tuple = ()
+    moved: bool = False
 
 
 @dataclass
@@ -112,13 +116,33 @@ class Layout:
         return out
 
 
-def plan_distributed(circuit: Circuit, g: int, layout: Layout | None = None, policy: str = "furthest"):
+# An exchange moving a whole slice over NVLink (about 770 GB/s per direction) costs this many local
+# sweeps (one read and one write of the slice in HBM, about 6.5 TB/s).
+EXCHANGE_SWEEPS_PER_SLICE = 6.5e12 / (2 * 770e9)
+
+
+def plan_cost(steps) -> float:
+    """Estimated data movement of a plan beyond its gates, in local sweeps: every exchange of k bits
+    moves (1 - 2^-k) of the slice, every planner-inserted SWAP is one local sweep."""
+    ex = sum(1.0 - 2.0 ** -len(s.gbits) for s in steps if isinstance(s, ExchangeStep))
+    moved = sum(1 for s in steps if isinstance(s, LocalStep) for op in s.ops if op.moved)
+    return ex * EXCHANGE_SWEEPS_PER_SLICE + moved
+
+
+def plan_distributed(circuit: Circuit, g: int, layout: Layout | None = None, policy: str = "auto"):
     """Steps (``LocalStep`` / ``ExchangeStep``) that run ``circuit`` on 2^g ranks from ``layout``
     (identity when None); returns ``(steps, final_layout)``. Every rank computes the same plan.
 
     ``policy`` picks the local qubits that leave at an exchange: "furthest" (next use furthest
-    ahead, moved into the top positions by local SWAPs) or "top" (whatever sits in the top
-    positions, no SWAPs unless a qubit of the gate is there)."""
+    ahead, moved into the top positions by local SWAPs: fewer exchanges), "top" (whatever sits in
+    the top positions, no SWAPs unless a qubit of the gate is there), or "auto" (both, keeping the
+    one with the lower ``plan_cost``)."""
+    if policy == "auto":
+        a = plan_distributed(circuit, g, layout, "furthest")
+        b = plan_distributed(circuit, g, layout, "top")
+        return a if plan_cost(a[0]) <= plan_cost(b[0]) else b
+    if policy not in ("furthest", "top"):
+        raise ValueError(f"unknown policy {policy!r}")
     n = circuit.n_qubits()
     if g < 0 or n - g < 6:
         raise ValueError("a distributed state needs at least 6 local qubits per rank")
@@ -129,7 +153,7 @@ def plan_distributed(circuit: Circuit, g: int, layout: Layout | None = None, pol
     nxt = _next_uses(circuit)
 
     def push_swap(a: int, b: int):
-        cur.ops.append(LocalOp(G.swap().matrix, ((0, a), (1, b))))
+        cur.ops.append(LocalOp(G.swap().matrix, ((0, a), (1, b)), moved=True))
         lay.swap_positions(a, b)
 
     for i, op in enumerate(circuit.ops()):
@@ -295,7 +319,8 @@ class DistributedState:
     every rank (slices on one device); otherwise it owns rank ``comm.rank`` and the group has
     ``2**global_qubits`` members. ``chunk_elems``: amplitudes per transfer (the receive buffer)."""
 
-    def __init__(self, n_qubits: int, global_qubits: int, engine, comm=None, chunk_elems: int = 1 << 25):
+    def __init__(self, n_qubits: int, global_qubits: int, engine, comm=None, chunk_elems: int = 1 << 25,
+                 policy: str = "auto"):
         self.n, self.g = int(n_qubits), int(global_qubits)
         self.nl = self.n - self.g
         if self.nl < 6:
@@ -308,6 +333,7 @@ class DistributedState:
         self.slices = {r: engine.alloc(self.nl) for r in self.owned}
         self.layout = Layout(self.n, self.g)
         self.chunk = max(1, int(chunk_elems))
+        self.policy = policy
         self.stats = {"exchanges": 0, "exchanged_bytes_per_rank": 0, "local_steps": 0}
 
     # -- preparation
@@ -323,7 +349,7 @@ class DistributedState:
     def run(self, circuit: Circuit) -> dict:
         if circuit.n_qubits() != self.n:
             raise ValueError("circuit width does not match the state")
-        steps, self.layout = plan_distributed(circuit, self.g, self.layout)
+        steps, self.layout = plan_distributed(circuit, self.g, self.layout, self.policy)
         for s in steps:
             if isinstance(s, LocalStep):
                 self.stats["local_steps"] += 1

@@ -16,7 +16,7 @@ from rustatevec_b200 import gate as G
 from rustatevec_b200.circuit import Circuit
 from rustatevec_b200.circuits import brickwork, ghz_chain, qaoa_maxcut, qft, random_circuit
 from rustatevec_b200.distributed import (DistributedState, ExchangeStep, LocalStep, Layout, TorchComm,
-                                         plan_distributed, rank_circuit)
+                                         plan_cost, plan_distributed, rank_circuit)
 
 
 class OracleSliceEngine:
@@ -141,6 +141,27 @@ def test_rank_circuits_fix_the_global_bits():
     steps, _ = plan_distributed(c, 2)
     assert [len(rank_circuit(steps[0], 7, r)) for r in range(4)] == [0, 0, 0, 1]
     assert np.allclose(rank_circuit(steps[0], 7, 3).ops()[0].gate.matrix, -np.eye(2))
+
+
+def test_auto_policy_keeps_the_cheaper_plan():
+    # brickwork uses every qubit every layer: moving victims by SWAP costs more than it saves;
+    # QAOA's mixers and cost layers reuse qubits unevenly: furthest-next-use wins
+    for c, g in ((brickwork(16, 8, 1), 1), (qaoa_maxcut(16, 3, 2), 1), (qft(14), 2), (random_circuit(14, 200, 7), 2)):
+        costs = {p: plan_cost(plan_distributed(c, g, policy=p)[0]) for p in ("furthest", "top")}
+        auto = plan_cost(plan_distributed(c, g, policy="auto")[0])
+        assert auto == min(costs.values())
+    with pytest.raises(ValueError):
+        plan_distributed(Circuit(8), 1, policy="nearest")
+
+
+@pytest.mark.parametrize("policy", ["furthest", "top"])
+def test_both_policies_match_the_whole_state(built, policy):
+    n, g = 10, 2
+    for c in circuits(n):
+        ds = DistributedState(n, g, OracleSliceEngine(), policy=policy)
+        ds.init_basis(0)
+        ds.run(c)
+        assert np.max(np.abs(ds.gather() - whole(c))) < 1e-12
 
 
 def test_rejects_too_few_local_qubits():
