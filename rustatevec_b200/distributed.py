@@ -91,6 +91,22 @@ def _next_uses(circuit: Circuit):
     return out
 
 
+def _next_mixing_uses(circuit: Circuit):
+    """next_mix[i][q]: index of the first gate after gate i whose matrix mixes q's values (or
+    infinity): the next gate that would need q local."""
+    ops = circuit.ops()
+    n = circuit.n_qubits()
+    inf = len(ops) + 1
+    nxt = [inf] * n
+    out = [None] * len(ops)
+    for i in range(len(ops) - 1, -1, -1):
+        out[i] = list(nxt)
+        for j, q in enumerate(ops[i].qubits):
+            if _mixes(ops[i].gate.matrix, j):
+                nxt[q] = i
+    return out
+
+
 class Layout:
     """Logical qubit -> physical position (positions >= n_local are global bits)."""
 
@@ -129,18 +145,23 @@ def plan_cost(steps) -> float:
     return ex * EXCHANGE_SWEEPS_PER_SLICE + moved
 
 
-def plan_distributed(circuit: Circuit, g: int, layout: Layout | None = None, policy: str = "auto"):
+MAX_EXCHANGE_BITS = 4  # global qubits one exchange brings in when it groups upcoming needs
+
+
+def plan_distributed(circuit: Circuit, g: int, layout: Layout | None = None, policy: str = "auto",
+                     group: bool = False):
     """Steps (``LocalStep`` / ``ExchangeStep``) that run ``circuit`` on 2^g ranks from ``layout``
     (identity when None); returns ``(steps, final_layout)``. Every rank computes the same plan.
 
     ``policy`` picks the local qubits that leave at an exchange: "furthest" (next use furthest
     ahead, moved into the top positions by local SWAPs: fewer exchanges), "top" (whatever sits in
-    the top positions, no SWAPs unless a qubit of the gate is there), or "auto" (both, keeping the
-    one with the lower ``plan_cost``)."""
+    the top positions, no SWAPs unless a qubit of the gate is there), or "auto" (every policy, with
+    and without grouping, keeping the plan with the lowest ``plan_cost``). ``group``: an exchange
+    also brings in the global qubits that a gate within the next n gates will need local (k bits
+    at once move 1 - 2^-k of the slice, against k/2 one at a time), up to MAX_EXCHANGE_BITS."""
     if policy == "auto":
-        a = plan_distributed(circuit, g, layout, "furthest")
-        b = plan_distributed(circuit, g, layout, "top")
-        return a if plan_cost(a[0]) <= plan_cost(b[0]) else b
+        plans = [plan_distributed(circuit, g, layout, p, grp) for p in ("furthest", "top") for grp in (False, True)]
+        return min(plans, key=lambda pl: plan_cost(pl[0]))
     if policy not in ("furthest", "top"):
         raise ValueError(f"unknown policy {policy!r}")
     n = circuit.n_qubits()
@@ -151,6 +172,7 @@ def plan_distributed(circuit: Circuit, g: int, layout: Layout | None = None, pol
     steps: list = []
     cur = LocalStep()
     nxt = _next_uses(circuit)
+    nxm = _next_mixing_uses(circuit) if group else None
 
     def push_swap(a: int, b: int):
         cur.ops.append(LocalOp(G.swap().matrix, ((0, a), (1, b)), moved=True))
@@ -160,11 +182,17 @@ def plan_distributed(circuit: Circuit, g: int, layout: Layout | None = None, pol
         qs, mat = op.qubits, op.gate.matrix
         need = [j for j, q in enumerate(qs) if lay.phys[q] >= nl and _mixes(mat, j)]
         if need:
-            k = len(need)
-            top = list(range(nl - 1, nl - 1 - k, -1))
             gate_q = set(qs)
-            # local qubits that may leave: not in this gate; furthest next use first
+            # local qubits that may leave: not in this gate
             cand = [q for q in range(n) if lay.phys[q] < nl and q not in gate_q]
+            bring = [qs[j] for j in need]
+            if group:  # global qubits soon needed local come in with this exchange
+                room = min(MAX_EXCHANGE_BITS, len(cand)) - len(bring)
+                soon = [q for q in range(n) if lay.phys[q] >= nl and q not in gate_q and nxm[i][q] <= i + n]
+                soon.sort(key=lambda q: nxm[i][q])
+                bring += soon[:max(0, room)]
+            k = len(bring)
+            top = list(range(nl - 1, nl - 1 - k, -1))
             if policy == "top":
                 cand.sort(key=lambda q: (-lay.phys[q], -nxt[i][q]))
             else:
@@ -179,7 +207,7 @@ def plan_distributed(circuit: Circuit, g: int, layout: Layout | None = None, pol
             if cur.ops:
                 steps.append(cur)
                 cur = LocalStep()
-            gbits = tuple(lay.phys[qs[j]] - nl for j in need)
+            gbits = tuple(lay.phys[q] - nl for q in bring)
             tpos = tuple(lay.phys[q] for q in leave)
             steps.append(ExchangeStep(gbits, tpos))
             for gb, t in zip(gbits, tpos):
@@ -317,7 +345,9 @@ class TorchComm:
 class DistributedState:
     """A state of ``n_qubits`` over ``2**global_qubits`` ranks. ``comm`` None: this process owns
     every rank (slices on one device); otherwise it owns rank ``comm.rank`` and the group has
-    ``2**global_qubits`` members. ``chunk_elems``: amplitudes per transfer (the receive buffer)."""
+    ``2**global_qubits`` members. ``chunk_elems``: amplitudes per transfer (the receive buffer).
+    ``policy``: the exchange planner's policy (see ``plan_distributed``; "furthest+group" or
+    "top+group" for a fixed policy with grouped exchanges)."""
 
     def __init__(self, n_qubits: int, global_qubits: int, engine, comm=None, chunk_elems: int = 1 << 25,
                  policy: str = "auto"):
@@ -349,7 +379,10 @@ class DistributedState:
     def run(self, circuit: Circuit) -> dict:
         if circuit.n_qubits() != self.n:
             raise ValueError("circuit width does not match the state")
-        steps, self.layout = plan_distributed(circuit, self.g, self.layout, self.policy)
+        policy, grp = self.policy, False
+        if policy.endswith("+group"):  # e.g. "top+group": that policy with grouped exchanges
+            policy, grp = policy[: -len("+group")], True
+        steps, self.layout = plan_distributed(circuit, self.g, self.layout, policy, grp)
         for s in steps:
             if isinstance(s, LocalStep):
                 self.stats["local_steps"] += 1

@@ -147,16 +147,17 @@ def test_auto_policy_keeps_the_cheaper_plan():
     # brickwork uses every qubit every layer: moving victims by SWAP costs more than it saves;
     # QAOA's mixers and cost layers reuse qubits unevenly: furthest-next-use wins
     for c, g in ((brickwork(16, 8, 1), 1), (qaoa_maxcut(16, 3, 2), 1), (qft(14), 2), (random_circuit(14, 200, 7), 2)):
-        costs = {p: plan_cost(plan_distributed(c, g, policy=p)[0]) for p in ("furthest", "top")}
+        costs = [plan_cost(plan_distributed(c, g, policy=p, group=grp)[0])
+                 for p in ("furthest", "top") for grp in (False, True)]
         auto = plan_cost(plan_distributed(c, g, policy="auto")[0])
-        assert auto == min(costs.values())
+        assert auto == min(costs)
     with pytest.raises(ValueError):
         plan_distributed(Circuit(8), 1, policy="nearest")
 
 
-@pytest.mark.parametrize("policy", ["furthest", "top"])
-def test_both_policies_match_the_whole_state(built, policy):
-    n, g = 10, 2
+@pytest.mark.parametrize("policy", ["furthest", "top", "furthest+group", "top+group"])
+def test_every_policy_matches_the_whole_state(built, policy):
+    n, g = 10, 3
     for c in circuits(n):
         ds = DistributedState(n, g, OracleSliceEngine(), policy=policy)
         ds.init_basis(0)
