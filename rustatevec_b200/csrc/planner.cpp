@@ -22,6 +22,7 @@
 #include <cstring>
 #include <future>
 #include <numeric>
+#include <thread>
 
 #include "cost_model.h"
 #include "qsvb_internal.h"
@@ -172,12 +173,8 @@ Gate compose_diag(const std::vector<uint32_t>& q, const std::vector<const Gate*>
 // three or more qubits that holds a non-diagonal gate becomes a placeholder with no matrix (it
 // classifies as a dense sweep, whose cost does not depend on the entries); groups whose kind the
 // entries decide (diagonal, or at most two qubits) are still composed.
-void emit_group(std::vector<Gate>& out, const std::vector<const Gate*>& grp, bool cost_only) {
-  if (grp.empty()) return;
-  if (grp.size() == 1) {
-    out.push_back(*grp[0]);
-    return;
-  }
+Gate make_group(const std::vector<const Gate*>& grp, bool cost_only) {
+  if (grp.size() == 1) return *grp[0];
   uint64_t mask = 0;
   bool all_diag = true;
   for (const Gate* g : grp) {
@@ -187,30 +184,50 @@ void emit_group(std::vector<Gate>& out, const std::vector<const Gate*>& grp, boo
   std::vector<uint32_t> q;
   for (uint32_t b = 0; b < 64; ++b)
     if ((mask >> b) & 1) q.push_back(b);
-  if (cost_only && all_diag) {
-    out.push_back(compose_diag(q, grp));
-  } else if (cost_only && q.size() > 2) {
+  if (cost_only && all_diag) return compose_diag(q, grp);
+  if (cost_only && q.size() > 2) {
     Gate ph;
     ph.m = uint32_t(q.size());
     for (size_t j = 0; j < q.size(); ++j) ph.q[j] = q[j];
-    out.push_back(std::move(ph));
-  } else {
-    out.push_back(compose(q, grp));
+    return ph;
   }
+  return compose(q, grp);
+}
+
+// The fused gates of a grouping, in order. Full compositions of many groups run on host threads
+// (each group is independent; the result does not depend on the split).
+std::vector<Gate> emit_groups(const std::vector<std::vector<const Gate*>>& groups, bool cost_only) {
+  std::vector<Gate> out(groups.size());
+  auto range = [&](size_t lo, size_t hi) {
+    for (size_t i = lo; i < hi; ++i) out[i] = make_group(groups[i], cost_only);
+  };
+  const size_t nth = std::min<size_t>(std::max(1u, std::thread::hardware_concurrency()), 16);
+  if (cost_only || groups.size() < 32 || nth == 1) {
+    range(0, groups.size());
+    return out;
+  }
+  std::vector<std::future<void>> fut;
+  for (size_t t = 0; t < nth; ++t)
+    fut.push_back(std::async(std::launch::async, range, groups.size() * t / nth, groups.size() * (t + 1) / nth));
+  for (auto& f : fut) f.get();
+  return out;
 }
 
 // fusion.rs:39-77 — consecutive-only greedy.
 std::vector<Gate> fuse_greedy(const std::vector<Gate>& in, uint32_t maxq, bool cost_only = false) {
   maxq = std::max<uint32_t>(maxq, 1);
-  std::vector<Gate> out;
+  std::vector<std::vector<const Gate*>> groups;
   std::vector<const Gate*> grp;
   std::vector<uint32_t> gq;  // insertion order, as the reference keeps it
+  auto close = [&] {
+    if (!grp.empty()) groups.push_back(grp);
+    grp.clear();
+  };
   for (const Gate& g : in) {
     if (g.m > maxq) {
-      emit_group(out, grp, cost_only);
-      grp.clear();
+      close();
       gq.clear();
-      out.push_back(g);
+      groups.push_back({&g});
       continue;
     }
     std::vector<uint32_t> uni = gq;
@@ -223,14 +240,13 @@ std::vector<Gate> fuse_greedy(const std::vector<Gate>& in, uint32_t maxq, bool c
       gq = uni;
       grp.push_back(&g);
     } else {
-      emit_group(out, grp, cost_only);
-      grp.clear();
+      close();
       gq.assign(g.q, g.q + g.m);
       grp.push_back(&g);
     }
   }
-  emit_group(out, grp, cost_only);
-  return out;
+  close();
+  return emit_groups(groups, cost_only);
 }
 
 // Commutation-aware window fusion: a later gate may join the open group when its qubits are
@@ -239,7 +255,7 @@ std::vector<Gate> fuse_window(const std::vector<Gate>& in, uint32_t maxq, bool c
                               size_t lookahead = 1024) {
   maxq = std::max<uint32_t>(maxq, 1);
   std::vector<char> done(in.size(), 0);
-  std::vector<Gate> out;
+  std::vector<std::vector<const Gate*>> groups;
   size_t first = 0;
   std::vector<const Gate*> grp;
   while (true) {
@@ -248,7 +264,7 @@ std::vector<Gate> fuse_window(const std::vector<Gate>& in, uint32_t maxq, bool c
     done[first] = 1;
     const Gate& g0 = in[first];
     if (g0.m > maxq) {
-      out.push_back(g0);
+      groups.push_back({&g0});
       continue;
     }
     grp.assign(1, &g0);
@@ -268,9 +284,9 @@ std::vector<Gate> fuse_window(const std::vector<Gate>& in, uint32_t maxq, bool c
         if (uint32_t(__builtin_popcountll(gmask)) == maxq && (gmask & ~blocked) == 0) break;
       }
     }
-    emit_group(out, grp, cost_only);
+    groups.push_back(grp);
   }
-  return out;
+  return emit_groups(groups, cost_only);
 }
 
 bool phase_representable(const Gate& g) {
