@@ -218,3 +218,26 @@ def test_gloo_ranks_match_the_whole_state(built, g):
             assert out[r][i][2] == ex
             if r:
                 assert out[r][i][0] is None
+
+
+def test_random_circuits_every_policy_property(built):
+    """Property check over seeded random cases: any width, global-bit count, policy and grouping
+    gives the oracle's whole-state result."""
+    from hypothesis import given, settings, strategies as st
+
+    @settings(max_examples=40, deadline=None, derandomize=True)
+    @given(n=st.integers(8, 11), g=st.integers(1, 3), depth=st.integers(5, 60), seed=st.integers(0, 10 ** 6),
+           policy=st.sampled_from(["auto", "furthest", "top", "furthest+group", "top+group"]))
+    def check(n, g, depth, seed, policy):
+        if n - g < 6:
+            return
+        c = random_circuit(n, depth, seed)
+        ds = DistributedState(n, g, OracleSliceEngine(), policy=policy, chunk_elems=1 + seed % 300)
+        ds.init_basis(seed % (1 << n))
+        ds.run(c)
+        psi0 = np.zeros(1 << n)
+        psi0[seed % (1 << n)] = 1.0
+        re, im = oracle.run(c, oracle.REF, oracle.F64, state=(psi0, np.zeros(1 << n)))
+        assert np.max(np.abs(ds.gather() - (re + 1j * im))) < 1e-12
+
+    check()
