@@ -701,6 +701,9 @@ KERNEL_CASES = {
     "1q_high": ("f32", lambda n: [("h", [n - 1])]),
     "cx_high": ("f32", lambda n: [("cx", [n - 1, n - 2])]),
     "cz_high": ("f32", lambda n: [("cz", [n - 1, n - 2])]),
+    # FP64 reductions (no circuit): <Z_mask> over the whole state, one read of it per call
+    "reduce_z": ("f32", lambda n: []),
+    "reduce_z_c128": ("f64", lambda n: []),
     "dense4_cuda": ("f32", lambda n: [("u4", [0, 1, 2, 3])]),
     "dense6_cuda": ("f32", lambda n: [("u6", list(range(6)))]),
     "tc4": ("f32", lambda n: [("u4", [0, 1, 2, 3])]),
@@ -746,6 +749,29 @@ def run_kernel_case(args):
         planner = L.PLAN_TILE
     be = B200Backend(0, precision=prec)
     st = be.alloc(n)
+    if args.kernel_case.startswith("reduce"):
+        be.init_gaussian(st, 7)
+        stream = torch.cuda.ExternalStream(be.stream())
+        mask = (1 << n) - 1
+        for _ in range(2):
+            be.expectation_z(st, mask)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.reps):
+            be.expectation_z(st, mask)
+        e1.record(stream)
+        e1.synchronize()
+        t = e0.elapsed_time(e1) * 1e-3 / args.reps
+        nbytes = float(1 << n) * (16 if prec == "f64" else 8)  # one read of the state
+        peak, kind = peaks()
+        print(json.dumps({"kernel_case": args.kernel_case, "qubits": n, "precision": prec, "input": "gaussian",
+                          "sweeps": ["reduce"], "us_per_call": round(t * 1e6, 2), "algorithmic_bytes": nbytes,
+                          "GB/s": round(nbytes / t / 1e9, 1), "frac_of_peak": round(nbytes / t / 1e9 / peak, 4),
+                          "peak": f"{peak} ({kind})",
+                          "note": "per call: the reduction kernels plus the 16-byte result copy and a synchronize"}))
+        st.free()
+        be.close()
+        return
     # a dense random state by default: a basis state leaves almost every streamed amplitude zero,
     # which draws less power and times optimistically
     if args.input == "basis":
