@@ -94,7 +94,9 @@ typedef struct qsvb_plan_stats {
   double algorithmic_bytes;   /* sum over sweeps of 2 * (amplitudes the sweep may change) * bytes/amp */
   double full_sweep_bytes;    /* sum over sweeps of 2 * 2^n * bytes/amp */
   double flops;               /* complex-MAC flops of the dense sweeps (8 * 2^k per amplitude) */
-  double predicted_seconds;   /* planner's cost-model estimate */
+  double predicted_seconds;   /* planner's cost-model estimate (0 where nothing is predicted) */
+  double measured_seconds;    /* device seconds measured by the call itself (qsvb_execute_batch*,
+                                 qsvb_batch_run); 0 where the call measures nothing */
 } qsvb_plan_stats;
 
 /* ---------------------------------------------------------------- lifecycle */
@@ -181,10 +183,14 @@ int qsvb_amplitude(qsvb_ctx* ctx, const qsvb_state* st, uint64_t index, double o
 int qsvb_probabilities(qsvb_ctx* ctx, const qsvb_state* st, void* out, int out_dtype);
 /* Backend::expectation_z (mod.rs:57-59; sample.rs:177-200), FP64 on device. */
 int qsvb_expectation_z(qsvb_ctx* ctx, const qsvb_state* st, uint64_t mask, double* out);
-/* `shots` measurement outcomes drawn on the device (no probability download): shot k returns the
- * outcome whose FP64 cumulative-probability interval holds u_k * total, u_k the k-th unit() value
- * of SplitMix64(seed) (crates/qsv-core/src/circuits.rs:22-46). Same distribution as the trait's
- * sample (crates/qsv-core/src/sample.rs:84-97, alias method), not the same draws. shots <= 2^30. */
+/* Backend::sample overridden on the device (mod.rs:52-54: "a device backend overrides this"),
+ * drawing as cdf_sample does (crates/qsv-core/src/sample.rs:163-172): shot k returns the first
+ * outcome i whose FP64 cumulative probability is >= u_k * total, u_k the k-th unit() value of
+ * SplitMix64(seed) (crates/qsv-core/src/circuits.rs:22-46), i.e. seed = the caller's rng state
+ * before the call, which then advances by `shots` draws. Probabilities are |amp|^2 rounded in the
+ * state's precision, as Backend::probabilities computes them; the FP64 prefix sums run in another
+ * order than the reference's, so a draw can differ only where u_k * total lies within rounding of
+ * a cumulative value. No probability download. shots <= 2^30. */
 int qsvb_sample(qsvb_ctx* ctx, const qsvb_state* st, uint64_t shots, uint64_t seed, uint64_t* out);
 /* StateVector::norm_sqr (crates/qsv-core/src/state/mod.rs:112-118), FP64 on device. */
 int qsvb_norm_sqr(qsvb_ctx* ctx, const qsvb_state* st, double* out);
@@ -196,9 +202,12 @@ int qsvb_inner_product(qsvb_ctx* ctx, const qsvb_state* a, const qsvb_state* b, 
  * (NULL = default stream) and a host `out`, needs no context, and calls no cudaMalloc / cudaFree.
  * Its reduction scratch is a fixed 16.4 KB __device__ array inside the library (held on every GPU
  * that loads it until exit; partial sums of at most 1024 CTAs; n_qubits up to 34, larger or
- * malformed requests return QSVB_E_INVALID). All calls share that array, so calls whose kernels
- * overlap on the GPU race; the first call on a device sets the array up and must come before any
- * stream capture. No counterpart in the reference: it exists for hosts that run under a fixed
+ * malformed requests return QSVB_E_INVALID). d_re and d_im must be device or managed memory of
+ * the current device and 16-byte aligned; host pointers, another device's memory and misaligned
+ * offsets return QSVB_E_INVALID before any launch. All calls share that array, so calls whose
+ * kernels overlap on the GPU race; the first call on a device (and the first after a
+ * cudaDeviceReset, which invalidates the array's address) sets the array up and must come before
+ * any stream capture. No counterpart in the reference: it exists for hosts that run under a fixed
  * device-memory budget or own every device allocation themselves. Waits for its result. */
 int qsvb_expectation_z_noalloc(const void* d_re, const void* d_im, uint32_t n_qubits, int dtype, uint64_t mask,
                                void* stream, double* out);
@@ -236,7 +245,7 @@ int qsvb_costmodel_predict(const float* features, size_t n, float* out_log2_seco
  * or packed in circuit order when probs_offset == NULL. Each circuit starts from |0..0>.
  * stats (optional): n_sweeps = passes over shared-memory tiles, n_sweeps_by_kind[0] = register
  * phases, algorithmic_bytes = HBM bytes of those passes plus the probabilities, flops = gate
- * arithmetic, predicted_seconds = measured device seconds of the batched kernels. Replaces a host
+ * arithmetic, measured_seconds = measured device seconds of the batched kernels. Replaces a host
  * loop of Backend::execute over the circuits (crates/qsv-core/src/backend/mod.rs:66-73) followed
  * by expectation_z (crates/qsv-core/src/sample.rs:177-200). */
 int qsvb_execute_batch(qsvb_ctx* ctx, const qsvb_circuit* circuits, size_t n_circuits, int dtype,
@@ -251,6 +260,12 @@ int qsvb_batch_create(qsvb_ctx* ctx, const qsvb_circuit* circuits, size_t n_circ
                       uint32_t local_qubits, uint32_t register_qubits, qsvb_batch** out);
 int qsvb_batch_run(qsvb_ctx* ctx, qsvb_batch* batch, double* z0_out, double* probs_out,
                    const uint64_t* probs_offset, qsvb_plan_stats* stats);
+/* Failure detection of the batched runner (no trait counterpart): a tile of pass p waits for
+ * every tile of pass p-1 of its circuit; each such wait may take at most `cycles` clock64 cycles
+ * (0 restores the default, 2^32, about 2 s; at most 2^40). A wait that runs out fails the run:
+ * every block abandons its remaining work, and qsvb_batch_run returns QSVB_E_TIMEOUT with the
+ * context still usable. */
+int qsvb_batch_set_wait_budget(qsvb_ctx* ctx, qsvb_batch* batch, uint64_t cycles);
 int qsvb_batch_free(qsvb_ctx* ctx, qsvb_batch* batch);
 /* Times each tile shape (local qubits from two below the limit up to it, both register widths)
  * on this batch; writes the fastest to *best_local / *best_register and, when seconds != NULL,

@@ -155,3 +155,30 @@ def expectation_z(probs, mask: int) -> float:
 
 def set_threads(n: int):
     lib().orc_set_threads(n)
+
+
+_G = np.uint64(0x9E3779B97F4A7C15)
+
+
+def splitmix_units(state: int, count: int) -> np.ndarray:
+    """The next ``count`` ``unit()`` values of ``SplitMix64`` whose state is ``state``
+    (crates/qsv-core/src/circuits.rs:22-46), vectorised: draw k mixes ``state + (k + 1) * G``."""
+    k = np.arange(1, count + 1, dtype=np.uint64)
+    with np.errstate(over="ignore"):
+        z = np.uint64(state) + k * _G
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        z = z ^ (z >> np.uint64(31))
+    return (z >> np.uint64(11)).astype(np.float64) * 2.0 ** -53
+
+
+def cdf_sample(weights, shots: int, state: int):
+    """``cdf_sample`` (crates/qsv-core/src/sample.rs:163-172): the FP64 inclusive prefix sum of the
+    weights, ``u = unit() * total`` per shot, and the first index whose cumulative value is
+    ``>= u`` (``partition_point(|&c| c < u)``), clamped to the last index. The prefix sum is
+    sequential (the reference's chunked parallel scan differs from it only by rounding). Returns
+    ``(outcomes, u, cdf)``."""
+    cdf = np.cumsum(np.asarray(weights, dtype=np.float64))
+    u = splitmix_units(state, shots) * cdf[-1]
+    idx = np.minimum(np.searchsorted(cdf, u, side="left"), len(cdf) - 1)
+    return idx, u, cdf

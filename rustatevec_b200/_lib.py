@@ -53,7 +53,7 @@ class PlanStats(C.Structure):
     _fields_ = [("n_gates_in", C.c_uint64), ("n_sweeps", C.c_uint64),
                 ("n_sweeps_by_kind", C.c_uint64 * 8), ("algorithmic_bytes", C.c_double),
                 ("full_sweep_bytes", C.c_double), ("flops", C.c_double),
-                ("predicted_seconds", C.c_double)]
+                ("predicted_seconds", C.c_double), ("measured_seconds", C.c_double)]
 
     def to_dict(self) -> dict:
         return {
@@ -62,6 +62,7 @@ class PlanStats(C.Structure):
             "algorithmic_bytes": float(self.algorithmic_bytes),
             "full_sweep_bytes": float(self.full_sweep_bytes), "flops": float(self.flops),
             "predicted_seconds": float(self.predicted_seconds),
+            "measured_seconds": float(self.measured_seconds),
         }
 
 
@@ -128,6 +129,7 @@ SIGNATURES = {
     "qsvb_batch_create": (_i, [_vp, C.POINTER(CircuitS), _sz, _i, _u32, _u32, C.POINTER(_vp)]),
     "qsvb_batch_run": (_i, [_vp, _vp, _dp, _dp, C.POINTER(_u64), C.POINTER(PlanStats)]),
     "qsvb_batch_free": (_i, [_vp, _vp]),
+    "qsvb_batch_set_wait_budget": (_i, [_vp, _vp, _u64]),
     "qsvb_batch_autotune": (_i, [_vp, C.POINTER(CircuitS), _sz, _i, C.POINTER(_u32), C.POINTER(_u32), _dp, _sz,
                                  C.POINTER(_sz)]),
     "qsvb_execute_batch_ex": (_i, [_vp, C.POINTER(CircuitS), _sz, _i, _u32, _u32, _dp, _dp, C.POINTER(_u64),

@@ -138,13 +138,25 @@ class B200Backend:
         return out
 
     def sample(self, state: DeviceState, shots: int, rng) -> list:
-        """Trait default (mod.rs:52-54): alias sampling over the downloaded probabilities."""
+        """``Backend::sample`` (mod.rs:52-54) overridden on the device, as the trait's doc asks of a
+        device backend: inverse-CDF draws (cdf_sample, sample.rs:163-172) from ``rng``'s stream,
+        one ``unit()`` per shot, with no probability download; ``rng`` advances by ``shots`` draws.
+        """
+        out = self.sample_device(state, shots, rng.state)
+        rng.state = (rng.state + shots * 0x9E3779B97F4A7C15) & 0xFFFFFFFFFFFFFFFF
+        return [int(x) for x in out]
+
+    def sample_alias(self, state: DeviceState, shots: int, rng) -> list:
+        """The trait's default body (mod.rs:52-54): Vose alias sampling (sample.rs:84-97) over the
+        downloaded FP64 probabilities, two ``unit()`` per shot. Same distribution as ``sample``,
+        other draws; it downloads 2^n probabilities, so it suits small states only."""
         from .sample import alias_sample
         return alias_sample(self.probabilities(state, fp64=True), shots, rng)
 
     def sample_device(self, state: DeviceState, shots: int, seed: int) -> np.ndarray:
         """``shots`` outcomes drawn on the device by inverse-CDF sampling (qsvb_sample): shot k uses
-        the k-th ``unit()`` of ``SplitMix64(seed)``; no probability download."""
+        the k-th ``unit()`` of ``SplitMix64(seed)`` and takes the first outcome whose cumulative
+        probability reaches ``unit() * total``; no probability download."""
         out = np.empty(shots, dtype=np.uint64)
         L.check(L.lib().qsvb_sample(self.ctx, state.handle, shots, seed,
                                     out.ctypes.data_as(C.POINTER(C.c_uint64))))
@@ -206,7 +218,7 @@ class B200Backend:
 
         Returns ``(z0, probs, stats)``: ``z0`` f64[count]; ``probs`` one FP64 array of 2^n_i per
         circuit (views into one packed buffer) or None; ``stats`` the batch statistics with
-        ``predicted_seconds`` = measured device seconds."""
+        ``measured_seconds`` = measured device seconds."""
         pb = circuits if isinstance(circuits, L.PackedBatch) else L.PackedBatch(circuits)
         z0 = np.zeros(pb.count, dtype=np.float64)
         probs = None

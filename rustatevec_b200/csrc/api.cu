@@ -749,6 +749,14 @@ int qsvb_batch_run(qsvb_ctx* c, qsvb_batch* b, double* z0_out, double* probs_out
   });
 }
 
+int qsvb_batch_set_wait_budget(qsvb_ctx* c, qsvb_batch* b, uint64_t cycles) {
+  return guarded([&] {
+    check_ctx(c);
+    DeviceGuard dg(c->device);
+    qsvb::batch_set_wait_budget(c, b, cycles);
+  });
+}
+
 int qsvb_batch_free(qsvb_ctx* c, qsvb_batch* b) {
   return guarded([&] {
     check_ctx(c);

@@ -53,7 +53,7 @@ namespace {
 
 constexpr int kMaxLocal = 14;
 constexpr int kMaxHi = 512;                   // 2^(kMaxLocal - 5): entries of the address / swizzle tables
-constexpr long long kSpinBudget = 1ll << 32;  // clock64 cycles (about 2 s)
+constexpr long long kSpinBudget = 1ll << 32;  // default dependency-wait budget, clock64 cycles (about 2 s)
 constexpr uint32_t kStageBytes = 32768;       // shared memory for one pass's program
 constexpr uint32_t kTileStageBytes = 16384;   // the same for tile sweeps (four blocks per SM)
 
@@ -704,7 +704,7 @@ __global__ void __launch_bounds__(NT, MINB)
             const PhaseDev* __restrict__ phases, const Instr* __restrict__ prog, const R* __restrict__ coef,
             R* __restrict__ sre, R* __restrict__ sim, double* __restrict__ probs, double* __restrict__ zpart,
             uint32_t* __restrict__ done, uint32_t* __restrict__ queue, int* __restrict__ err, uint32_t lbits,
-            long long* __restrict__ prof, uint32_t fixed) {
+            long long* __restrict__ prof, uint32_t fixed, const long long* __restrict__ wait_budget) {
   extern __shared__ __align__(16) uint8_t smem_raw[];
   R* xr = reinterpret_cast<R*>(smem_raw);
   R* xi = xr + (size_t(1) << lbits);  // every pass has nlocal <= lbits
@@ -717,6 +717,9 @@ __global__ void __launch_bounds__(NT, MINB)
   __shared__ double s_red[NT / 32];
   __shared__ int s_ok;
   const int tid = threadIdx.x;
+  // clock64 cycles one dependency wait may take before the run is failed (device memory, so that a
+  // captured graph picks up a changed value; nullptr: the default)
+  const long long budget = wait_budget != nullptr ? *wait_budget : kSpinBudget;
   // swizzle table over the index bits above W
   for (uint32_t h = tid; h < (1u << (lbits - W)); h += NT) {
     uint32_t v = 0;
@@ -744,7 +747,7 @@ __global__ void __launch_bounds__(NT, MINB)
         if (d.load(cuda::memory_order_acquire) < need) {
           const long long t0 = clock64();
           while (d.load(cuda::memory_order_acquire) < need) {
-            if (clock64() - t0 > kSpinBudget) {
+            if (clock64() - t0 > budget) {
               ok = 0;
               atomicExch(err, 1);
               break;
@@ -1766,6 +1769,7 @@ struct qsvb_batch {
   uint32_t* d_done = nullptr;
   uint32_t* d_queue = nullptr;
   long long* d_prof = nullptr;  // per-block cycle counters (QSVB_BATCH_PROFILE)
+  long long* d_wait = nullptr;  // dependency-wait budget in clock64 cycles (qsvb_batch_set_wait_budget)
   cudaGraphExec_t graph = nullptr;
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   int grid = 0;
@@ -1775,7 +1779,7 @@ struct qsvb_batch {
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
     void* ptrs[] = {d_items, d_passes, d_phases, d_prog, d_coef, d_sre, d_sim, d_zcnt, d_zoff,
-                    d_probs, d_zpart, d_z0, d_done, d_queue, d_prof};
+                    d_probs, d_zpart, d_z0, d_done, d_queue, d_prof, d_wait};
     for (void* p : ptrs)
       if (p) cudaFree(p);
   }
@@ -1806,7 +1810,7 @@ template <class R, int RB, int W, int NT> void launch(qsvb_batch* b, qsvb_ctx* c
       static_cast<const Item*>(b->d_items), uint32_t(bp.items.size()), static_cast<const PassDev*>(b->d_passes),
       static_cast<const PhaseDev*>(b->d_phases), static_cast<const Instr*>(b->d_prog),
       static_cast<const R*>(b->d_coef), static_cast<R*>(b->d_sre), static_cast<R*>(b->d_sim), b->d_probs,
-      b->d_zpart, b->d_done, b->d_queue, c->d_err, bp.local_bits, b->d_prof, 0u);
+      b->d_zpart, b->d_done, b->d_queue, c->d_err, bp.local_bits, b->d_prof, 0u, b->d_wait);
 }
 
 // The kernel variants: register bits (a group of 2^RB amplitudes per thread) and block size. The
@@ -1882,6 +1886,11 @@ qsvb_batch* batch_create(qsvb_ctx* c, const qsvb_circuit* circuits, size_t n, in
   QSVB_CK(cudaMalloc(reinterpret_cast<void**>(&b->d_z0), size_t(bp.ncirc) * 8));
   QSVB_CK(cudaMalloc(reinterpret_cast<void**>(&b->d_done), bp.passes.size() * 4));
   QSVB_CK(cudaMalloc(reinterpret_cast<void**>(&b->d_queue), 4));
+  QSVB_CK(cudaMalloc(reinterpret_cast<void**>(&b->d_wait), sizeof(long long)));
+  {
+    const long long budget = kSpinBudget;
+    QSVB_CK(cudaMemcpyAsync(b->d_wait, &budget, sizeof(budget), cudaMemcpyHostToDevice, s));
+  }
   QSVB_CK(cudaStreamSynchronize(s));
   b->smem = ((size_t(2) * rb) << bp.local_bits) + kStageBytes;
   configure_any(b.get(), c, dtype, regb);
@@ -1915,6 +1924,15 @@ qsvb_batch* batch_create(qsvb_ctx* c, const qsvb_circuit* circuits, size_t n, in
   cudaGraphDestroy(g);
   QSVB_CK(inst);
   return b.release();
+}
+
+void batch_set_wait_budget(qsvb_ctx* c, qsvb_batch* b, uint64_t cycles) {
+  QSVB_REQUIRE(b != nullptr && b->plan, "null batch");
+  QSVB_REQUIRE(b->device == c->device, "batch belongs to another device");
+  QSVB_REQUIRE(cycles <= (uint64_t(1) << 40), "wait budget must be at most 2^40 cycles");
+  const long long v = cycles == 0 ? kSpinBudget : static_cast<long long>(cycles);
+  QSVB_CK(cudaMemcpyAsync(b->d_wait, &v, sizeof(v), cudaMemcpyHostToDevice, c->stream));
+  QSVB_CK(cudaStreamSynchronize(c->stream));
 }
 
 void batch_run(qsvb_ctx* c, qsvb_batch* b, double* z0_out, double* probs_out, const uint64_t* probs_offset,
@@ -1959,7 +1977,8 @@ void batch_run(qsvb_ctx* c, qsvb_batch* b, double* z0_out, double* probs_out, co
     float ms = 0;
     QSVB_CK(cudaEventElapsedTime(&ms, b->e0, b->e1));
     *stats = bp.stats;
-    stats->predicted_seconds = double(ms) * 1e-3;  // measured device seconds of the batched graph
+    stats->predicted_seconds = 0.0;  // the batched runner predicts nothing
+    stats->measured_seconds = double(ms) * 1e-3;  // device seconds of the batched graph
   }
 }
 
@@ -1978,9 +1997,9 @@ void batch_autotune(qsvb_ctx* c, const qsvb_circuit* circuits, size_t n, int dty
       qsvb_plan_stats st{};
       batch_run(c, b.get(), nullptr, nullptr, nullptr, &st);
       batch_run(c, b.get(), nullptr, nullptr, nullptr, &st);
-      if (seconds && idx < cap) seconds[idx] = st.predicted_seconds;
-      if (st.predicted_seconds < best_t) {
-        best_t = st.predicted_seconds;
+      if (seconds && idx < cap) seconds[idx] = st.measured_seconds;
+      if (st.measured_seconds < best_t) {
+        best_t = st.measured_seconds;
         *best_local = L;
         *best_reg = rb;
       }
@@ -2035,7 +2054,7 @@ void launch_tile_variant(const LaunchEnv& e, R* re, R* im, const Sweep& s, const
                                    reinterpret_cast<const PhaseDev*>(base + s.tile_off_phase),
                                    reinterpret_cast<const Instr*>(base + s.tile_off_prog),
                                    reinterpret_cast<const R*>(base + s.tile_off_coef), re, im, nullptr, nullptr,
-                                   nullptr, nullptr, e.err_flag, s.tile_lbits, nullptr, 1u);
+                                   nullptr, nullptr, e.err_flag, s.tile_lbits, nullptr, 1u, nullptr);
   QSVB_CK(cudaGetLastError());
 }
 }  // namespace

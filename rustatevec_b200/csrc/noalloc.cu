@@ -16,10 +16,18 @@
 //     streams, no ordering between them) race and may return wrong values;
 //   - the first call on a device looks the array's device address up with cudaGetSymbolAddress
 //     (the host-side symbol is only a stand-in for it); make that first call before any stream
-//     capture begins.
+//     capture begins. The address is kept per device together with the id of the CUDA context it
+//     belongs to, so after a cudaDeviceReset the next call (in the new context) looks it up again;
+//   - d_re and d_im must be device (or managed) memory of the current device, each 16-byte
+//     aligned (the reduction reads them with 16-byte vector loads). Host pointers, memory of
+//     another device and misaligned sub-buffer offsets are refused with QSVB_E_INVALID before any
+//     kernel is launched.
 // It calls no cudaMalloc, cudaFree or allocating library routine.
 
+#include <cuda.h>
 #include <cuda_runtime.h>
+
+#include <cstdint>
 
 #include <mutex>
 #include <string>
@@ -37,17 +45,57 @@ static __device__ __align__(256) double g_noalloc_scratch[kNoAllocScratchDoubles
 constexpr int kMaxDevices = 64;
 std::mutex g_mu;
 double* g_scratch_addr[kMaxDevices] = {};
+unsigned long long g_scratch_ctx[kMaxDevices] = {};  // id of the context the address belongs to
 
-// Device address of the scratch array on the current device (set up once per device).
+// Driver entry points through the runtime (the library does not link the driver library itself).
+template <class F> F driver_fn(const char* name) {
+  void* fn = nullptr;
+  cudaDriverEntryPointQueryResult q;
+  QSVB_CK(cudaGetDriverEntryPoint(name, &fn, cudaEnableDefault, &q));
+  QSVB_REQUIRE(q == cudaDriverEntryPointSuccess && fn != nullptr, std::string("driver entry point missing: ") + name);
+  return reinterpret_cast<F>(fn);
+}
+
+// Id of the current CUDA context (unique for the life of the process; a context created after a
+// cudaDeviceReset gets a new one).
+unsigned long long current_context_id() {
+  using GetCurrent = CUresult (*)(CUcontext*);
+  using GetId = CUresult (*)(CUcontext, unsigned long long*);
+  static const GetCurrent get_current = driver_fn<GetCurrent>("cuCtxGetCurrent");
+  static const GetId get_id = driver_fn<GetId>("cuCtxGetId");
+  CUcontext ctx = nullptr;
+  unsigned long long id = 0;
+  QSVB_REQUIRE(get_current(&ctx) == CUDA_SUCCESS && ctx != nullptr, "no current CUDA context");
+  QSVB_REQUIRE(get_id(ctx, &id) == CUDA_SUCCESS, "cuCtxGetId failed");
+  return id;
+}
+
+// Device address of the scratch array on the current device (set up once per device and context).
 double* scratch_for(int dev) {
   QSVB_REQUIRE(dev >= 0 && dev < kMaxDevices, "device ordinal out of range");
+  const unsigned long long ctx = current_context_id();
   std::lock_guard<std::mutex> lk(g_mu);
-  if (!g_scratch_addr[dev]) {
+  if (!g_scratch_addr[dev] || g_scratch_ctx[dev] != ctx) {
     void* p = nullptr;
     QSVB_CK(cudaGetSymbolAddress(&p, g_noalloc_scratch));
     g_scratch_addr[dev] = static_cast<double*>(p);
+    g_scratch_ctx[dev] = ctx;
   }
   return g_scratch_addr[dev];
+}
+
+// The caller's buffer must be device or managed memory of `dev`, 16-byte aligned.
+void require_device_buffer(const void* p, int dev, const char* name) {
+  QSVB_REQUIRE(reinterpret_cast<uintptr_t>(p) % 16 == 0, std::string(name) + " must be 16-byte aligned");
+  cudaPointerAttributes a{};
+  const cudaError_t e = cudaPointerGetAttributes(&a, p);
+  if (e != cudaSuccess) {
+    (void)cudaGetLastError();  // reset the runtime's last-error state that the failed query set
+    throw Error(QSVB_E_INVALID, std::string(name) + " is not a CUDA pointer");
+  }
+  QSVB_REQUIRE(a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged,
+               std::string(name) + " must be device or managed memory");
+  QSVB_REQUIRE(a.device == dev, std::string(name) + " belongs to another device");
 }
 
 }  // namespace
@@ -64,6 +112,9 @@ extern "C" int qsvb_expectation_z_noalloc(const void* d_re, const void* d_im, ui
     QSVB_REQUIRE(dtype == QSVB_C64 || dtype == QSVB_C128, "dtype must be QSVB_C64 or QSVB_C128");
     int dev = 0, sms = 0;
     QSVB_CK(cudaGetDevice(&dev));
+    QSVB_CK(cudaSetDevice(dev));  // makes the device's primary context current (no allocation)
+    require_device_buffer(d_re, dev, "d_re");
+    require_device_buffer(d_im, dev, "d_im");
     QSVB_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     QSVB_REQUIRE(reduce_partials_needed(sms) <= size_t(2 * kNoAllocMaxCtas),
                  "device has more SMs than the allocation-free scratch (1024 partial sums) serves");

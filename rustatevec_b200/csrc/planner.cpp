@@ -589,6 +589,7 @@ void sweep_costs(const std::vector<Sweep>& sw, uint32_t n, int dtype, qsvb_plan_
     if (s.kind == SK_TILE) st->flops += s.tile_flops;
   }
   st->predicted_seconds = predict_plan_seconds(sw, n, dtype);
+  st->measured_seconds = 0.0;
 }
 
 }  // namespace qsvb

@@ -186,6 +186,7 @@ qsvb_batch* batch_create(qsvb_ctx* c, const qsvb_circuit* circuits, size_t n, in
                          uint32_t register_qubits);
 void batch_run(qsvb_ctx* c, qsvb_batch* b, double* z0_out, double* probs_out, const uint64_t* probs_offset,
                qsvb_plan_stats* stats);
+void batch_set_wait_budget(qsvb_ctx* c, qsvb_batch* b, uint64_t cycles);
 void batch_autotune(qsvb_ctx* c, const qsvb_circuit* circuits, size_t n, int dtype, uint32_t* best_local,
                     uint32_t* best_reg, double* seconds, size_t cap, size_t* count);
 }  // namespace qsvb

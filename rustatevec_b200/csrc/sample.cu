@@ -1,14 +1,18 @@
-// Measurement sampling on the device: shots drawn from the state's FP64 outcome distribution
-// without downloading it.
+// Measurement sampling on the device: shots drawn from the state's outcome distribution without
+// downloading it, by the inverse-CDF rule of qsv's cdf_sample (crates/qsv-core/src/sample.rs:163-172).
 //
 // Shot k takes the k-th `unit()` value of SplitMix64(seed) (crates/qsv-core/src/circuits.rs:22-46),
-// u_k in [0, 1), and returns the outcome i with CDF(i-1) <= u_k * total < CDF(i), CDF being the
-// inclusive prefix sum of |amp|^2 in index order (inverse-CDF sampling; the trait default in
-// crates/qsv-core/src/sample.rs:84-97 draws from an alias table instead, so the two agree in
-// distribution, not draw by draw). Steps: FP64 sums of 8192-amplitude blocks; an exclusive scan of
-// those; the scaled uniforms sorted with their shot numbers; then one pass over the blocks: a block
-// holding sorted shots scans its own probabilities in shared memory and places each shot by binary
-// search, writing the outcome at the shot's original position.
+// u_k in [0, 1), scales it by the total probability, x_k = u_k * total, and returns the first
+// outcome i whose cumulative probability CDF(i) >= x_k (cdf_sample's `partition_point(|&c| c < u)`,
+// a lower bound; the last outcome if rounding leaves none). The probabilities are |amp|^2 computed
+// as the trait's `probabilities` does, in the state's precision (re*re + im*im, no fused
+// multiply-add), and accumulated in FP64; the device sums them in another order than the
+// reference's chunked scan, so a draw can differ only where x_k lies within rounding of a CDF value.
+// Steps: the FP64 total of each 8192-amplitude block; an exclusive scan of those; the scaled
+// uniforms sorted with their shot numbers; then one pass over the blocks: block b takes the sorted
+// values x with CDFstart(b) < x <= CDFstart(b + 1) (block 0 also x = 0), builds its inclusive
+// prefix in shared memory and places each shot by binary search, writing the outcome at the shot's
+// original position.
 
 #include <cuda_runtime.h>
 
@@ -34,6 +38,13 @@ template <class T> struct DevBuf {
   DevBuf& operator=(const DevBuf&) = delete;
 };
 
+// |amp|^2 rounded as StateVector::probabilities computes it in the state's precision
+// (crates/qsv-core/src/state/mod.rs:130-134: re*re + im*im with separate roundings), widened to FP64.
+__device__ __forceinline__ double prob_of(float x, float y) {
+  return double(__fadd_rn(__fmul_rn(x, x), __fmul_rn(y, y)));
+}
+__device__ __forceinline__ double prob_of(double x, double y) { return __dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y)); }
+
 __device__ __forceinline__ uint64_t mix64s(uint64_t z) {
   z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
   z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
@@ -51,8 +62,7 @@ __global__ void __launch_bounds__(kSampleThreads) k_block_sums(const R* __restri
     double acc = 0.0;
     for (uint32_t i = threadIdx.x; i < B; i += kSampleThreads) {
       const uint64_t a = (b << bb) + i;
-      const double x = double(re[a]), y = double(im[a]);
-      acc += x * x + y * y;
+      acc += prob_of(re[a], im[a]);
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
@@ -80,18 +90,19 @@ __global__ void k_uniforms(uint64_t shots, uint64_t seed, const double* __restri
   }
 }
 
-__device__ __forceinline__ uint64_t lower_bound_keys(const uint64_t* __restrict__ keys, uint64_t n, double x) {
+// First index of the sorted keys whose value is > x.
+__device__ __forceinline__ uint64_t upper_bound_keys(const uint64_t* __restrict__ keys, uint64_t n, double x) {
   uint64_t lo = 0, hi = n;
   while (lo < hi) {
     const uint64_t mid = (lo + hi) >> 1;
-    if (__longlong_as_double(keys[mid]) < x) lo = mid + 1;
+    if (__longlong_as_double(keys[mid]) <= x) lo = mid + 1;
     else hi = mid;
   }
   return lo;
 }
 
-// Each block that holds shots (the sorted scaled uniforms in [bcdf[b], bcdf[b+1])) scans its
-// probabilities (FP64, inclusive) and places its shots.
+// Each block that holds shots (the sorted scaled uniforms in (bcdf[b], bcdf[b+1]]; block 0 from
+// 0 inclusive) scans its probabilities (FP64, inclusive) and places its shots.
 template <class R>
 __global__ void __launch_bounds__(kSampleThreads) k_assign(const R* __restrict__ re, const R* __restrict__ im,
                                                            uint32_t bb, uint64_t nblocks,
@@ -107,9 +118,8 @@ __global__ void __launch_bounds__(kSampleThreads) k_assign(const R* __restrict__
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   for (uint64_t b = blockIdx.x; b < nblocks; b += gridDim.x) {
     if (tid == 0) {
-      const double lo = bcdf[b];
-      s_range[0] = lower_bound_keys(keys, shots, lo);
-      s_range[1] = b + 1 == nblocks ? shots : lower_bound_keys(keys, shots, bcdf[b + 1]);
+      s_range[0] = b == 0 ? 0 : upper_bound_keys(keys, shots, bcdf[b]);
+      s_range[1] = b + 1 == nblocks ? shots : upper_bound_keys(keys, shots, bcdf[b + 1]);
     }
     __syncthreads();
     const uint64_t j0 = s_range[0], j1 = s_range[1];
@@ -121,8 +131,7 @@ __global__ void __launch_bounds__(kSampleThreads) k_assign(const R* __restrict__
       if (first < B)
         for (uint32_t e = 0; e < per; ++e) {
           const uint64_t a = (b << bb) + first + e;
-          const double x = double(re[a]), y = double(im[a]);
-          run += x * x + y * y;
+          run += prob_of(re[a], im[a]);
           s_pre[first + e] = run;
         }
       // exclusive scan of the run totals across the block
@@ -148,16 +157,20 @@ __global__ void __launch_bounds__(kSampleThreads) k_assign(const R* __restrict__
       if (first < B)
         for (uint32_t e = 0; e < per; ++e) s_pre[first + e] += off;
       __syncthreads();
+      const double base = bcdf[b];
       for (uint64_t j = j0 + tid; j < j1; j += kSampleThreads) {
-        const double t = __longlong_as_double(keys[j]) - bcdf[b];
-        uint32_t lo = 0, hi = B - 1;  // first index with prefix > t (the last one if none)
+        const double x = __longlong_as_double(keys[j]);
+        // the first index whose cumulative probability base + prefix is >= x (the block's last
+        // one if none: rounding can leave x just above the block's own total)
+        uint32_t lo = 0, hi = B - 1;
         while (lo < hi) {
           const uint32_t mid = (lo + hi) >> 1;
-          if (s_pre[mid] > t) hi = mid;
+          if (__dadd_rn(base, s_pre[mid]) >= x) hi = mid;
           else lo = mid + 1;
         }
-        // rounding can leave t at the block's very end: step back over trailing zero probabilities
-        while (lo > 0 && s_pre[lo] == s_pre[lo - 1] && s_pre[lo] <= t) --lo;
+        // in that clamped case, step back over trailing zero probabilities
+        if (__dadd_rn(base, s_pre[lo]) < x)
+          while (lo > 0 && s_pre[lo] == s_pre[lo - 1]) --lo;
         out[vals[j]] = (b << bb) + lo;
       }
     }

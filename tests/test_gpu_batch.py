@@ -46,7 +46,8 @@ def check_batch(be, circuits, local_qubits=0, register_qubits=0):
         got = probs[off:off + sizes[i]]
         off += sizes[i]
         assert np.max(np.abs(got - want)) <= TOL[be.precision], (i, c.n_qubits(), local_qubits)
-        assert abs(z0[i] - oracle.expectation_z(want, 1)) <= 4 * TOL[be.precision] * max(1, c.n_qubits()), i
+        zerr = abs(z0[i] - oracle.expectation_z(want, 1))
+        assert zerr <= TOL[be.precision], (i, zerr)
     return st.to_dict()
 
 
@@ -164,7 +165,7 @@ def test_backend_execute_batch_matches_single_circuit_path(be):
         assert np.max(np.abs(probs[i] - p)) <= TOL[be.precision]
         assert abs(z0[i] - be.expectation_z(s, 1)) <= (1e-4 if be.precision == "f32" else 1e-10)
         s.free()
-    assert st["predicted_seconds"] > 0
+    assert st["measured_seconds"] > 0 and st["predicted_seconds"] == 0
 
 
 def test_batch_rejects_invalid_input(be):
@@ -179,3 +180,33 @@ def test_batch_rejects_invalid_input(be):
                                            z0.ctypes.data_as(C.POINTER(C.c_double)), None, None, None)
         assert rc == L.QSVB_E_INVALID, (circuits[0].n_qubits(), lq, rq)
     assert L.lib().qsvb_execute_batch(be.ctx, None, 0, be.dtype, None, None, None, None) == L.QSVB_E_INVALID
+
+
+def test_dependency_wait_that_runs_out_fails_the_run_and_the_context_recovers(be):
+    """A multi-pass batch with a dependency-wait budget of one clock64 cycle: the tiles of pass 1
+    that are taken while pass 0 is still running give up at once, the run returns QSVB_E_TIMEOUT,
+    and with the default budget restored the same batch object runs correctly on the same context."""
+    rng = SplitMix64(2024)
+    circuits = [ansatz_circuit(20, 6, rng), ansatz_circuit(19, 5, rng)]
+    pb = L.PackedBatch(circuits)
+    lib = L.lib()
+    h = C.c_void_p()
+    L.check(lib.qsvb_batch_create(be.ctx, pb.ptr(), pb.count, be.dtype, 12, 0, C.byref(h)))
+    try:
+        z0 = np.zeros(pb.count)
+        zp = z0.ctypes.data_as(C.POINTER(C.c_double))
+        st = L.PlanStats()
+        L.check(lib.qsvb_batch_run(be.ctx, h, zp, None, None, C.byref(st)))
+        assert st.n_sweeps >= 4  # several passes over HBM per circuit: tiles wait on earlier passes
+        L.check(lib.qsvb_batch_set_wait_budget(be.ctx, h, 1))
+        codes = [lib.qsvb_batch_run(be.ctx, h, zp, None, None, None) for _ in range(3)]
+        assert L.QSVB_E_TIMEOUT in codes, codes
+        assert "budget" in lib.qsvb_last_error().decode()
+        L.check(lib.qsvb_batch_set_wait_budget(be.ctx, h, 0))
+        L.check(lib.qsvb_batch_run(be.ctx, h, zp, None, None, None))
+        for i, c in enumerate(circuits):
+            want = oracle.expectation_z(oracle_probs(c), 1)
+            assert abs(z0[i] - want) <= TOL[be.precision], (i, z0[i], want)
+        assert lib.qsvb_batch_set_wait_budget(be.ctx, h, 1 << 41) == L.QSVB_E_INVALID
+    finally:
+        L.check(lib.qsvb_batch_free(be.ctx, h))

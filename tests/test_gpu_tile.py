@@ -88,7 +88,7 @@ def test_ghz_chain_known_answer(be):
     got, st = run(be, ghz_chain(n))
     p = np.abs(got) ** 2
     assert abs(p[0] - 0.5) < TOL[be.precision] and abs(p[-1] - 0.5) < TOL[be.precision]
-    assert abs(p.sum() - 1.0) < 10 * TOL[be.precision]
+    assert abs(p.sum() - 1.0) < TOL[be.precision]
 
 
 def test_wider_gates_split_tile_runs(be):

@@ -222,3 +222,25 @@ def test_circuit_push_validation():
         c.push(G.h(), [3])
     with pytest.raises(ValueError):
         c.push(G.cx(), [1, 1])
+
+
+def test_samplers_against_the_reference_unit_tests():
+    """Host samplers: the alias table (sample.rs:217-232) and the cdf_sample restatement
+    (sample.rs:163-172), on the reference's own test distributions and SplitMix64 seeds."""
+    from rustatevec_b200.circuits import SplitMix64
+    from rustatevec_b200.sample import alias_sample
+    w = np.array([0.1, 0.6, 0.0, 0.3])
+    counts = np.bincount(alias_sample(w, 40000, SplitMix64(0xDEADBEEF)), minlength=4)
+    assert counts[2] == 0
+    assert np.max(np.abs(counts / 40000 - w)) < 0.01
+    idx, u, cdf = oracle.cdf_sample(w, 40000, 0xDEADBEEF)
+    assert np.count_nonzero(idx == 2) == 0 and np.max(np.abs(np.bincount(idx, minlength=4) / 40000 - w)) < 0.01
+    # the vectorised stream equals the scalar generator, and the rule is a lower bound
+    r = SplitMix64(5)
+    assert np.array_equal(oracle.splitmix_units(5, 16), np.array([r.unit() for _ in range(16)]))
+    cdf = np.cumsum([0.0, 0.5, 0.5])
+    assert int(np.searchsorted(cdf, 0.5, side="left")) == 1  # u on a boundary takes the lower outcome
+    w2 = np.array([0.25, 0.25, 0.4, 0.1])
+    a = np.bincount(alias_sample(w2, 40000, SplitMix64(1)), minlength=4) / 40000
+    b = np.bincount(oracle.cdf_sample(w2, 40000, 2)[0], minlength=4) / 40000
+    assert np.max(np.abs(a - b)) < 0.02
