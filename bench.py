@@ -155,6 +155,47 @@ def cpu_baseline(circuit, budget_s: float = 15.0) -> dict:
                       f"({hist}; {dt:.1f} s, OpenMP x{cores}); value = sum over arities of ops x mean time"}
 
 
+def lscpu_summary() -> dict:
+    """Host CPU facts for the baseline (lscpu), so the core count the baseline uses is checkable."""
+    keys = ("Model name", "Socket(s)", "Core(s) per socket", "Thread(s) per core", "CPU(s)", "NUMA node(s)")
+    out = {}
+    try:
+        txt = subprocess.run(["lscpu"], capture_output=True, text=True, timeout=10).stdout
+        for line in txt.splitlines():
+            k, _, v = line.partition(":")
+            if k.strip() in keys:
+                out[k.strip()] = v.strip()
+    except Exception as e:  # lscpu missing: report why
+        out["error"] = str(e)
+    return out
+
+
+def cpu_full_circuits(sizes=(24, 26, 28)) -> dict:
+    """The CpuBackend restatement (OpenMP, all host threads) on the WHOLE reference-fused brickwork
+    circuit (same depth and seed) at smaller sizes: every op timed, nothing sampled. These anchor
+    the sampled 30-qubit estimate; the per-amplitude cost at 28 qubits times 4 is a second,
+    fully-timed extrapolation to 30 qubits."""
+    import oracle
+    from rustatevec_b200.circuits import brickwork
+    L = oracle.lib()
+    out = {}
+    for n in sizes:
+        c = brickwork(n, DEPTH, SEED)
+        arity, qubits, mats = oracle.fuse(c, 4, oracle.F32)
+        re = np.zeros(1 << n, dtype=np.float32)
+        im = np.zeros(1 << n, dtype=np.float32)
+        re[0] = 1.0
+        t0 = time.perf_counter()
+        rc = L.orc_run(oracle.CPU_PARALLEL, oracle.F32, n, re.ctypes.data, im.ctypes.data, len(arity), arity, qubits,
+                       mats)
+        out[str(n)] = round(time.perf_counter() - t0, 3)
+        if rc:
+            raise RuntimeError("oracle rejected the circuit")
+    if "28" in out:
+        out["extrapolated_30q_from_28q"] = round(out["28"] * 4.0, 2)
+    return out
+
+
 # ------------------------------------------------------------------ GPU
 def dist_setup():
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -225,14 +266,25 @@ def run_gpu(args):
         "window_k4_cuda": L.make_opts(PLAN_WINDOW, 4, ENGINE_CUDA_CORE),
         "learned_cuda": L.make_opts(PLAN_LEARNED, 6, ENGINE_CUDA_CORE),
         "greedy_k6_tc": L.make_opts(PLAN_GREEDY, 6, ENGINE_TENSOR_CORE),
+        "window_k6_tc": L.make_opts(PLAN_WINDOW, 6, ENGINE_TENSOR_CORE),
         "tile": L.make_opts(L.PLAN_TILE, 4, ENGINE_AUTO),
+        "chain_m2": L.make_opts(L.PLAN_CHAIN, 6, ENGINE_AUTO, chain_max_matrices=2),
+        "chain_m3": L.make_opts(L.PLAN_CHAIN, 6, ENGINE_AUTO, chain_max_matrices=3),
+        # the learned planner with the cost model removed (its analytic roofline model instead)
+        "learned_tc_roofline_model": L.make_opts(PLAN_LEARNED, 6, ENGINE_AUTO),
         "learned_tc": L.make_opts(PLAN_LEARNED, 6, ENGINE_AUTO),
     }
     headline = "learned_tc"
     results = {}
     plans = {}
     for name, o in methods.items():
-        p = Plan(be, circuit, o)
+        if name == "learned_tc_roofline_model":
+            tuning.install(None)
+            p = Plan(be, circuit, o)
+            if model_doc:
+                tuning.install(model_doc["model"])
+        else:
+            p = Plan(be, circuit, o)
         plans[name] = p
         if name == headline or args.quick:
             continue
@@ -317,6 +369,10 @@ def run_gpu(args):
         e2e = e0.elapsed_time(e1) * 1e-3 / e2e_steps
 
         cpu = cpu_baseline(circuit, budget_s=args.cpu_budget) if not args.no_cpu else None
+        if cpu is not None:
+            cpu["lscpu"] = lscpu_summary()
+            if not args.no_cpu_scaling:
+                cpu["full_circuit_seconds"] = cpu_full_circuits()
         n_launch = args.steps * (hst["n_sweeps"] + 1)
         out = {
             "metric": METRIC, "value": round(t_step, 6), "unit": "s", "n_gpus": world,
@@ -374,7 +430,7 @@ def run_reference(args):
            "vs_baseline": None, "dtype": "f32 (complex64)", "data": "synthetic (seeded brickwork circuit)",
            "config": {"workload": WORKLOAD, "n_qubits": N_QUBITS, "depth": DEPTH},
            "cpu_baseline": {"value": round(v, 3), "unit": "s", "cores": last["cores"], "kind": last["kind"],
-                            "sample": last["sample"]},
+                            "sample": last["sample"], "lscpu": lscpu_summary()},
            "e2e": {"value": round(v, 3), "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)
 
@@ -815,8 +871,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--quick", action="store_true", help="headline plan only")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--cpu-budget", type=float, default=15.0)
-    ap.add_argument("--ref-budget", type=float, default=6.0)
+    ap.add_argument("--cpu-budget", type=float, default=10.0)
+    ap.add_argument("--ref-budget", type=float, default=10.0)
+    ap.add_argument("--no-cpu-scaling", action="store_true", help="skip the full-circuit CPU runs at 24-28 qubits")
     ap.add_argument("--config", default="brickwork30", choices=["brickwork30", "ghz24", "qft32", "qaoa33", "batched"],
                     help="workload (the default is the headline bench line)")
     ap.add_argument("--circuits", type=int, default=4096, help="batched config: number of circuits")

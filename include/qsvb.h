@@ -66,10 +66,16 @@ typedef enum qsvb_planner {
   QSVB_PLAN_WINDOW = 2,   /* commutation-aware windows: gates on disjoint qubits reorder */
   QSVB_PLAN_LEARNED = 3,  /* cost-model planner (MLP cost model; greedy fallback); also weighs
                              tile passes against fused sweeps */
-  QSVB_PLAN_TILE = 4      /* tile passes: the 1- and 2-qubit gates acting inside a set of up to
+  QSVB_PLAN_TILE = 4,     /* tile passes: the 1- and 2-qubit gates acting inside a set of up to
                              12 qubits (11 for complex128) that commute past the gates left for
                              later, applied on shared-memory tiles in one read and one write of
                              the state; diagonal runs become phase sweeps, wider gates fused sweeps */
+  QSVB_PLAN_CHAIN = 5     /* tensor-core chain passes (complex64, n >= 12): each pass takes a set of
+                             12 qubits, applies up to chain_max_matrices fused 6-qubit matrices of
+                             the gates inside it on tcgen05 in one read and one write of the state,
+                             and relabels which qubits sit on the state's low bits for the next
+                             pass; permutation passes put every qubit back on its own bit at the end.
+                             Other states (complex128, n < 12, CUDA-core engine) plan as WINDOW. */
 } qsvb_planner;
 
 typedef enum qsvb_engine {
@@ -83,14 +89,16 @@ typedef struct qsvb_plan_opts {
   uint32_t max_fused_qubits; /* fusion width cap, 1..6 (ignored by AS_GIVEN) */
   uint32_t engine;           /* qsvb_engine */
   uint32_t use_graph;        /* capture the sweep sequence in a CUDA graph */
-  uint32_t reserved[4];
+  uint32_t chain_max_matrices; /* QSVB_PLAN_CHAIN: matrices per pass, 1..3 (0: chosen by cost) */
+  uint32_t reserved[3];
 } qsvb_plan_opts;
 
 /* What a plan does, for reports and rooflines. */
 typedef struct qsvb_plan_stats {
   uint64_t n_gates_in;        /* gates in the input circuit */
   uint64_t n_sweeps;          /* kernel sweeps launched per run */
-  uint64_t n_sweeps_by_kind[8]; /* 1q, ctrl1q, diag, phase, dense CUDA-core, dense TC, swap, other */
+  uint64_t n_sweeps_by_kind[10]; /* 1q, ctrl1q, diag, phase, dense CUDA-core, dense TC, tile pass,
+                                   other, tensor-core chain pass, tile permutation */
   double algorithmic_bytes;   /* sum over sweeps of 2 * (amplitudes the sweep may change) * bytes/amp */
   double full_sweep_bytes;    /* sum over sweeps of 2 * 2^n * bytes/amp */
   double flops;               /* complex-MAC flops of the dense sweeps (8 * 2^k per amplitude) */
@@ -144,9 +152,11 @@ int qsvb_plan_free(qsvb_ctx* ctx, qsvb_plan* plan);
 
 /* One sweep of a plan, as the planner and the cost model see it. */
 typedef struct qsvb_sweep_info {
-  uint32_t kind;                  /* 0 1q, 1 ctrl1q, 2 diag, 3 phase, 4 dense CUDA-core, 5 dense TC */
-  uint32_t n_qubits;              /* matrix qubits (dense/diag) */
-  uint32_t qubits[QSVB_MAX_GATE_QUBITS];
+  uint32_t kind;                  /* 0 1q, 1 ctrl1q, 2 diag, 3 phase, 4 dense CUDA-core, 5 dense TC,
+                                     6 tile pass, 8 tensor-core chain pass, 9 tile permutation */
+  uint32_t n_qubits;              /* matrix qubits (dense/diag); matrices of a chain pass */
+  uint32_t qubits[QSVB_MAX_GATE_QUBITS]; /* chain / permutation passes: the tile's state bits
+                                            above bit 5 */
   uint32_t target;                /* butterflies */
   uint32_t n_ctrl;                /* controls (ctrl1q) or skipped identity halves (diag) */
   uint32_t ctrl[QSVB_MAX_GATE_QUBITS];

@@ -22,11 +22,11 @@ QSVB_E_UNSUPPORTED = -4
 QSVB_E_TIMEOUT = -5
 
 C64, C128 = 0, 1
-PLAN_AS_GIVEN, PLAN_GREEDY, PLAN_WINDOW, PLAN_LEARNED, PLAN_TILE = 0, 1, 2, 3, 4
+PLAN_AS_GIVEN, PLAN_GREEDY, PLAN_WINDOW, PLAN_LEARNED, PLAN_TILE, PLAN_CHAIN = 0, 1, 2, 3, 4, 5
 ENGINE_AUTO, ENGINE_CUDA_CORE, ENGINE_TENSOR_CORE = 0, 1, 2
 MAX_GATE_QUBITS = 6
 
-SWEEP_KINDS = ("1q", "ctrl1q", "diag", "phase", "dense", "dense_tc", "tile", "other")
+SWEEP_KINDS = ("1q", "ctrl1q", "diag", "phase", "dense", "dense_tc", "tile", "other", "tc_chain", "permute")
 
 
 class QsvbError(RuntimeError):
@@ -46,12 +46,12 @@ class CircuitS(C.Structure):
 
 class PlanOpts(C.Structure):
     _fields_ = [("planner", C.c_uint32), ("max_fused_qubits", C.c_uint32), ("engine", C.c_uint32),
-                ("use_graph", C.c_uint32), ("reserved", C.c_uint32 * 4)]
+                ("use_graph", C.c_uint32), ("chain_max_matrices", C.c_uint32), ("reserved", C.c_uint32 * 3)]
 
 
 class PlanStats(C.Structure):
     _fields_ = [("n_gates_in", C.c_uint64), ("n_sweeps", C.c_uint64),
-                ("n_sweeps_by_kind", C.c_uint64 * 8), ("algorithmic_bytes", C.c_double),
+                ("n_sweeps_by_kind", C.c_uint64 * 10), ("algorithmic_bytes", C.c_double),
                 ("full_sweep_bytes", C.c_double), ("flops", C.c_double),
                 ("predicted_seconds", C.c_double), ("measured_seconds", C.c_double)]
 
@@ -229,10 +229,12 @@ class PackedBatch:
         return C.cast(self.circs.ctypes.data, C.POINTER(CircuitS))
 
 
-def make_opts(planner=PLAN_GREEDY, max_fused_qubits=4, engine=ENGINE_AUTO, use_graph=True) -> PlanOpts:
+def make_opts(planner=PLAN_GREEDY, max_fused_qubits=4, engine=ENGINE_AUTO, use_graph=True,
+              chain_max_matrices=0) -> PlanOpts:
     o = PlanOpts()
     o.planner = planner
     o.max_fused_qubits = max_fused_qubits
     o.engine = engine
     o.use_graph = 1 if use_graph else 0
+    o.chain_max_matrices = chain_max_matrices
     return o

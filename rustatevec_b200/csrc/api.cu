@@ -418,6 +418,10 @@ int qsvb_plan_sweep_info(const qsvb_plan* p, size_t i, qsvb_sweep_info* out) {
     out->n_ctrl = s.nctrl;
     out->n_terms = uint32_t(s.terms.size());
     out->n_gates = s.n_gates;
+    if (s.kind == SK_TC_CHAIN || s.kind == SK_PERMUTE) {
+      out->n_qubits = s.chain_nmat;
+      for (uint32_t j = 0; j < 6; ++j) out->qubits[j] = s.chain_tbits[6 + j];
+    }
     qsvb_plan_stats one{};
     sweep_costs(std::vector<Sweep>{s}, p->n_qubits, p->dtype, &one);
     out->algorithmic_bytes = one.algorithmic_bytes;

@@ -30,6 +30,10 @@ constexpr double kTileFp32Flops = 29.5e12;
 constexpr double kTileFp64Flops = 15.5e12;
 constexpr double kTileMemFactor32 = 1.95;
 constexpr double kTileMemFactor64 = 1.80;
+// chain and permutation passes (not in the cost model's training records: roofline times an
+// overhead factor)
+constexpr double kChainOverhead = 1.25;
+constexpr double kPermuteOverhead = 1.15;
 
 int lowest_bit(const Sweep& s) {
   uint32_t lo = 64;
@@ -93,6 +97,13 @@ double analytic_sweep_seconds(const Sweep& s, uint32_t n, int dtype) {
     comp = 8.0 * std::ldexp(1.0, int(s.m)) * dim / (dtype == QSVB_C128 ? kFp64FmaFlops : kFp32FmaFlops);
   if (s.kind == SK_DENSE_TC) comp = 3.0 * 8.0 * std::ldexp(1.0, int(s.m)) * dim / kTcFlops;
   if (s.kind == SK_PHASE) comp = double(s.terms.size()) * 4.0 * dim / 30.0e12 + 40.0 * dim / kFp64FmaFlops;
+  if (s.kind == SK_TC_CHAIN) {
+    // one read and one write of the state; per matrix three bf16 MMAs (1536 flops an amplitude)
+    // and its operand traffic through shared memory, overlapped with the memory stream
+    const double per_mat = 1536.0 * dim / kTcFlops;
+    return std::max(mem, double(s.chain_nmat) * per_mat) * kChainOverhead + kLaunchSeconds;
+  }
+  if (s.kind == SK_PERMUTE) return mem * kPermuteOverhead + kLaunchSeconds;
   if (s.kind == SK_TILE) {
     // each block loads, updates and stores its tile in turn: memory and arithmetic add up
     const double rate = dtype == QSVB_C128 ? kTileFp64Flops : kTileFp32Flops;
@@ -214,7 +225,8 @@ Sweep shrink_sweep(const Sweep& s, uint32_t n) {
 
 double predict_sweep_seconds(const Sweep& s, uint32_t n, int dtype) {
   const MlpModel& m = g_model;
-  if (m.hidden > 0 && s.kind != SK_TILE) {  // the model has not been trained on tile sweeps
+  // the model has not been trained on tile, chain or permutation passes
+  if (m.hidden > 0 && s.kind != SK_TILE && s.kind != SK_TC_CHAIN && s.kind != SK_PERMUTE) {
     float f[kNumFeatures];
     if (n > kModelMaxQubits && n - kModelMaxQubits <= 20) {
       sweep_features(shrink_sweep(s, n), kModelMaxQubits, dtype, f);

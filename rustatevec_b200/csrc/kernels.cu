@@ -984,6 +984,7 @@ size_t sweep_matrix_bytes(const Sweep& s, int dtype) {
     case SK_DENSE_TC: return tc_matrix_bytes(s);
     case SK_PHASE: return s.terms.size() * sizeof(PhaseTermDev);
     case SK_TILE: return s.tile_blob.size();
+    case SK_TC_CHAIN: return tc_chain_matrix_bytes(s);
     default: return 0;
   }
 }
@@ -1007,6 +1008,8 @@ void pack_sweep_matrix(const Sweep& s, int dtype, void* dst) {
     std::memcpy(dst, s.tile_blob.data(), s.tile_blob.size());
   } else if (s.kind == SK_DENSE_TC) {
     tc_pack_matrix(s, dst);
+  } else if (s.kind == SK_TC_CHAIN) {
+    tc_chain_pack(s, dst);
   } else if (s.kind == SK_PHASE) {
     PhaseTermDev* t = static_cast<PhaseTermDev*>(dst);
     for (size_t i = 0; i < s.terms.size(); ++i) {
@@ -1032,6 +1035,13 @@ void launch_sweep(const LaunchEnv& env, R* re, R* im, uint32_t n, const Sweep& s
       }
       throw Error(QSVB_E_UNSUPPORTED, "tensor-core sweeps need a complex64 state");
     case SK_TILE: launch_tile<R>(env, re, im, n, s, dev_mat); break;
+    case SK_TC_CHAIN:
+      if constexpr (sizeof(R) == 4) {
+        launch_tc_chain(env, reinterpret_cast<float*>(re), reinterpret_cast<float*>(im), n, s, dev_mat);
+        break;
+      }
+      throw Error(QSVB_E_UNSUPPORTED, "tensor-core chain passes need a complex64 state");
+    case SK_PERMUTE: launch_permute<R>(env, re, im, n, s); break;
     case SK_NONE: break;
     default: throw Error(QSVB_E_UNSUPPORTED, "unknown sweep kind");
   }

@@ -299,6 +299,9 @@ bool phase_representable(const Gate& g) {
 
 }  // namespace
 
+Gate compose_gates(const std::vector<uint32_t>& q, const std::vector<const Gate*>& ops) { return compose(q, ops); }
+uint64_t gate_mask(const Gate& g) { return qmask(g); }
+
 std::vector<Gate> fuse_greedy_public(const std::vector<Gate>& in, uint32_t maxq, bool cost_only) {
   return fuse_greedy(in, maxq, cost_only);
 }
@@ -402,6 +405,26 @@ std::vector<Sweep> plan_sweeps(const std::vector<Gate>& in, uint32_t n, const qs
   o.max_fused_qubits = std::min<uint32_t>(o.max_fused_qubits, std::min<uint32_t>(QSVB_MAX_GATE_QUBITS, n));
   // tile passes absorb diagonal runs themselves (per-tile phases outside the local set)
   if (o.planner == QSVB_PLAN_TILE) return plan_with(in, n, o, dtype, false, TILE_ALWAYS);
+  const bool chain_ok = dtype == QSVB_C64 && n >= 12 && o.engine != QSVB_ENGINE_CUDA_CORE;
+  if (o.planner == QSVB_PLAN_CHAIN) {
+    if (!chain_ok) {  // chain passes need a complex64 state of >= 12 qubits and the tensor cores
+      qsvb_plan_opts w = o;
+      w.planner = QSVB_PLAN_WINDOW;
+      return plan_with(in, n, w, dtype, false, TILE_NO);
+    }
+    if (o.chain_max_matrices != 0) return plan_chain(in, n, o.chain_max_matrices);
+    std::vector<Sweep> best;
+    double best_t = 1e300;
+    for (uint32_t m = 1; m <= uint32_t(kChainMaxMats); ++m) {
+      std::vector<Sweep> cand = plan_chain(in, n, m);
+      const double t = predict_plan_seconds(cand, n, dtype);
+      if (t < best_t) {
+        best_t = t;
+        best = std::move(cand);
+      }
+    }
+    return best;
+  }
   if (o.planner != QSVB_PLAN_LEARNED) return plan_with(in, n, o, dtype, false, TILE_NO);
   // learned: merging long diagonal runs into phase-polynomial sweeps, and running gate runs as
   // tile passes, are candidate choices weighed by predicted time
@@ -411,10 +434,14 @@ std::vector<Sweep> plan_sweeps(const std::vector<Gate>& in, uint32_t n, const qs
     fut.push_back(std::async(std::launch::async, [&, c] {
       return plan_with(in, n, o, dtype, (c & 1) == 0, c < 2 ? TILE_NO : TILE_CHOOSE);
     }));
+  // chain passes (complex64 on the tensor cores, states of >= 14 qubits) at 2 and 3 matrices a pass
+  if (chain_ok && n >= 14)
+    for (uint32_t m = 2; m <= uint32_t(kChainMaxMats); ++m)
+      fut.push_back(std::async(std::launch::async, [&, m] { return plan_chain(in, n, m); }));
   std::vector<Sweep> best;
   double best_t = 1e300;
-  for (int c = 0; c < 4; ++c) {
-    std::vector<Sweep> cand = fut[size_t(c)].get();
+  for (size_t c = 0; c < fut.size(); ++c) {
+    std::vector<Sweep> cand = fut[c].get();
     const double t = predict_plan_seconds(cand, n, dtype);
     if (t < best_t) {
       best_t = t;
@@ -579,7 +606,7 @@ void sweep_costs(const std::vector<Sweep>& sw, uint32_t n, int dtype, qsvb_plan_
   st->algorithmic_bytes = st->full_sweep_bytes = st->flops = 0;
   for (const Sweep& s : sw) {
     int kind = s.kind;
-    st->n_sweeps_by_kind[kind < 8 ? kind : 7]++;
+    st->n_sweeps_by_kind[kind < kNumSweepKinds ? kind : 7]++;
     double amps = dim;
     if (s.kind == SK_CTRL) amps = std::ldexp(dim, -int(s.nctrl));
     if (s.kind == SK_DIAG) amps = std::ldexp(dim, -int(s.nctrl));
@@ -587,6 +614,7 @@ void sweep_costs(const std::vector<Sweep>& sw, uint32_t n, int dtype, qsvb_plan_
     st->full_sweep_bytes += 2.0 * dim * b;
     if (s.kind == SK_DENSE || s.kind == SK_DENSE_TC) st->flops += 8.0 * std::ldexp(1.0, int(s.m)) * dim;
     if (s.kind == SK_TILE) st->flops += s.tile_flops;
+    if (s.kind == SK_TC_CHAIN) st->flops += double(s.chain_nmat) * 8.0 * 64.0 * dim;
   }
   st->predicted_seconds = predict_plan_seconds(sw, n, dtype);
   st->measured_seconds = 0.0;

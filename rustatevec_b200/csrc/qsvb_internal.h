@@ -42,8 +42,13 @@ enum SweepKind : int {
   SK_DENSE = 4,     // dense 2^k x 2^k on CUDA cores
   SK_DENSE_TC = 5,  // dense 2^k x 2^k on tcgen05 tensor cores (complex64 only)
   SK_TILE = 6,      // gate program on shared-memory tiles of 2^L amplitudes (one read + one write)
-  SK_NONE = 7       // identity (dropped)
+  SK_NONE = 7,      // identity (dropped)
+  SK_TC_CHAIN = 8,  // up to three dense 6-qubit matrices on one resident 4096-amplitude tile
+                    // (tcgen05), written back with a permutation of the tile's qubits
+  SK_PERMUTE = 9    // a permutation of the qubits of 4096-amplitude tiles (no arithmetic)
 };
+constexpr int kNumSweepKinds = 10;
+constexpr int kChainMaxMats = 3;
 
 struct Gate {  // host copy of an input gate, FP64
   uint32_t m = 0;
@@ -75,6 +80,18 @@ struct Sweep {
   uint32_t tile_rb = 0, tile_lbits = 0, tile_ntiles = 0;
   uint32_t tile_off_phase = 0, tile_off_prog = 0, tile_off_coef = 0;
   double tile_flops = 0;
+  // chain / permutation passes: the tile's 12 state bits (ascending, bits 0..5 always among them;
+  // tile position i <-> state bit chain_tbits[i]); chain_nmat matrices (64 x 64, row-major), matrix j
+  // acting on tile positions chain_rows[j][0..5] (gate-index bit i <-> chain_rows[j][i]) with its
+  // 64 columns ordered by chain_cols[j][0..5]; after the last matrix the amplitude at tile position
+  // bit i moves to tile position bit chain_perm[i] (the pass relabels which qubit each of its
+  // state bits holds)
+  uint32_t chain_tbits[12] = {0};
+  uint32_t chain_nmat = 0;
+  uint8_t chain_rows[kChainMaxMats][6] = {};
+  uint8_t chain_cols[kChainMaxMats][6] = {};
+  uint8_t chain_perm[12] = {};
+  std::vector<std::vector<cd>> chain_mats;
 };
 
 std::vector<Gate> gates_from_circuit(const qsvb_circuit* c);
@@ -86,6 +103,12 @@ std::vector<Gate> fuse_gates(const std::vector<Gate>& in, uint32_t n_qubits, con
 std::vector<Sweep> plan_sweeps(const std::vector<Gate>& in, uint32_t n_qubits,
                                const qsvb_plan_opts& o, int dtype);
 Sweep classify_gate(const Gate& g);
+// The product of `ops` (applied in order) on the qubit list q (index bit j <-> q[j]), in FP64.
+Gate compose_gates(const std::vector<uint32_t>& q, const std::vector<const Gate*>& ops);
+uint64_t gate_mask(const Gate& g);
+// Tensor-core chain passes with qubit relabelling, then the permutation passes that restore every
+// qubit to its own state bit (chain_planner.cpp). max_mats: matrices per pass (1..3).
+std::vector<Sweep> plan_chain(const std::vector<Gate>& in, uint32_t n, uint32_t max_mats);
 void sweep_costs(const std::vector<Sweep>& sw, uint32_t n, int dtype, qsvb_plan_stats* st);
 qsvb_plan_opts default_opts();
 
@@ -136,6 +159,15 @@ size_t tc_matrix_bytes(const Sweep& s);
 void tc_pack_matrix(const Sweep& s, void* host_dst);
 void launch_tc_dense(const LaunchEnv& e, float* re, float* im, uint32_t n, const Sweep& s,
                      const void* dev_mat);
+
+// Chained tensor-core passes and tile permutations (complex64): implemented in tc_chain.cu.
+void tc_chain_prepare(Sweep& s);  // puts matrices 1.. in the row/column order their conversion needs
+size_t tc_chain_matrix_bytes(const Sweep& s);
+void tc_chain_check(const Sweep& s, uint32_t n);  // builds and validates the kernel tables (host only)
+void tc_chain_pack(const Sweep& s, void* host_dst);
+void launch_tc_chain(const LaunchEnv& e, float* re, float* im, uint32_t n, const Sweep& s, const void* dev_mat);
+template <class R>
+void launch_permute(const LaunchEnv& e, R* re, R* im, uint32_t n, const Sweep& s);
 
 }  // namespace qsvb
 

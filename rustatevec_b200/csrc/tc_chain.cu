@@ -1,0 +1,957 @@
+// Chained tensor-core pass (complex64): up to three dense 6-qubit matrices applied, one after the
+// other, to a 4096-amplitude tile that stays on the SM, then written back with a permutation of
+// the tile's qubits. One read and one write of the state replace one sweep per matrix.
+//
+// A tile is the 2^12 amplitudes that share every state bit outside the pass's 12 tile bits (state
+// bits 0..5 are always tile bits, so every global access is a contiguous run of >= 64 amplitudes).
+// Matrix j acts on six tile positions (its rows) and sees the other six as 64 columns; it runs as
+// the real GEMM [Yr; Yi] = W [Xr; Xi], W = [[Ur, -Ui], [Ui, Ur]] (128 x 128), with bf16 hi/lo
+// split operands and an FP32 accumulator in tensor memory (Wlo Xhi + Whi Xlo + Whi Xhi), exactly
+// as the single-matrix sweep (tc_dense.cu) does.
+//
+// One persistent CTA per SM, warp-specialised:
+//   producer warp: one tiled TMA or bulk copies per component of each tile into one of four fp32
+//     input slots (address order);
+//   converter warps (8): for a tile's first matrix, split the staged fp32 tile into the bf16 hi/lo
+//     B operand (one of two B buffers; layout chosen by which matrix qubits are state bits 0, 1);
+//     for every later matrix, read the previous matrix's accumulator straight from tensor memory
+//     (each warp its lane quadrant and half of the 64 columns), split it and scatter it into the
+//     next B operand (MN-major; each element's byte offset is an XOR of a per-row and a per-column
+//     part, both precomputed on the host);
+//   MMA warp (one lane): 24 tcgen05.mma per matrix into one of two accumulators (64 columns each),
+//     the A operand (Whi, Wlo of matrix j) resident in tensor memory for the whole kernel;
+//   epilogue warps (4): after the last matrix, read the accumulator, stage it in shared memory in
+//     the permuted address order (an XOR swizzle per pass makes both the scattered writes and the
+//     reads of the write-back bank-conflict free) and write the tile back with 16-byte stores.
+// Work items are (tile, matrix) pairs. Two tiles are in flight at a time, and every role walks the
+// same item order: matrix 0 of tiles a and b, matrix 1 of tiles a and b, ..., so the MMA of one
+// tile overlaps the conversion of the other. Every item depends only on earlier items, so the
+// pipeline cannot deadlock; every mbarrier wait is bounded (a wait that runs out sets the context
+// error flag, the role stops and the host reports QSVB_E_TIMEOUT). No load uses cluster multicast.
+//
+// k_permute_tiles applies only a tile-qubit permutation (no arithmetic): the planner uses it to put
+// every qubit back on its own state bit after a run of chain passes.
+
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <type_traits>
+#include <vector>
+
+#include "qsvb_internal.h"
+#include "tc_common.cuh"
+
+namespace qsvb {
+
+namespace {
+using namespace tc;
+
+constexpr int kTileAmps = 4096;
+constexpr int kCvtWarps = 8;
+constexpr int kEpiWarps = 4;
+constexpr int kCvtThreads = kCvtWarps * 32;
+constexpr int kEpiThreads = kEpiWarps * 32;
+constexpr int kProdWarp = kCvtWarps;       // warp 8
+constexpr int kMmaWarp = kCvtWarps + 1;    // warp 9
+constexpr int kEpiWarp0 = kCvtWarps + 2;   // warps 10..13
+constexpr int kThreads = (kCvtWarps + 2 + kEpiWarps) * 32;
+constexpr int kBSlots = 2;
+constexpr int kIoSlots = 4;
+constexpr int kWave = 2;                   // tiles in flight through the matrix stages
+constexpr int kTmemCols = 512;             // 2 accumulators (64 columns) + 3 x (Whi, Wlo) (64 each)
+constexpr uint32_t kTmemA0 = 128;          // matrix j: Whi at kTmemA0 + 128 j, Wlo 64 columns later
+constexpr uint32_t kBBytes = 128u * 64u * 2u;  // one of Xhi / Xlo: K = 128 rows x N = 64 bf16
+constexpr uint32_t kIoBytes = kTileAmps * 8u;
+constexpr int kVC = kTileAmps / 4 / kCvtThreads;   // float4 per component per converter thread
+constexpr int kVE = kTileAmps / 4 / kEpiThreads;   // float4 per component per epilogue thread
+constexpr size_t kChainSmem = 1024 + kBSlots * 2 * size_t(kBBytes) + (kIoSlots + 1) * size_t(kIoBytes) +
+                              20 * 8 + 8 + 64 * 8 + 64 * 2 * 2 + 64 * 2 + 128 * 2;
+static_assert(kChainSmem <= 232448, "chain pass: shared memory above the 227 KB per-block limit");
+static_assert(kChainMaxMats * 128 + 128 <= kTmemCols, "chain pass: tensor memory");
+
+struct ChainParams {
+  // tile addressing (tile_layout)
+  uint32_t hibits[6];
+  uint64_t hioff[64];
+  uint32_t runbits;
+  uint32_t tm_rank, tm_start[5], tm_len[5];
+  uint32_t nmat;
+  // first matrix, read from the staged tile in address order: (row << 6 | column) of each value
+  // of the low / high six tile positions, the converters' work order, and the B layout details
+  uint16_t dstlo[64], dsthi[64];
+  uint16_t tplo[32], tphi[32];
+  uint32_t b2_bit0, pair_shift;
+  // matrix j >= 1 read from the accumulator of matrix j - 1: byte offset in the B buffer of
+  // accumulator row r (r = part * 64 + gate row) and of column c; the element's offset is the XOR
+  uint16_t crow[kChainMaxMats][128];
+  uint16_t ccol[kChainMaxMats][64];
+  // last matrix: byte offset in the output staging of accumulator row r and of column c (XOR)
+  uint16_t frow[128];
+  uint16_t fcol[64];
+  // the staging swizzle read by the write-back: word index of address-order position t is
+  // sig_lo[t & 63] ^ sig_hi[t >> 6]
+  uint16_t sig_lo[64], sig_hi[64];
+};
+
+// B layout of the first matrix (as in tc_dense.cu): 0 MN-major (state bits 0, 1 are columns),
+// 1 K-major vectors (they are the matrix's rows 0, 1), 2 K-major row pairs (exactly one is a row,
+// the lowest), 3 K-major vectors assembled from a lane pair (bit 0 a column, bit 1 row 0, row 1 one
+// of state bits 2..4).
+template <int BM>
+__device__ __forceinline__ void convert_first(const float* __restrict__ sre, const float* __restrict__ sim,
+                                              uint8_t* __restrict__ b_hi, uint8_t* __restrict__ b_lo,
+                                              const uint16_t* __restrict__ s_dlo, const uint16_t* __restrict__ s_dhi,
+                                              const uint16_t* __restrict__ s_tperm, const ChainParams& p, int tid,
+                                              int lane) {
+  constexpr uint32_t M2 = 64, NCB = 6, CMASK = 63;
+  constexpr bool b_mn = BM == 0;
+  float4 xra[kVC], xia[kVC];
+  uint32_t dda[kVC];
+  int tt[kVC];
+#pragma unroll
+  for (int j = 0; j < kVC; ++j) {
+    const uint32_t u = uint32_t(tid + j * kCvtThreads);
+    const int t = int(uint32_t(s_tperm[u & 31u]) | uint32_t(s_tperm[32 + (u >> 5)])) * 4;
+    tt[j] = t;
+    xra[j] = *reinterpret_cast<const float4*>(sre + t);
+    xia[j] = *reinterpret_cast<const float4*>(sim + t);
+    dda[j] = uint32_t(s_dlo[t & 63]) + s_dhi[t >> 6];
+  }
+#pragma unroll
+  for (int j = 0; j < kVC; ++j) {
+    const int t = tt[j], tlo = t & 63, thi = t >> 6;
+    const float4 xr = xra[j], xi = xia[j];
+    const float vr[4] = {xr.x, xr.y, xr.z, xr.w};
+    const float vi[4] = {xi.x, xi.y, xi.z, xi.w};
+    if constexpr (BM == 3) {
+      const uint32_t sh = p.pair_shift;
+      const bool odd = ((uint32_t(lane) >> sh) & 1u) != 0;
+      const int pm = 1 << sh;
+      const float rr0 = __shfl_xor_sync(0xffffffffu, odd ? xr.x : xr.y, pm);
+      const float rr1 = __shfl_xor_sync(0xffffffffu, odd ? xr.z : xr.w, pm);
+      const float ri0 = __shfl_xor_sync(0xffffffffu, odd ? xi.x : xi.y, pm);
+      const float ri1 = __shfl_xor_sync(0xffffffffu, odd ? xi.z : xi.w, pm);
+      const float wr[4] = {odd ? rr0 : xr.x, odd ? rr1 : xr.z, odd ? xr.y : rr0, odd ? xr.w : rr1};
+      const float wi[4] = {odd ? ri0 : xi.x, odd ? ri1 : xi.z, odd ? xi.y : ri0, odd ? xi.w : ri1};
+      const int tg = (t & ~(4 << sh)) | (odd ? 1 : 0);
+      const uint32_t d = uint32_t(s_dlo[tg & 63]) + s_dhi[tg >> 6];
+      const uint32_t s = d >> NCB, c = d & CMASK;
+      const uint32_t o_re = kmaj_off(c, s, 64), o_im = kmaj_off(c, M2 + s, 64);
+      __nv_bfloat16 hr[4], lr[4], hm[4], lm[4];
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        split_bf16(wr[e], hr[e], lr[e]);
+        split_bf16(wi[e], hm[e], lm[e]);
+      }
+      *reinterpret_cast<uint2*>(b_hi + o_re) = pack4(hr);
+      *reinterpret_cast<uint2*>(b_lo + o_re) = pack4(lr);
+      *reinterpret_cast<uint2*>(b_hi + o_im) = pack4(hm);
+      *reinterpret_cast<uint2*>(b_lo + o_im) = pack4(lm);
+    } else if constexpr (BM == 2) {
+      const int step = p.b2_bit0 ? 1 : 2;
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        const int e = p.b2_bit0 ? 2 * q : q;
+        const uint32_t d = uint32_t(s_dlo[tlo + e]) + s_dhi[thi];
+        const uint32_t s = d >> NCB, c = d & CMASK;
+        const uint32_t o_re = kmaj_off(c, s, 64), o_im = kmaj_off(c, M2 + s, 64);
+        __nv_bfloat16 h0, l0, h1, l1;
+        split_bf16(vr[e], h0, l0);
+        split_bf16(vr[e + step], h1, l1);
+        *reinterpret_cast<uint32_t*>(b_hi + o_re) =
+            uint32_t(__bfloat16_as_ushort(h0)) | (uint32_t(__bfloat16_as_ushort(h1)) << 16);
+        *reinterpret_cast<uint32_t*>(b_lo + o_re) =
+            uint32_t(__bfloat16_as_ushort(l0)) | (uint32_t(__bfloat16_as_ushort(l1)) << 16);
+        split_bf16(vi[e], h0, l0);
+        split_bf16(vi[e + step], h1, l1);
+        *reinterpret_cast<uint32_t*>(b_hi + o_im) =
+            uint32_t(__bfloat16_as_ushort(h0)) | (uint32_t(__bfloat16_as_ushort(h1)) << 16);
+        *reinterpret_cast<uint32_t*>(b_lo + o_im) =
+            uint32_t(__bfloat16_as_ushort(l0)) | (uint32_t(__bfloat16_as_ushort(l1)) << 16);
+      }
+    } else {
+      const uint32_t d = dda[j];
+      const uint32_t s = d >> NCB, c = d & CMASK;
+      const uint32_t o_re = b_mn ? mnmaj_off(s, c) : kmaj_off(c, s, 64);
+      const uint32_t o_im = b_mn ? mnmaj_off(M2 + s, c) : kmaj_off(c, M2 + s, 64);
+      __nv_bfloat16 hr[4], lr[4], hm[4], lm[4];
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        split_bf16(vr[e], hr[e], lr[e]);
+        split_bf16(vi[e], hm[e], lm[e]);
+      }
+      *reinterpret_cast<uint2*>(b_hi + o_re) = pack4(hr);
+      *reinterpret_cast<uint2*>(b_lo + o_re) = pack4(lr);
+      *reinterpret_cast<uint2*>(b_hi + o_im) = pack4(hm);
+      *reinterpret_cast<uint2*>(b_lo + o_im) = pack4(lm);
+    }
+  }
+}
+
+// Matrix J >= 1: the accumulator of matrix J - 1 (this warp's 32 lanes, 32 of its 64 columns,
+// already in registers) split and scattered into the MN-major B operand of matrix J. The column
+// offsets are compile-time indices into the parameter bank.
+template <int J>
+__device__ __forceinline__ void convert_next(const uint32_t (&v)[32], uint32_t half, uint32_t rbase,
+                                             uint8_t* __restrict__ b_hi, uint8_t* __restrict__ b_lo,
+                                             const ChainParams& p) {
+  const uint32_t hoff = half ? uint32_t(p.ccol[J][32]) : 0u;  // column bit 5 (XOR-linear)
+#pragma unroll
+  for (int q = 0; q < 32; ++q) {
+    const uint32_t off = (rbase ^ hoff) ^ uint32_t(p.ccol[J][q]);
+    __nv_bfloat16 h, l;
+    split_bf16(__uint_as_float(v[q]), h, l);
+    *reinterpret_cast<__nv_bfloat16*>(b_hi + off) = h;
+    *reinterpret_cast<__nv_bfloat16*>(b_lo + off) = l;
+  }
+}
+
+template <int BM>
+__global__ void __launch_bounds__(kThreads, 1) k_tc_chain(float* __restrict__ re, float* __restrict__ im,
+                                                          uint64_t ntiles, const uint4* __restrict__ wpack,
+                                                          const __grid_constant__ ChainParams p, int* err,
+                                                          const __grid_constant__ CUtensorMap tm_re,
+                                                          const __grid_constant__ CUtensorMap tm_im) {
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint8_t* bbuf = smem;                                                    // slot s: hi, then lo
+  float* io = reinterpret_cast<float*>(bbuf + kBSlots * 2 * kBBytes);      // slot s: re [4096], im [4096]
+  float* ostage = io + kIoSlots * 2 * kTileAmps;                           // the epilogue's result
+  uint64_t* bars = reinterpret_cast<uint64_t*>(ostage + 2 * kTileAmps);
+  uint64_t* iofull = bars;        // [4] TMA complete_tx -> converters
+  uint64_t* ioempty = bars + 4;   // [4] converters -> producer
+  uint64_t* bfull = bars + 8;     // [2] converters -> MMA
+  uint64_t* bfree = bars + 10;    // [2] MMA commit -> converters
+  uint64_t* dfull = bars + 12;    // [2] MMA commit -> converters (matrices 0..nmat-2) / epilogue (last)
+  uint64_t* dfree = bars + 14;    // [2] accumulator read -> MMA
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 20);
+  uint64_t* s_hioff = reinterpret_cast<uint64_t*>(bars + 21);
+  uint16_t* s_dlo = reinterpret_cast<uint16_t*>(s_hioff + 64);
+  uint16_t* s_dhi = s_dlo + 64;
+  uint16_t* s_tperm = s_dhi + 64;   // tplo [32], tphi [32]
+  uint16_t* s_sig = s_tperm + 64;   // sig_lo [64], sig_hi [64]
+
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const uint32_t nmat = p.nmat;
+  for (int i = tid; i < 64; i += kThreads) {
+    s_hioff[i] = p.hioff[i];
+    s_dlo[i] = p.dstlo[i];
+    s_dhi[i] = p.dsthi[i];
+    s_sig[i] = p.sig_lo[i];
+    s_sig[64 + i] = p.sig_hi[i];
+  }
+  for (int i = tid; i < 32; i += kThreads) {
+    s_tperm[i] = p.tplo[i];
+    s_tperm[32 + i] = p.tphi[i];
+  }
+  if (warp == kMmaWarp) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(kTmemCols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (tid == 0) {
+    for (int s = 0; s < kIoSlots; ++s) {
+      mbar_init(&iofull[s], 1);
+      mbar_init(&ioempty[s], kCvtThreads);
+    }
+    for (int s = 0; s < 2; ++s) {
+      mbar_init(&bfull[s], kCvtThreads);
+      mbar_init(&bfree[s], 1);
+      mbar_init(&dfull[s], 1);
+      // every converter thread (count 1) or every epilogue thread (count 2) once it has read the
+      // accumulator
+      mbar_init(&dfree[s], kCvtThreads);
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;");
+  }
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tmem_slot;
+  if (warp >= kEpiWarp0) {
+    // A (Whi, Wlo of every matrix) into tensor memory: lane m holds row m, 64 32-bit columns of
+    // packed bf16 pairs (element 2j in the low half)
+    const uint32_t quad = uint32_t(warp & 3), m = quad * 32 + uint32_t(lane);
+    for (uint32_t j = 0; j < nmat; ++j)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        uint32_t r[64];
+        const uint4* src = wpack + ((size_t(j) * 2 + size_t(h)) * 128 + m) * 16;
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+          const uint4 u = src[q];
+          r[4 * q] = u.x;
+          r[4 * q + 1] = u.y;
+          r[4 * q + 2] = u.z;
+          r[4 * q + 3] = u.w;
+        }
+        tmem_st64(tmem + ((quad * 32) << 16) + kTmemA0 + 128u * j + 64u * uint32_t(h), r);
+      }
+    asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+
+  auto tile_base = [&](uint64_t tile) {
+    uint64_t base = tile << 6;
+#pragma unroll
+    for (int j = 0; j < 6; ++j) {
+      const uint32_t b = p.hibits[j];
+      const uint64_t lo = base & ((1ull << b) - 1ull);
+      base = ((base - lo) << 1) | lo;
+    }
+    return base;
+  };
+  const uint64_t my_tiles = uint64_t(blockIdx.x) < ntiles ? (ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+
+  if (warp == kProdWarp) {
+    // ============================ producer: the tile's runs into an input slot (address order)
+    const uint32_t rb = p.runbits, nruns = uint32_t(kTileAmps) >> rb, run_bytes = 4u << rb;
+    for (uint64_t i = 0; i < my_tiles; ++i) {
+      const uint32_t slot = uint32_t(i % kIoSlots), par = uint32_t((i / kIoSlots) & 1);
+      bool ok = true;
+      if (lane == 0) {
+        ok = mbar_wait(&ioempty[slot], par ^ 1u);
+        if (ok) mbar_arrive_expect_tx(&iofull[slot], kIoBytes);
+        else atomicExch(err, 1);
+      }
+      ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
+      if (!ok) break;
+      const uint64_t base = tile_base(blockIdx.x + i * gridDim.x);
+      float* dre = io + slot * 2 * kTileAmps;
+      float* dim_ = dre + kTileAmps;
+      if (p.tm_rank > 0) {
+        if (lane == 0) {
+          int c[5];
+#pragma unroll
+          for (uint32_t d = 0; d < 5; ++d)
+            c[d] = d < p.tm_rank ? int((base >> p.tm_start[d]) & ((1ull << p.tm_len[d]) - 1ull)) : 0;
+          tma_tensor_g2s(dre, &tm_re, c, p.tm_rank, &iofull[slot]);
+          tma_tensor_g2s(dim_, &tm_im, c, p.tm_rank, &iofull[slot]);
+        }
+        continue;
+      }
+      for (uint32_t j = lane; j < nruns; j += 32) {
+        const uint32_t t0 = j << rb;
+        const uint64_t a = base + s_hioff[t0 >> 6];
+        bulk_g2s(dre + t0, re + a, run_bytes, &iofull[slot]);
+        bulk_g2s(dim_ + t0, im + a, run_bytes, &iofull[slot]);
+      }
+    }
+  } else if (warp < kCvtWarps) {
+    // ============================ converters: B operand of every (tile, matrix) item
+    const uint32_t quad = uint32_t(warp & 3), half = uint32_t(warp >> 2);
+    const uint32_t row = quad * 32 + uint32_t(lane);  // accumulator row this thread reads
+    uint32_t rb1 = 0, rb2 = 0;                        // its byte offsets in the B of matrices 1 and 2
+    if (nmat > 1) rb1 = p.crow[1][row];
+    if (nmat > 2) rb2 = p.crow[2][row];
+    uint32_t g = 0;
+    bool stop = false;
+    for (uint64_t w0 = 0; w0 < my_tiles && !stop; w0 += kWave) {
+      const uint32_t nt = my_tiles - w0 < uint64_t(kWave) ? uint32_t(my_tiles - w0) : uint32_t(kWave);
+      for (uint32_t j = 0; j < nmat && !stop; ++j)
+        for (uint32_t tt = 0; tt < nt; ++tt, ++g) {
+          const uint64_t i = w0 + tt;
+          const uint32_t slot = uint32_t(i % kIoSlots);
+          const uint32_t bs = g & 1u, bpar = (g >> 1) & 1u;
+          // the input: the staged tile (matrix 0) or the accumulator of this tile's previous
+          // matrix, which the MMA wrote for item g - nt
+          const uint32_t src = g - nt, ds = src & 1u, dpar = (src >> 1) & 1u;
+          bool ready = j == 0 ? mbar_wait(&iofull[slot], uint32_t((i / kIoSlots) & 1))
+                              : mbar_wait(&dfull[ds], dpar);
+          ready = ready && mbar_wait(&bfree[bs], bpar ^ 1u);
+          if (!__all_sync(0xffffffffu, ready)) {
+            atomicExch(err, 1);
+            stop = true;
+            break;
+          }
+          uint8_t* b_hi = bbuf + bs * 2 * kBBytes;
+          uint8_t* b_lo = b_hi + kBBytes;
+          if (j == 0) {
+            const float* sre = io + slot * 2 * kTileAmps;
+            convert_first<BM>(sre, sre + kTileAmps, b_hi, b_lo, s_dlo, s_dhi, s_tperm, p, tid, lane);
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            mbar_arrive(&bfull[bs]);
+            mbar_arrive(&ioempty[slot]);  // the staged tile has been read
+          } else {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            uint32_t v[32];
+            const uint32_t taddr = tmem + ((quad * 32) << 16) + ds * 64u + half * 32u;
+            uint32_t (&v0)[16] = *reinterpret_cast<uint32_t(*)[16]>(&v[0]);
+            uint32_t (&v1)[16] = *reinterpret_cast<uint32_t(*)[16]>(&v[16]);
+            tmem_ld16(taddr, v0);
+            tmem_ld16(taddr + 16u, v1);
+            asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            mbar_arrive(&dfree[ds]);  // this thread's part of the accumulator is in registers
+            if (j == 1) convert_next<1>(v, half, rb1, b_hi, b_lo, p);
+            else convert_next<2>(v, half, rb2, b_hi, b_lo, p);
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            mbar_arrive(&bfull[bs]);
+          }
+        }
+    }
+  } else if (warp == kMmaWarp) {
+    // ============================ MMA issue: one lane
+    if (lane == 0) {
+      // idesc: f32 accumulate, bf16 A and B, K-major A; B MN-major (bit 16) for every matrix but
+      // a K-major first one; N = 64, M = 128
+      const uint32_t idesc_k =
+          (1u << 4) | (1u << 7) | (1u << 10) | (uint32_t(64 >> 3) << 17) | (uint32_t(128 >> 4) << 24);
+      const uint32_t idesc_mn = idesc_k | (1u << 16);
+      uint32_t g = 0;
+      bool stop = false;
+      for (uint64_t w0 = 0; w0 < my_tiles && !stop; w0 += kWave) {
+        const uint32_t nt = my_tiles - w0 < uint64_t(kWave) ? uint32_t(my_tiles - w0) : uint32_t(kWave);
+        for (uint32_t j = 0; j < nmat && !stop; ++j)
+          for (uint32_t tt = 0; tt < nt; ++tt, ++g) {
+            const uint32_t bs = g & 1u, par = (g >> 1) & 1u;
+            if (!mbar_wait(&bfull[bs], par) || !mbar_wait(&dfree[bs], par ^ 1u)) {
+              atomicExch(err, 1);
+              stop = true;
+              break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const bool mn = j > 0 || BM == 0;
+            const uint32_t idesc = mn ? idesc_mn : idesc_k;
+            const uint32_t b_lbo = mn ? 128u * 128u : 16u;
+            const uint32_t b_hi_s = smem_u32(bbuf + bs * 2 * kBBytes), b_lo_s = b_hi_s + kBBytes;
+            const uint32_t d_tmem = tmem + bs * 64u;
+            const uint32_t a_hi = tmem + kTmemA0 + 128u * j, a_lo = a_hi + 64u;
+#pragma unroll 1
+            for (int s = 0; s < 8; ++s) {
+              const uint32_t bk = mn ? uint32_t(s) * 2048u : (s >> 2) * (64u * 128u) + (s & 3) * 32u;
+              const uint64_t dbh = sw128_desc(b_hi_s + bk, b_lbo, 1024u), dbl = sw128_desc(b_lo_s + bk, b_lbo, 1024u);
+              mma_bf16_ts(d_tmem, a_lo + uint32_t(s) * 8u, dbh, idesc, s > 0 ? 1u : 0u);
+              mma_bf16_ts(d_tmem, a_hi + uint32_t(s) * 8u, dbl, idesc, 1u);
+              mma_bf16_ts(d_tmem, a_hi + uint32_t(s) * 8u, dbh, idesc, 1u);
+            }
+            mma_commit(&bfree[bs]);  // B buffer consumed
+            mma_commit(&dfull[bs]);  // accumulator ready
+          }
+      }
+    }
+    __syncwarp();
+  } else {
+    // ============================ epilogue: last matrix's accumulator -> staging -> global
+    const int quad = warp & 3;
+    const int et = tid - kEpiWarp0 * 32;
+    const uint32_t row = uint32_t(quad * 32 + lane);
+    const uint32_t frow = p.frow[row];
+    uint32_t g = 0;
+    bool stop = false;
+    for (uint64_t w0 = 0; w0 < my_tiles && !stop; w0 += kWave) {
+      const uint32_t nt = my_tiles - w0 < uint64_t(kWave) ? uint32_t(my_tiles - w0) : uint32_t(kWave);
+      g += (nmat - 1) * nt;  // items of the earlier matrices belong to the converters
+      for (uint32_t tt = 0; tt < nt; ++tt, ++g) {
+        const uint32_t ds = g & 1u, dpar = (g >> 1) & 1u;
+        const bool ready = mbar_wait(&dfull[ds], dpar);
+        // one decision for all epilogue threads; reaching this barrier also means every thread's
+        // reads of the previous tile's staging are done
+        if (!named_all(2, kEpiThreads, ready)) {
+          atomicExch(err, 1);
+          stop = true;
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        uint32_t v[4][16];
+        const uint32_t taddr = tmem + (uint32_t(quad * 32) << 16) + ds * 64u;
+#pragma unroll
+        for (int cb = 0; cb < 4; ++cb) tmem_ld16(taddr + uint32_t(cb * 16), v[cb]);
+        asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        mbar_arrive_cnt(&dfree[ds], 2);  // 128 epilogue threads stand for the 256 converter arrivals
+        char* st = reinterpret_cast<char*>(ostage);
+#pragma unroll
+        for (int cb = 0; cb < 4; ++cb)
+#pragma unroll
+          for (int q = 0; q < 16; ++q)
+            *reinterpret_cast<float*>(st + (frow ^ uint32_t(p.fcol[cb * 16 + q]))) = __uint_as_float(v[cb][q]);
+        named_sync(1, kEpiThreads);  // the whole result is staged
+        const uint64_t base = tile_base(blockIdx.x + (w0 + tt) * gridDim.x);
+        const uint32_t s1 = p.sig_lo[1], s2 = p.sig_lo[2], s3 = p.sig_lo[3];
+#pragma unroll
+        for (int j = 0; j < kVE; ++j) {
+          const int t = (et + j * kEpiThreads) * 4, tlo = t & 63, thi = t >> 6;
+          const uint64_t a = base + s_hioff[thi] + uint64_t(tlo);
+          const uint32_t w = uint32_t(s_sig[tlo]) ^ s_sig[64 + thi];
+          float4 xr, xi;
+          xr.x = ostage[w];
+          xr.y = ostage[w ^ s1];
+          xr.z = ostage[w ^ s2];
+          xr.w = ostage[w ^ s3];
+          xi.x = ostage[kTileAmps + w];
+          xi.y = ostage[kTileAmps + (w ^ s1)];
+          xi.z = ostage[kTileAmps + (w ^ s2)];
+          xi.w = ostage[kTileAmps + (w ^ s3)];
+          __stcs(reinterpret_cast<float4*>(re + a), xr);
+          __stcs(reinterpret_cast<float4*>(im + a), xi);
+        }
+      }
+    }
+  }
+  __syncwarp();  // roles may leave their loops at different iterations after a timeout
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == kMmaWarp) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols));
+  }
+}
+
+// ---------------------------------------------------------------- tile permutation (no arithmetic)
+constexpr int kPermThreads = 256;
+
+struct PermParams {
+  uint32_t hibits[6];
+  uint64_t hioff[64];
+  uint16_t plo[64], phi[64];  // destination tile position of each value of the low / high six bits
+};
+
+// Each block moves its tiles through shared memory: 16-byte loads of the tile in address order,
+// scalar stores at the permuted positions, 16-byte stores back to the same tile's addresses (the
+// set of addresses a tile covers is closed under its permutation, so the update is in place).
+template <class R>
+__global__ void __launch_bounds__(kPermThreads) k_permute_tiles(R* __restrict__ re, R* __restrict__ im, uint64_t ntiles,
+                                                                const __grid_constant__ PermParams p) {
+  using V = typename std::conditional<sizeof(R) == 4, float4, double2>::type;
+  constexpr int VN = 16 / sizeof(R);  // amplitudes per 16-byte vector
+  extern __shared__ __align__(16) uint8_t smem_raw[];
+  R* sre = reinterpret_cast<R*>(smem_raw);
+  R* sim = sre + kTileAmps;
+  __shared__ uint64_t s_hioff[64];
+  __shared__ uint16_t s_plo[64], s_phi[64];
+  for (int i = threadIdx.x; i < 64; i += kPermThreads) {
+    s_hioff[i] = p.hioff[i];
+    s_plo[i] = p.plo[i];
+    s_phi[i] = p.phi[i];
+  }
+  __syncthreads();
+  for (uint64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    uint64_t base = tile << 6;
+#pragma unroll
+    for (int j = 0; j < 6; ++j) {
+      const uint32_t b = p.hibits[j];
+      const uint64_t lo = base & ((1ull << b) - 1ull);
+      base = ((base - lo) << 1) | lo;
+    }
+    for (int u = threadIdx.x; u < kTileAmps / VN; u += kPermThreads) {
+      const int t = u * VN, tlo = t & 63, thi = t >> 6;
+      const uint64_t a = base + s_hioff[thi] + uint64_t(tlo);
+      const V xr = *reinterpret_cast<const V*>(re + a);
+      const V xi = *reinterpret_cast<const V*>(im + a);
+      const R* vr = reinterpret_cast<const R*>(&xr);
+      const R* vi = reinterpret_cast<const R*>(&xi);
+      const uint32_t dhi = s_phi[thi];
+#pragma unroll
+      for (int e = 0; e < VN; ++e) {
+        const uint32_t d = dhi ^ s_plo[tlo + e];
+        sre[d] = vr[e];
+        sim[d] = vi[e];
+      }
+    }
+    __syncthreads();
+    for (int u = threadIdx.x; u < kTileAmps / VN; u += kPermThreads) {
+      const int t = u * VN, tlo = t & 63, thi = t >> 6;
+      const uint64_t a = base + s_hioff[thi] + uint64_t(tlo);
+      *reinterpret_cast<V*>(re + a) = *reinterpret_cast<const V*>(sre + t);
+      *reinterpret_cast<V*>(im + a) = *reinterpret_cast<const V*>(sim + t);
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------- host-side tables
+uint32_t deposit6(uint32_t v, const uint8_t (&pos)[6]) {
+  uint32_t t = 0;
+  for (int i = 0; i < 6; ++i)
+    if ((v >> i) & 1u) t |= 1u << pos[i];
+  return t;
+}
+uint32_t gather6(uint32_t t, const uint8_t (&pos)[6]) {
+  uint32_t v = 0;
+  for (int i = 0; i < 6; ++i) v |= ((t >> pos[i]) & 1u) << i;
+  return v;
+}
+uint32_t permute12(uint32_t t, const uint8_t (&perm)[12]) {
+  uint32_t o = 0;
+  for (int i = 0; i < 12; ++i)
+    if ((t >> i) & 1u) o |= 1u << perm[i];
+  return o;
+}
+int rank5(std::vector<uint32_t> v) {  // GF(2) rank of 5-bit vectors
+  int r = 0;
+  for (int bit = 4; bit >= 0; --bit) {
+    size_t piv = v.size();
+    for (size_t i = size_t(r); i < v.size(); ++i)
+      if ((v[i] >> bit) & 1u) {
+        piv = i;
+        break;
+      }
+    if (piv == v.size()) continue;
+    std::swap(v[size_t(r)], v[piv]);
+    for (size_t i = 0; i < v.size(); ++i)
+      if (i != size_t(r) && ((v[i] >> bit) & 1u)) v[i] ^= v[size_t(r)];
+    ++r;
+  }
+  return r;
+}
+
+// The output staging swizzle: word index of position t = t ^ A(t >> 5), A a 7 -> 5 bit GF(2) map
+// (bits 5..11 stay, so it is a bijection), chosen so that the epilogue's 32 lanes (positions
+// lane_pos[0..4] for lane bits 0..4) and the write-back's 32 lanes (position bits 2..6) each hit
+// 32 distinct banks. Deterministic search; A = 0 (correct, with bank conflicts) if none is found.
+void staging_swizzle(const uint32_t (&lane_pos)[5], uint16_t (&sig_lo)[64], uint16_t (&sig_hi)[64]) {
+  uint32_t A[7] = {0, 0, 0, 0, 0, 0, 0};
+  auto bank_of_bit = [&](uint32_t pos, const uint32_t (&a)[7]) { return pos < 5 ? (1u << pos) : a[pos - 5]; };
+  uint64_t rng = 0x9E3779B97F4A7C15ull;
+  for (int attempt = 0; attempt < 20000; ++attempt) {
+    uint32_t a[7];
+    for (int i = 0; i < 7; ++i) {
+      rng ^= rng << 13;
+      rng ^= rng >> 7;
+      rng ^= rng << 17;
+      a[i] = uint32_t(rng) & 31u;
+    }
+    if (attempt == 0) std::fill(a, a + 7, 0u);
+    std::vector<uint32_t> w = {bank_of_bit(2, a), bank_of_bit(3, a), bank_of_bit(4, a), bank_of_bit(5, a),
+                               bank_of_bit(6, a)};
+    std::vector<uint32_t> e;
+    for (uint32_t b : lane_pos) e.push_back(bank_of_bit(b, a));
+    if (rank5(w) == 5 && rank5(e) == 5) {
+      std::copy(a, a + 7, A);
+      break;
+    }
+  }
+  auto sig = [&](uint32_t t) {
+    uint32_t w = t;
+    for (int i = 0; i < 7; ++i)
+      if ((t >> (5 + i)) & 1u) w ^= A[i];
+    return w;
+  };
+  for (uint32_t i = 0; i < 64; ++i) {
+    sig_lo[i] = uint16_t(sig(i));
+    sig_hi[i] = uint16_t(sig(i << 6));
+  }
+}
+
+// Row and column orders of matrix j >= 1 (both internal to the pass) chosen so that the scattered
+// B stores of its conversion are bank-conflict free: the converter lanes carry matrix j-1's gate
+// rows 0..4; those that are rows of matrix j take row slots 0..2 (byte bits 7..9, swizzled into
+// bank bits), those that are its columns take column bits 0..2 first (one of them shares a 4-byte
+// word with its neighbour), then the column bits whose swizzle partner row bit is unused.
+void order_for_conversion(const uint8_t (&prev_rows)[6], uint64_t rows_set, uint8_t (&rows)[6], uint8_t (&cols)[6]) {
+  std::vector<uint8_t> lane_rows, lane_cols;
+  for (int b = 0; b < 5; ++b) {
+    if ((rows_set >> prev_rows[b]) & 1u) lane_rows.push_back(prev_rows[b]);
+    else lane_cols.push_back(prev_rows[b]);
+  }
+  int ri = 0;
+  bool row_used[6] = {false}, col_used[6] = {false};
+  uint8_t r_out[6], c_out[6];
+  for (uint8_t p : lane_rows) {
+    r_out[ri] = p;
+    row_used[ri] = true;
+    ++ri;
+  }
+  // column slots in preference order: 0, 1, 2, then 3 + k for row slots k that are unused
+  std::vector<int> cslots = {0, 1, 2};
+  for (int k = 0; k < 3; ++k)
+    if (k >= ri) cslots.push_back(3 + k);
+  for (int k = 0; k < 3; ++k)
+    if (k < ri) cslots.push_back(3 + k);
+  size_t ci = 0;
+  for (uint8_t p : lane_cols) {
+    c_out[cslots[ci]] = p;
+    col_used[cslots[ci]] = true;
+    ++ci;
+  }
+  // the remaining rows and columns in ascending tile position
+  std::vector<uint8_t> rest_rows, rest_cols;
+  for (int t = 0; t < 12; ++t) {
+    const bool in_lane = std::find(prev_rows, prev_rows + 5, uint8_t(t)) != prev_rows + 5;
+    if (in_lane) continue;
+    if ((rows_set >> t) & 1u) rest_rows.push_back(uint8_t(t));
+    else rest_cols.push_back(uint8_t(t));
+  }
+  size_t k = 0;
+  for (int i = 0; i < 6; ++i)
+    if (!row_used[i]) r_out[i] = rest_rows[k++];
+  k = 0;
+  for (int i = 0; i < 6; ++i)
+    if (!col_used[i]) c_out[i] = rest_cols[k++];
+  std::copy(r_out, r_out + 6, rows);
+  std::copy(c_out, c_out + 6, cols);
+}
+
+// Every table entry the kernel indexes shared memory with stays inside its buffer and maps its
+// domain one to one (a violated check is a planner or table bug, reported before any launch).
+void check_chain_params(const ChainParams& p, uint32_t nm) {
+  std::vector<char> seen(size_t(1) << 15);
+  auto reset = [&] { std::fill(seen.begin(), seen.end(), 0); };
+  reset();
+  for (uint32_t h = 0; h < 64; ++h)
+    for (uint32_t l = 0; l < 64; ++l) {
+      const uint32_t d = uint32_t(p.dstlo[l]) ^ p.dsthi[h];
+      QSVB_REQUIRE(d < 4096 && !seen[d], "chain pass: first-matrix index table is not a bijection");
+      seen[d] = 1;
+    }
+  for (uint32_t j = 1; j < nm; ++j) {
+    reset();
+    for (uint32_t r = 0; r < 128; ++r)
+      for (uint32_t c = 0; c < 64; ++c) {
+        const uint32_t o = uint32_t(p.crow[j][r]) ^ p.ccol[j][c];
+        QSVB_REQUIRE(o < kBBytes && (o & 1u) == 0 && !seen[o], "chain pass: operand scatter table out of range");
+        seen[o] = 1;
+      }
+  }
+  reset();
+  for (uint32_t r = 0; r < 128; ++r)
+    for (uint32_t c = 0; c < 64; ++c) {
+      const uint32_t o = uint32_t(p.frow[r]) ^ p.fcol[c];
+      QSVB_REQUIRE(o < 2u * kTileAmps * 4u && (o & 3u) == 0 && !seen[o >> 2],
+                   "chain pass: output staging table out of range");
+      seen[o >> 2] = 1;
+    }
+  reset();
+  for (uint32_t h = 0; h < 64; ++h)
+    for (uint32_t l = 0; l < 64; ++l) {
+      const uint32_t w = uint32_t(p.sig_lo[l]) ^ p.sig_hi[h];
+      QSVB_REQUIRE(w < 4096 && !seen[w], "chain pass: staging swizzle is not a bijection");
+      seen[w] = 1;
+    }
+  reset();
+  for (uint32_t u = 0; u < 1024; ++u) {
+    const uint32_t t4 = uint32_t(p.tplo[u & 31u]) | p.tphi[u >> 5];
+    QSVB_REQUIRE(t4 < 1024 && !seen[t4], "chain pass: converter work order is not a permutation");
+    seen[t4] = 1;
+  }
+}
+
+// The kernel's parameter tables for one chain pass (tile addressing, operand scatter offsets,
+// output staging), checked to stay inside their buffers; returns the first matrix's B layout mode.
+uint32_t build_chain_params(const Sweep& s, uint32_t n, float* re, float* im, ChainParams& p, TileLayout& lay) {
+  QSVB_REQUIRE(n >= 12, "chain pass: state too small");
+  QSVB_REQUIRE(s.chain_nmat >= 1 && s.chain_nmat <= uint32_t(kChainMaxMats), "chain pass: 1..3 matrices");
+  const uint32_t nm = s.chain_nmat;
+  std::memset(&p, 0, sizeof(p));
+  p.nmat = nm;
+  tile_layout(n, s.chain_tbits, re, im, lay);
+  std::copy(lay.hibits, lay.hibits + 6, p.hibits);
+  std::copy(lay.hioff, lay.hioff + 64, p.hioff);
+  p.runbits = lay.runbits;
+  p.tm_rank = lay.tm_rank;
+  std::copy(lay.tm_start, lay.tm_start + 5, p.tm_start);
+  std::copy(lay.tm_len, lay.tm_len + 5, p.tm_len);
+  // matrix orders (tc_chain_prepare has put matrices 1.. in their conversion order)
+  uint8_t rows[kChainMaxMats][6], cols[kChainMaxMats][6];
+  for (uint32_t j = 0; j < nm; ++j) {
+    std::copy(s.chain_rows[j], s.chain_rows[j] + 6, rows[j]);
+    std::copy(s.chain_cols[j], s.chain_cols[j] + 6, cols[j]);
+    uint32_t all = 0;
+    for (int i = 0; i < 6; ++i) all |= (1u << rows[j][i]) | (1u << cols[j][i]);
+    QSVB_REQUIRE(all == 0xFFFu, "chain pass: rows and columns must cover the 12 tile positions");
+  }
+  // first matrix, read in address order
+  auto d_of = [&](uint32_t j, uint32_t t) { return (gather6(t, rows[j]) << 6) | gather6(t, cols[j]); };
+  for (uint32_t l = 0; l < 64; ++l) {
+    p.dstlo[l] = uint16_t(d_of(0, l));
+    p.dsthi[l] = uint16_t(d_of(0, l << 6));
+  }
+  int rank0[12];
+  for (int t = 0; t < 12; ++t) rank0[t] = -1;
+  for (int i = 0; i < 6; ++i) rank0[rows[0][i]] = i;
+  bool cols_ascending = true, rows_ascending = true;
+  for (int i = 1; i < 6; ++i) {
+    cols_ascending = cols_ascending && cols[0][i] > cols[0][i - 1];
+    rows_ascending = rows_ascending && rows[0][i] > rows[0][i - 1];
+  }
+  QSVB_REQUIRE(cols_ascending && rows_ascending, "chain pass: the first matrix's rows and columns must ascend");
+  const bool low_cols = rank0[0] < 0 && rank0[1] < 0;
+  const bool low_rows = rank0[0] == 0 && rank0[1] == 1;
+  int row1_pos = -1;
+  for (int t = 0; t < 12; ++t)
+    if (rank0[t] == 1) row1_pos = t;
+  const bool lane_pair = rank0[0] < 0 && rank0[1] == 0 && row1_pos >= 2 && row1_pos <= 4;
+  const uint32_t bmode = low_cols ? 0u : (low_rows ? 1u : (lane_pair ? 3u : 2u));
+  p.b2_bit0 = rank0[0] == 0 ? 1u : 0u;
+  p.pair_shift = lane_pair ? uint32_t(row1_pos - 2) : 0u;
+  {
+    // converter work order (as in tc_dense.cu): float4 index bits 0..2 stay; for K-major layouts the
+    // lane bits 3 and 4 take the two float4 bits that spread the warp's B stores over most banks
+    auto perm_t4 = [](uint32_t u, const int (&pi)[10]) {
+      uint32_t t4 = 0;
+      for (int i = 0; i < 10; ++i)
+        if ((u >> i) & 1u) t4 |= 1u << pi[i];
+      return t4;
+    };
+    auto conflict = [&](const int (&pi)[10]) {
+      int worst = 0;
+      const int nst = bmode == 2 ? 2 : 1;
+      for (int q = 0; q < nst; ++q) {
+        int count[32] = {0};
+        for (uint32_t ln = 0; ln < 32; ++ln) {
+          const uint32_t t = perm_t4(ln, pi) * 4u;
+          const uint32_t e = bmode == 2 ? (p.b2_bit0 ? 2u * q : uint32_t(q)) : 0u;
+          uint32_t tl = t + e;
+          if (bmode == 3) tl = (t & ~(4u << p.pair_shift)) | ((ln >> p.pair_shift) & 1u);
+          const uint32_t d = uint32_t(p.dstlo[tl & 63u]) + p.dsthi[tl >> 6];
+          const uint32_t off = kmaj_off(d & 63u, d >> 6, 64);
+          const uint32_t bank = bmode == 2 ? (off >> 2) & 31u : ((off >> 3) & 15u) + 16u * (ln >> 4);
+          worst = std::max(worst, ++count[bank]);
+        }
+      }
+      return worst;
+    };
+    int best[10];
+    for (int i = 0; i < 10; ++i) best[i] = i;
+    if (bmode != 0) {
+      int best_c = conflict(best);
+      for (int a = 3; a < 10; ++a)
+        for (int b = 3; b < 10; ++b) {
+          if (a == b) continue;
+          int pi[10] = {0, 1, 2, a, b, 0, 0, 0, 0, 0};
+          int nxt = 5;
+          for (int v = 3; v < 10; ++v)
+            if (v != a && v != b) pi[nxt++] = v;
+          const int cc = conflict(pi);
+          if (cc < best_c) {
+            best_c = cc;
+            std::copy(pi, pi + 10, best);
+          }
+        }
+    }
+    for (uint32_t u = 0; u < 32; ++u) {
+      p.tplo[u] = uint16_t(perm_t4(u, best));
+      p.tphi[u] = uint16_t(perm_t4(u << 5, best));
+    }
+  }
+  // later matrices: B byte offset of accumulator element (row r = part * 64 + gate row, column c)
+  // of matrix j - 1 = crow[j][r] ^ ccol[j][c] (the MN-major layout is XOR-linear in its bits)
+  auto pos_of = [&](uint32_t j, uint32_t srow, uint32_t col) { return deposit6(srow, rows[j]) | deposit6(col, cols[j]); };
+  for (uint32_t j = 1; j < nm; ++j) {
+    for (uint32_t r = 0; r < 128; ++r) {
+      const uint32_t d = d_of(j, pos_of(j - 1, r & 63u, 0));
+      p.crow[j][r] = uint16_t(mnmaj_off((r >> 6) * 64u + (d >> 6), d & 63u));
+    }
+    for (uint32_t c = 0; c < 64; ++c) {
+      const uint32_t d = d_of(j, pos_of(j - 1, 0, c));
+      p.ccol[j][c] = uint16_t(mnmaj_off(d >> 6, d & 63u));
+    }
+  }
+  // last matrix -> output staging at the permuted position, swizzled
+  uint32_t lane_pos[5];
+  for (int b = 0; b < 5; ++b)
+    lane_pos[b] = uint32_t(__builtin_ctz(permute12(1u << rows[nm - 1][b], s.chain_perm)));
+  staging_swizzle(lane_pos, p.sig_lo, p.sig_hi);
+  auto sig = [&](uint32_t t) { return uint32_t(p.sig_lo[t & 63u]) ^ p.sig_hi[t >> 6]; };
+  for (uint32_t r = 0; r < 128; ++r)
+    p.frow[r] =
+        uint16_t((r >> 6) * uint32_t(kTileAmps) * 4u + 4u * sig(permute12(pos_of(nm - 1, r & 63u, 0), s.chain_perm)));
+  for (uint32_t c = 0; c < 64; ++c) p.fcol[c] = uint16_t(4u * sig(permute12(pos_of(nm - 1, 0, c), s.chain_perm)));
+  check_chain_params(p, nm);
+  return bmode;
+}
+
+}  // namespace
+
+void tc_chain_prepare(Sweep& s) {
+  QSVB_REQUIRE(s.chain_nmat >= 1 && s.chain_nmat <= uint32_t(kChainMaxMats), "chain pass: 1..3 matrices");
+  for (uint32_t j = 0; j < s.chain_nmat; ++j)
+    QSVB_REQUIRE(s.chain_mats[j].size() == 64 * 64, "chain pass: matrices are 64 x 64");
+  for (uint32_t j = 1; j < s.chain_nmat; ++j) {
+    uint64_t rset = 0;
+    for (int i = 0; i < 6; ++i) rset |= 1ull << s.chain_rows[j][i];
+    uint8_t nr[6], nc[6];
+    order_for_conversion(s.chain_rows[j - 1], rset, nr, nc);
+    // the matrix in the new row order: index bit i now means tile position nr[i]
+    int from[6];
+    for (int i = 0; i < 6; ++i) from[i] = int(std::find(s.chain_rows[j], s.chain_rows[j] + 6, nr[i]) - s.chain_rows[j]);
+    const std::vector<cd>& m = s.chain_mats[j];
+    std::vector<cd> m2(64 * 64);
+    for (uint32_t r = 0; r < 64; ++r)
+      for (uint32_t c = 0; c < 64; ++c) {
+        uint32_t ro = 0, co = 0;
+        for (int i = 0; i < 6; ++i) {
+          ro |= ((r >> i) & 1u) << from[i];
+          co |= ((c >> i) & 1u) << from[i];
+        }
+        m2[size_t(r) * 64 + c] = m[size_t(ro) * 64 + co];
+      }
+    s.chain_mats[j] = std::move(m2);
+    std::copy(nr, nr + 6, s.chain_rows[j]);
+    std::copy(nc, nc + 6, s.chain_cols[j]);
+  }
+}
+
+size_t tc_chain_matrix_bytes(const Sweep& s) { return size_t(s.chain_nmat) * 2 * 128 * 128 * 2; }
+
+// Per matrix: A = [[Ur, -Ui], [Ui, Ur]] (128 x 128), split into bf16 hi/lo, in the tensor-memory
+// image order of tc_pack_matrix (hi then lo, each 128 rows x 64 words of bf16 pairs).
+void tc_chain_pack(const Sweep& s, void* dst) {
+  for (uint32_t j = 0; j < s.chain_nmat; ++j) {
+    Sweep one;
+    one.kind = SK_DENSE_TC;
+    one.m = 6;
+    one.mat = s.chain_mats[j];
+    tc_pack_matrix(one, static_cast<char*>(dst) + size_t(j) * 2 * 128 * 128 * 2);
+  }
+}
+
+void tc_chain_check(const Sweep& s, uint32_t n) {
+  ChainParams p;
+  TileLayout lay;
+  (void)build_chain_params(s, n, nullptr, nullptr, p, lay);
+}
+
+void launch_tc_chain(const LaunchEnv& env, float* re, float* im, uint32_t n, const Sweep& s, const void* dev_mat) {
+  QSVB_REQUIRE(env.err_flag != nullptr, "chain pass needs the context error flag");
+  ChainParams p;
+  TileLayout lay;
+  const uint32_t bmode = build_chain_params(s, n, re, im, p, lay);
+  const uint64_t ntiles = 1ull << (n - 12);
+  auto kern = bmode == 0 ? k_tc_chain<0> : bmode == 1 ? k_tc_chain<1> : bmode == 2 ? k_tc_chain<2> : k_tc_chain<3>;
+  QSVB_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kChainSmem)));
+  QSVB_CK(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
+                               int(cudaSharedmemCarveoutMaxShared)));
+  // one persistent CTA per SM (the tensor-memory allocation of 512 columns assumes it)
+  const unsigned grid = unsigned(std::max<uint64_t>(1, std::min<uint64_t>(ntiles, uint64_t(env.num_sms))));
+  kern<<<grid, kThreads, kChainSmem, env.stream>>>(re, im, ntiles, static_cast<const uint4*>(dev_mat), p,
+                                                     env.err_flag, lay.maps[0], lay.maps[1]);
+  QSVB_CK(cudaGetLastError());
+}
+
+template <class R>
+void launch_permute(const LaunchEnv& env, R* re, R* im, uint32_t n, const Sweep& s) {
+  QSVB_REQUIRE(n >= 12, "permutation pass: state too small");
+  PermParams p;
+  std::memset(&p, 0, sizeof(p));
+  TileLayout lay;
+  tile_layout(n, s.chain_tbits, nullptr, nullptr, lay);
+  std::copy(lay.hibits, lay.hibits + 6, p.hibits);
+  std::copy(lay.hioff, lay.hioff + 64, p.hioff);
+  for (uint32_t i = 0; i < 64; ++i) {
+    p.plo[i] = uint16_t(permute12(i, s.chain_perm));
+    p.phi[i] = uint16_t(permute12(i << 6, s.chain_perm));
+  }
+  const uint64_t ntiles = 1ull << (n - 12);
+  const size_t smem = 2 * sizeof(R) * kTileAmps;
+  QSVB_CK(cudaFuncSetAttribute(k_permute_tiles<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+  int occ = 0;
+  QSVB_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_permute_tiles<R>, kPermThreads, smem));
+  QSVB_REQUIRE(occ >= 1, "permutation kernel does not fit on an SM");
+  const unsigned grid = unsigned(std::max<uint64_t>(1, std::min<uint64_t>(ntiles, uint64_t(env.num_sms) * occ)));
+  k_permute_tiles<R><<<grid, kPermThreads, smem, env.stream>>>(re, im, ntiles, p);
+  QSVB_CK(cudaGetLastError());
+}
+template void launch_permute<float>(const LaunchEnv&, float*, float*, uint32_t, const Sweep&);
+template void launch_permute<double>(const LaunchEnv&, double*, double*, uint32_t, const Sweep&);
+
+}  // namespace qsvb
