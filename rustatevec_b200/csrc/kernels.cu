@@ -409,18 +409,32 @@ struct DenseP {
   uint32_t vecstore;    // 1 when the low LOG address bits are column bits
 };
 
-template <class R, int K, int NCB>
+// cp.async copies global -> shared (16 bytes cached in L2 only, or one 4- / 8-byte element).
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(static_cast<uint32_t>(__cvta_generic_to_shared(dst))),
+               "l"(src)
+               : "memory");
+}
+template <class R> __device__ __forceinline__ void cp_async_elem(R* dst, const R* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(static_cast<uint32_t>(__cvta_generic_to_shared(dst))),
+               "l"(src), "n"(int(sizeof(R)))
+               : "memory");
+}
+
+// DB: two tile buffers, the gather of tile i + grid (cp.async) in flight while tile i is
+// multiplied and written back; otherwise one buffer, gathered with vector loads.
+template <class R, int K, int NCB, bool DB>
 __global__ void __launch_bounds__(kThreads) k_dense(R* __restrict__ re, R* __restrict__ im,
                                                     uint64_t ntiles, const R* __restrict__ ut,
                                                     DenseP p) {
   constexpr int M = 1 << K, NC = 1 << NCB, N = VecT<R>::N;
   constexpr int RG = kThreads / NC;  // row groups
   constexpr int RPT = M / RG;        // rows per thread
+  constexpr int NB = DB ? 2 : 1;     // tile buffers
   static_assert(RG * NC == kThreads && RPT * RG == M, "tile shape");
   extern __shared__ __align__(16) char smem_raw[];
-  R* xr = reinterpret_cast<R*>(smem_raw);
-  R* xi = xr + M * NC;
-  R* us = xi + M * NC;  // [s][r] complex interleaved
+  R* xbuf = reinterpret_cast<R*>(smem_raw);  // buffer b: re [M * NC], im [M * NC]
+  R* us = xbuf + NB * 2 * M * NC;            // [s][r] complex interleaved
   uint32_t* dlo = reinterpret_cast<uint32_t*>(us + 2 * M * M);
   uint32_t* dhi = dlo + NC;
   uint64_t* hio = reinterpret_cast<uint64_t*>(dhi + M);  // 8-byte aligned: NC + M is even
@@ -432,7 +446,7 @@ __global__ void __launch_bounds__(kThreads) k_dense(R* __restrict__ re, R* __res
   }
   const int col = threadIdx.x % NC, rg = threadIdx.x / NC;
   const bool vs = p.vecstore != 0;
-  for (uint64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+  auto tile_base = [&](uint64_t tile) {
     uint64_t base = tile << NCB;
 #pragma unroll
     for (int j = 0; j < K; ++j) {
@@ -440,27 +454,69 @@ __global__ void __launch_bounds__(kThreads) k_dense(R* __restrict__ re, R* __res
       const uint64_t lo = base & ((1ull << b) - 1ull);
       base = ((base - lo) << 1) | lo;
     }
-    __syncthreads();
+    return base;
+  };
+  // the tile's gather into buffer b: contiguous runs of >= NC amplitudes, scattered into the
+  // (row, column) tile layout
+  auto gather = [&](uint64_t base, int b) {
+    R* xr = xbuf + b * 2 * M * NC;
+    R* xi = xr + M * NC;
     for (int v = threadIdx.x; v < M * NC / N; v += kThreads) {
       const int t = v * N, tlo = t & (NC - 1), thi = t >> NCB;
       const uint64_t a = base + hio[thi] + uint64_t(tlo);
-      R vr[N], vi[N];
-      vld(re + a, vr);
-      vld(im + a, vi);
-      if (vs) {
-        const uint32_t d = dlo[tlo] + dhi[thi];
-        vst(xr + d, vr);
-        vst(xi + d, vi);
-      } else {
+      if constexpr (DB) {
+        if (vs) {
+          const uint32_t d = dlo[tlo] + dhi[thi];
+          cp_async16(xr + d, re + a);
+          cp_async16(xi + d, im + a);
+        } else {
 #pragma unroll
-        for (int e = 0; e < N; ++e) {
-          const uint32_t d = dlo[tlo + e] + dhi[thi];
-          xr[d] = vr[e];
-          xi[d] = vi[e];
+          for (int e = 0; e < N; ++e) {
+            const uint32_t d = dlo[tlo + e] + dhi[thi];
+            cp_async_elem(xr + d, re + a + e);
+            cp_async_elem(xi + d, im + a + e);
+          }
+        }
+      } else {
+        R vr[N], vi[N];
+        vld(re + a, vr);
+        vld(im + a, vi);
+        if (vs) {
+          const uint32_t d = dlo[tlo] + dhi[thi];
+          vst(xr + d, vr);
+          vst(xi + d, vi);
+        } else {
+#pragma unroll
+          for (int e = 0; e < N; ++e) {
+            const uint32_t d = dlo[tlo + e] + dhi[thi];
+            xr[d] = vr[e];
+            xi[d] = vi[e];
+          }
         }
       }
     }
+  };
+  __syncthreads();  // tables ready
+  if constexpr (DB) {
+    if (blockIdx.x < ntiles) gather(tile_base(blockIdx.x), 0);
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  }
+  int cur = 0;
+  for (uint64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, cur ^= NB - 1) {
+    const uint64_t base = tile_base(tile);
+    if constexpr (DB) {
+      // the next tile's gather goes into the other buffer (its last reads ended at the barrier
+      // closing the previous iteration); then wait for this tile's group only
+      const uint64_t nxt = tile + gridDim.x;
+      if (nxt < ntiles) gather(tile_base(nxt), cur ^ 1);
+      asm volatile("cp.async.commit_group;" ::: "memory");
+      asm volatile("cp.async.wait_group 1;" ::: "memory");
+    } else {
+      gather(base, 0);
+    }
     __syncthreads();
+    R* xr = xbuf + cur * 2 * M * NC;
+    R* xi = xr + M * NC;
     R ar[RPT], ai[RPT];
 #pragma unroll
     for (int r = 0; r < RPT; ++r) ar[r] = ai[r] = R(0);
@@ -497,7 +553,9 @@ __global__ void __launch_bounds__(kThreads) k_dense(R* __restrict__ re, R* __res
       vst(re + a, vr);
       vst(im + a, vi);
     }
+    __syncthreads();  // this buffer's reads are done before a later gather reuses it
   }
+  if constexpr (DB) asm volatile("cp.async.wait_all;" ::: "memory");
 }
 
 // Small-state fallback: one 2^K block per thread (gather, matvec, scatter).
@@ -835,10 +893,14 @@ template <class R> constexpr int dense_ncb(int K) {
   return sizeof(R) == 4 ? 7 : (K <= 3 ? 8 : (K == 6 ? 5 : 6));
 }
 
+// Double-buffered gathers where the sweep is memory-bound (k <= 4); the compute-bound k = 5, 6
+// CUDA-core tiles keep one buffer and twice the blocks per SM.
+template <class R> constexpr bool dense_db(int K) { return K <= 4; }
+
 template <class R, int K>
 size_t dense_smem_bytes() {
-  constexpr int M = 1 << K, NC = 1 << dense_ncb<R>(K);
-  return size_t(2) * M * NC * sizeof(R) + size_t(2) * M * M * sizeof(R) + (NC + M) * 4 + M * 8;
+  constexpr int M = 1 << K, NC = 1 << dense_ncb<R>(K), NB = dense_db<R>(K) ? 2 : 1;
+  return size_t(2) * NB * M * NC * sizeof(R) + size_t(2) * M * M * sizeof(R) + (NC + M) * 4 + M * 8;
 }
 
 template <class R, int K>
@@ -898,13 +960,14 @@ void launch_dense_k(const LaunchEnv& env, R* re, R* im, uint32_t n, const Sweep&
     if (gate_rank[b] >= 0) p.vecstore = 0;
   const uint64_t ntiles = 1ull << (n - K - NCB);
   const size_t smem = dense_smem_bytes<R, K>();
-  QSVB_CK(cudaFuncSetAttribute(k_dense<R, K, NCB>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-  QSVB_CK(cudaFuncSetAttribute(k_dense<R, K, NCB>, cudaFuncAttributePreferredSharedMemoryCarveout,
+  constexpr bool DB = dense_db<R>(K);
+  QSVB_CK(cudaFuncSetAttribute(k_dense<R, K, NCB, DB>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+  QSVB_CK(cudaFuncSetAttribute(k_dense<R, K, NCB, DB>, cudaFuncAttributePreferredSharedMemoryCarveout,
                                int(cudaSharedmemCarveoutMaxShared)));
   int occ = 1;
-  QSVB_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_dense<R, K, NCB>, kThreads, smem));
+  QSVB_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_dense<R, K, NCB, DB>, kThreads, smem));
   const unsigned grid = unsigned(std::max<uint64_t>(1, std::min<uint64_t>(ntiles, uint64_t(env.num_sms) * std::max(occ, 1))));
-  k_dense<R, K, NCB><<<grid, kThreads, smem, env.stream>>>(re, im, ntiles, ut, p);
+  k_dense<R, K, NCB, DB><<<grid, kThreads, smem, env.stream>>>(re, im, ntiles, ut, p);
   check_launch();
 }
 
