@@ -779,6 +779,10 @@ KERNEL_CASES = {
     "dense4_c128": ("f64", lambda n: [("u4", [0, 1, 2, 3])]),
     "dense5_c128": ("f64", lambda n: [("u5", [2, 3, 9, 10, 20])]),
     "dense4_c128": ("f64", lambda n: [("u4", [0, 1, 2, 3])]),
+    # tensor-core chain passes: one pass of 1 / 2 / 3 Haar 6-qubit matrices on the qubits 0..11
+    "chain1": ("f32", lambda n: [("u6", list(range(6, 12)))]),
+    "chain2": ("f32", lambda n: [("u6", list(range(6, 12))), ("u6", list(range(6)))]),
+    "chain3": ("f32", lambda n: [("u6", list(range(6, 12))), ("u6", list(range(6))), ("u6", list(range(3, 9)))]),
 }
 
 
@@ -837,7 +841,10 @@ def run_kernel_case(args):
         be.init_basis(st, 0)
     else:
         be.init_gaussian(st, 7)
-    p = Plan(be, c, L.make_opts(planner, 2, engine, use_graph=False))
+    opts = L.make_opts(planner, 2, engine, use_graph=False)
+    if args.kernel_case.startswith("chain"):
+        opts = L.make_opts(L.PLAN_CHAIN, 6, L.ENGINE_AUTO, use_graph=False, chain_max_matrices=3)
+    p = Plan(be, c, opts)
     info = p.sweeps()
     stream = torch.cuda.ExternalStream(be.stream())
     for _ in range(2):
