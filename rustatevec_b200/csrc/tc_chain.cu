@@ -227,8 +227,12 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_chain(float* __restrict__ re
   uint64_t* ioempty = bars + 4;   // [4] converters -> producer
   uint64_t* bfull = bars + 8;     // [2] converters -> MMA
   uint64_t* bfree = bars + 10;    // [2] MMA commit -> converters
-  uint64_t* dfull = bars + 12;    // [2] MMA commit -> converters (matrices 0..nmat-2) / epilogue (last)
-  uint64_t* dfree = bars + 14;    // [2] accumulator read -> MMA
+  // accumulators: each barrier has one consumer role that waits on every one of its phases in
+  // order (a parity wait cannot tell a completion from the one two phases later, so no role may
+  // skip phases that belong to another)
+  uint64_t* dfull_c = bars + 12;  // [2] MMA commit -> converters (accumulators of matrices 0..nmat-2)
+  uint64_t* dfull_e = bars + 14;  // [2] MMA commit -> epilogue (accumulators of the last matrix)
+  uint64_t* dfree = bars + 16;    // [2] accumulator read -> MMA
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 20);
   uint64_t* s_hioff = reinterpret_cast<uint64_t*>(bars + 21);
   uint16_t* s_dlo = reinterpret_cast<uint16_t*>(s_hioff + 64);
@@ -262,7 +266,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_chain(float* __restrict__ re
     for (int s = 0; s < 2; ++s) {
       mbar_init(&bfull[s], kCvtThreads);
       mbar_init(&bfree[s], 1);
-      mbar_init(&dfull[s], 1);
+      mbar_init(&dfull_c[s], 1);
+      mbar_init(&dfull_e[s], 1);
       // every converter thread (count 1) or every epilogue thread (count 2) once it has read the
       // accumulator
       mbar_init(&dfree[s], kCvtThreads);
@@ -353,6 +358,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_chain(float* __restrict__ re
     if (nmat > 1) rb1 = p.crow[1][row];
     if (nmat > 2) rb2 = p.crow[2][row];
     uint32_t g = 0;
+    uint32_t cph[2] = {0, 0};  // accumulators of each slot consumed so far (phases of dfull_c)
     bool stop = false;
     for (uint64_t w0 = 0; w0 < my_tiles && !stop; w0 += kWave) {
       const uint32_t nt = my_tiles - w0 < uint64_t(kWave) ? uint32_t(my_tiles - w0) : uint32_t(kWave);
@@ -362,10 +368,12 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_chain(float* __restrict__ re
           const uint32_t slot = uint32_t(i % kIoSlots);
           const uint32_t bs = g & 1u, bpar = (g >> 1) & 1u;
           // the input: the staged tile (matrix 0) or the accumulator of this tile's previous
-          // matrix, which the MMA wrote for item g - nt
-          const uint32_t src = g - nt, ds = src & 1u, dpar = (src >> 1) & 1u;
+          // matrix, which the MMA wrote for item g - nt; the converters consume every
+          // intermediate accumulator, slot by slot in item order
+          const uint32_t ds = (g - nt) & 1u;
           bool ready = j == 0 ? mbar_wait(&iofull[slot], uint32_t((i / kIoSlots) & 1))
-                              : mbar_wait(&dfull[ds], dpar);
+                              : mbar_wait(&dfull_c[ds], cph[ds] & 1u);
+          if (j > 0) ++cph[ds];
           ready = ready && mbar_wait(&bfree[bs], bpar ^ 1u);
           if (!__all_sync(0xffffffffu, ready)) {
             atomicExch(err, 1);
@@ -383,12 +391,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_chain(float* __restrict__ re
           } else {
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             uint32_t v[32];
-            const uint32_t taddr = tmem + ((quad * 32) << 16) + ds * 64u + half * 32u;
-            uint32_t (&v0)[16] = *reinterpret_cast<uint32_t(*)[16]>(&v[0]);
-            uint32_t (&v1)[16] = *reinterpret_cast<uint32_t(*)[16]>(&v[16]);
-            tmem_ld16(taddr, v0);
-            tmem_ld16(taddr + 16u, v1);
-            asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+            tmem_ld32_wait(tmem + ((quad * 32) << 16) + ds * 64u + half * 32u, v);
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
             mbar_arrive(&dfree[ds]);  // this thread's part of the accumulator is in registers
             if (j == 1) convert_next<1>(v, half, rb1, b_hi, b_lo, p);
@@ -434,7 +437,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_chain(float* __restrict__ re
               mma_bf16_ts(d_tmem, a_hi + uint32_t(s) * 8u, dbh, idesc, 1u);
             }
             mma_commit(&bfree[bs]);  // B buffer consumed
-            mma_commit(&dfull[bs]);  // accumulator ready
+            mma_commit(j + 1 < nmat ? &dfull_c[bs] : &dfull_e[bs]);  // accumulator ready for its consumer
           }
       }
     }
@@ -446,13 +449,15 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_chain(float* __restrict__ re
     const uint32_t row = uint32_t(quad * 32 + lane);
     const uint32_t frow = p.frow[row];
     uint32_t g = 0;
+    uint32_t eph[2] = {0, 0};  // final accumulators of each slot consumed so far (phases of dfull_e)
     bool stop = false;
     for (uint64_t w0 = 0; w0 < my_tiles && !stop; w0 += kWave) {
       const uint32_t nt = my_tiles - w0 < uint64_t(kWave) ? uint32_t(my_tiles - w0) : uint32_t(kWave);
       g += (nmat - 1) * nt;  // items of the earlier matrices belong to the converters
       for (uint32_t tt = 0; tt < nt; ++tt, ++g) {
-        const uint32_t ds = g & 1u, dpar = (g >> 1) & 1u;
-        const bool ready = mbar_wait(&dfull[ds], dpar);
+        const uint32_t ds = g & 1u;
+        const bool ready = mbar_wait(&dfull_e[ds], eph[ds] & 1u);
+        ++eph[ds];
         // one decision for all epilogue threads; reaching this barrier also means every thread's
         // reads of the previous tile's staging are done
         if (!named_all(2, kEpiThreads, ready)) {
@@ -461,11 +466,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_chain(float* __restrict__ re
           break;
         }
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        uint32_t v[4][16];
-        const uint32_t taddr = tmem + (uint32_t(quad * 32) << 16) + ds * 64u;
-#pragma unroll
-        for (int cb = 0; cb < 4; ++cb) tmem_ld16(taddr + uint32_t(cb * 16), v[cb]);
-        asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+        uint32_t v[64];
+        tmem_ld64_wait(tmem + (uint32_t(quad * 32) << 16) + ds * 64u, v);
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
         mbar_arrive_cnt(&dfree[ds], 2);  // 128 epilogue threads stand for the 256 converter arrivals
         char* st = reinterpret_cast<char*>(ostage);
@@ -473,7 +475,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_chain(float* __restrict__ re
         for (int cb = 0; cb < 4; ++cb)
 #pragma unroll
           for (int q = 0; q < 16; ++q)
-            *reinterpret_cast<float*>(st + (frow ^ uint32_t(p.fcol[cb * 16 + q]))) = __uint_as_float(v[cb][q]);
+            *reinterpret_cast<float*>(st + (frow ^ uint32_t(p.fcol[cb * 16 + q]))) = __uint_as_float(v[cb * 16 + q]);
         named_sync(1, kEpiThreads);  // the whole result is staged
         const uint64_t base = tile_base(blockIdx.x + (w0 + tt) * gridDim.x);
         const uint32_t s1 = p.sig_lo[1], s2 = p.sig_lo[2], s3 = p.sig_lo[3];

@@ -411,11 +411,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_dense(float* __restrict__ 
       }
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       const long long ta = clock64();
-      uint32_t v[4][16];
-      const uint32_t taddr = tmem + (uint32_t(quad * 32) << 16) + ds * kMmaN;
-#pragma unroll
-      for (int cb = 0; cb < 4; ++cb) tmem_ld16(taddr + uint32_t(cb * 16), v[cb]);
-      asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+      uint32_t v[64];  // column c of this lane's accumulator row
+      tmem_ld64_wait(tmem + (uint32_t(quad * 32) << 16) + ds * kMmaN, v);
       asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
       mbar_arrive(&dfree[ds]);  // accumulator may be overwritten now
       const long long tb = clock64();
@@ -427,15 +424,15 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_dense(float* __restrict__ 
 #pragma unroll
           for (int q = 0; q < 4; ++q) {
             *reinterpret_cast<float4*>(st + (sch[cb] ^ p.tcl[q * 4])) =
-                make_float4(__uint_as_float(v[cb][4 * q]), __uint_as_float(v[cb][4 * q + 1]),
-                            __uint_as_float(v[cb][4 * q + 2]), __uint_as_float(v[cb][4 * q + 3]));
+                make_float4(__uint_as_float(v[cb * 16 + 4 * q]), __uint_as_float(v[cb * 16 + 4 * q + 1]),
+                            __uint_as_float(v[cb * 16 + 4 * q + 2]), __uint_as_float(v[cb * 16 + 4 * q + 3]));
           }
       } else {
 #pragma unroll
         for (int cb = 0; cb < 4; ++cb)
 #pragma unroll
           for (int q = 0; q < 16; ++q)
-            *reinterpret_cast<float*>(reinterpret_cast<char*>(st) + (sch[cb] ^ p.tclb[q])) = __uint_as_float(v[cb][q]);
+            *reinterpret_cast<float*>(reinterpret_cast<char*>(st) + (sch[cb] ^ p.tclb[q])) = __uint_as_float(v[cb * 16 + q]);
       }
       const long long tc0 = clock64();
       w3 += tc0 - tb;
