@@ -81,23 +81,43 @@ int tile_pos(const uint32_t (&tb)[12], uint32_t bit) {
 
 // Moves the qubits of S so that `low` (6 qubits of S) sit on state bits 0..5; the other qubits of S
 // take the state bits of the tile those vacate: a qubit whose own state bit is among them goes home,
-// qubits already in place stay. Returns the tile permutation (tile position i -> perm[i]) and
-// updates the layout.
-void relabel(Layout& lay, const uint32_t (&tb)[12], uint64_t low, uint8_t (&perm)[12]) {
+// qubits already in place stay. State bits 0 and 1 take two qubits of `low` that are columns of
+// the pass's last matrix (`lastcols`) when there are two, so that the kernel's epilogue writes
+// 16-byte vectors. Returns the tile permutation (tile position i -> perm[i]) and updates the layout.
+void relabel(Layout& lay, const uint32_t (&tb)[12], uint64_t low, uint64_t lastcols, uint8_t (&perm)[12]) {
   std::vector<uint32_t> occ(12);
   for (int i = 0; i < 12; ++i) occ[size_t(i)] = lay.log_at[tb[i]];
   std::vector<int> dest(12, -1);
   std::vector<char> taken(12, 0);
   auto want_low = [&](int i) { return ((low >> occ[size_t(i)]) & 1u) != 0; };
+  std::vector<int> pref;  // tile positions holding preferred qubits, those already on bit 0 / 1 first
+  for (int i = 0; i < 2; ++i)
+    if (want_low(i) && ((lastcols >> occ[size_t(i)]) & 1u)) pref.push_back(i);
+  for (int i = 2; i < 12; ++i)
+    if (want_low(i) && ((lastcols >> occ[size_t(i)]) & 1u)) pref.push_back(i);
+  if (pref.size() >= 2) {
+    for (int k = 0; k < 2; ++k)  // a preferred qubit already on bit 0 or 1 keeps it
+      if (pref[size_t(k)] < 2) {
+        dest[size_t(pref[size_t(k)])] = pref[size_t(k)];
+        taken[size_t(pref[size_t(k)])] = 1;
+      }
+    for (int k = 0; k < 2; ++k) {
+      const int i = pref[size_t(k)];
+      if (dest[size_t(i)] >= 0) continue;
+      const int t = taken[0] ? 1 : 0;
+      dest[size_t(i)] = t;
+      taken[size_t(t)] = 1;
+    }
+  }
   // qubits already on the right side stay
   for (int i = 0; i < 12; ++i)
-    if (want_low(i) == (i < 6)) {
+    if (dest[size_t(i)] < 0 && want_low(i) == (i < 6) && !taken[size_t(i)]) {
       dest[size_t(i)] = i;
       taken[size_t(i)] = 1;
     }
   // qubits leaving the low bits go home when their own bit is free in the tile
   for (int i = 0; i < 6; ++i) {
-    if (dest[size_t(i)] >= 0) continue;
+    if (dest[size_t(i)] >= 0 || want_low(i)) continue;
     const int home = tile_pos(tb, occ[size_t(i)]);
     if (home >= 6 && !taken[size_t(home)]) {
       dest[size_t(i)] = home;
@@ -319,8 +339,14 @@ std::vector<Sweep> plan_chain(const std::vector<Gate>& in, uint32_t n, uint32_t 
     }
     for (uint32_t b = 0; b < 6 && popc(next_low) < 6; ++b) next_low |= 1ull << lay.log_at[b];
     for (int i = 0; i < 12 && popc(next_low) < 6; ++i) next_low |= 1ull << lay.log_at[tb[i]];
+    uint64_t lastcols = 0;  // qubits that are columns of the pass's last matrix
+    {
+      uint64_t lastrows = 0;
+      for (int i = 0; i < 6; ++i) lastrows |= 1ull << lay.log_at[tb[s.chain_rows[s.chain_nmat - 1][i]]];
+      lastcols = S & ~lastrows;
+    }
     if (pending.empty()) assign_home(lay, tb, s.chain_perm);  // last pass: towards the identity
-    else relabel(lay, tb, next_low, s.chain_perm);
+    else relabel(lay, tb, next_low, lastcols, s.chain_perm);
     tc_chain_prepare(s);
     out.push_back(std::move(s));
   }

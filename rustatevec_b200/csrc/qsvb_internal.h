@@ -92,6 +92,10 @@ struct Sweep {
   uint8_t chain_cols[kChainMaxMats][6] = {};
   uint8_t chain_perm[12] = {};
   std::vector<std::vector<cd>> chain_mats;
+  // set by tc_chain_prepare: B operand of matrix j >= 1 K-major (1) or MN-major (0), and whether
+  // the last matrix's columns 0, 1 land on output tile positions 0, 1 (16-byte epilogue stores)
+  uint8_t chain_bk[kChainMaxMats] = {};
+  uint8_t chain_evec = 0;
 };
 
 std::vector<Gate> gates_from_circuit(const qsvb_circuit* c);
@@ -161,7 +165,9 @@ void launch_tc_dense(const LaunchEnv& e, float* re, float* im, uint32_t n, const
                      const void* dev_mat);
 
 // Chained tensor-core passes and tile permutations (complex64): implemented in tc_chain.cu.
-void tc_chain_prepare(Sweep& s);  // puts matrices 1.. in the row/column order their conversion needs
+// Chooses each later matrix's operand layout and row / column order (and reorders its entries) so
+// that the kernel's conversions and epilogue use 16-byte shared-memory accesses; needs chain_perm.
+void tc_chain_prepare(Sweep& s);
 size_t tc_chain_matrix_bytes(const Sweep& s);
 void tc_chain_check(const Sweep& s, uint32_t n);  // builds and validates the kernel tables (host only)
 void tc_chain_pack(const Sweep& s, void* host_dst);

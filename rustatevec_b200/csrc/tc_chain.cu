@@ -14,15 +14,19 @@
 //     input slots (address order);
 //   converter warps (8): for a tile's first matrix, split the staged fp32 tile into the bf16 hi/lo
 //     B operand (one of two B buffers; layout chosen by which matrix qubits are state bits 0, 1);
-//     for every later matrix, read the previous matrix's accumulator straight from tensor memory
-//     (each warp its lane quadrant and half of the 64 columns), split it and scatter it into the
-//     next B operand (MN-major; each element's byte offset is an XOR of a per-row and a per-column
-//     part, both precomputed on the host);
+//     for every later matrix, gather 32 of the previous matrix's accumulator columns straight from
+//     tensor memory (each warp its lane quadrant, one column per load, in the order the next
+//     operand needs), split them and write them into the next B operand as 16-byte chunks of 8
+//     bf16: the operand is MN- or K-major, whichever has three of its contiguous bits among the
+//     previous matrix's columns (one of the two always does); chunk offsets are an XOR of a per-row
+//     and a per-chunk part, both precomputed on the host;
 //   MMA warp (one lane): 24 tcgen05.mma per matrix into one of two accumulators (64 columns each),
 //     the A operand (Whi, Wlo of matrix j) resident in tensor memory for the whole kernel;
 //   epilogue warps (4): after the last matrix, read the accumulator, stage it in shared memory in
-//     the permuted address order (an XOR swizzle per pass makes both the scattered writes and the
-//     reads of the write-back bank-conflict free) and write the tile back with 16-byte stores.
+//     the permuted address order (16-byte stores when the pass's permutation puts the last matrix's
+//     first two columns on output bits 0 and 1, which the planner arranges; scalar stores
+//     otherwise; a per-pass XOR swizzle keeps both the staging writes and the write-back's reads
+//     bank-conflict free) and write the tile back with 16-byte stores.
 // Work items are (tile, matrix) pairs. Two tiles are in flight at a time, and every role walks the
 // same item order: matrix 0 of tiles a and b, matrix 1 of tiles a and b, ..., so the MMA of one
 // tile overlaps the conversion of the other. Every item depends only on earlier items, so the
@@ -86,10 +90,14 @@ struct ChainParams {
   uint16_t dstlo[64], dsthi[64];
   uint16_t tplo[32], tphi[32];
   uint32_t b2_bit0, pair_shift;
-  // matrix j >= 1 read from the accumulator of matrix j - 1: byte offset in the B buffer of
-  // accumulator row r (r = part * 64 + gate row) and of column c; the element's offset is the XOR
+  // matrix j >= 1 read from the accumulator of matrix j - 1: the converter warp of half w gathers,
+  // for chunk m (0..3) and element e (0..7), accumulator column cw[w] ^ cm[m] ^ ce[e]; the chunk's 8
+  // bf16 go to B at byte offset crow[r] ^ cchunk[w][m] (+ 2 e), r = part * 64 + gate row
   uint16_t crow[kChainMaxMats][128];
-  uint16_t ccol[kChainMaxMats][64];
+  uint16_t cchunk[kChainMaxMats][2][4];
+  uint8_t ce[kChainMaxMats][8], cm[kChainMaxMats][4], cw[kChainMaxMats][2];
+  uint8_t bk[kChainMaxMats];  // B of matrix j >= 1 is K-major
+  uint32_t evec;              // the epilogue's staging writes and reads are 16-byte vectors
   // last matrix: byte offset in the output staging of accumulator row r and of column c (XOR)
   uint16_t frow[128];
   uint16_t fcol[64];
@@ -193,21 +201,53 @@ __device__ __forceinline__ void convert_first(const float* __restrict__ sre, con
   }
 }
 
-// Matrix J >= 1: the accumulator of matrix J - 1 (this warp's 32 lanes, 32 of its 64 columns,
-// already in registers) split and scattered into the MN-major B operand of matrix J. The column
-// offsets are compile-time indices into the parameter bank.
-template <int J>
-__device__ __forceinline__ void convert_next(const uint32_t (&v)[32], uint32_t half, uint32_t rbase,
-                                             uint8_t* __restrict__ b_hi, uint8_t* __restrict__ b_lo,
-                                             const ChainParams& p) {
-  const uint32_t hoff = half ? uint32_t(p.ccol[J][32]) : 0u;  // column bit 5 (XOR-linear)
+// Eight accumulator columns of this warp's 32 lanes, one column per load (addresses a0 + d[e]),
+// defined only once the loads have completed.
+__device__ __forceinline__ void tmem_ld_gather8(uint32_t a0, const uint32_t (&d)[8], uint32_t (&r)[8]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x1.b32 {%0}, [%8];\n\t"
+      "tcgen05.ld.sync.aligned.32x32b.x1.b32 {%1}, [%9];\n\t"
+      "tcgen05.ld.sync.aligned.32x32b.x1.b32 {%2}, [%10];\n\t"
+      "tcgen05.ld.sync.aligned.32x32b.x1.b32 {%3}, [%11];\n\t"
+      "tcgen05.ld.sync.aligned.32x32b.x1.b32 {%4}, [%12];\n\t"
+      "tcgen05.ld.sync.aligned.32x32b.x1.b32 {%5}, [%13];\n\t"
+      "tcgen05.ld.sync.aligned.32x32b.x1.b32 {%6}, [%14];\n\t"
+      "tcgen05.ld.sync.aligned.32x32b.x1.b32 {%7}, [%15];\n\t"
+      "tcgen05.wait::ld.sync.aligned;\n"
+      : "=&r"(r[0]), "=&r"(r[1]), "=&r"(r[2]), "=&r"(r[3]), "=&r"(r[4]), "=&r"(r[5]), "=&r"(r[6]), "=&r"(r[7])
+      : "r"(a0 + d[0]), "r"(a0 + d[1]), "r"(a0 + d[2]), "r"(a0 + d[3]), "r"(a0 + d[4]), "r"(a0 + d[5]),
+        "r"(a0 + d[6]), "r"(a0 + d[7])
+      : "memory");
+}
+
+// bf16 hi/lo split of two values, packed as bf16 pairs (the first value in the low half).
+__device__ __forceinline__ void split2(uint32_t x0, uint32_t x1, uint32_t& hi, uint32_t& lo) {
+  const float2 f = make_float2(__uint_as_float(x0), __uint_as_float(x1));
+  const __nv_bfloat162 h = __float22bfloat162_rn(f);
+  const float2 hf = __bfloat1622float2(h);
+  const __nv_bfloat162 l = __float22bfloat162_rn(make_float2(f.x - hf.x, f.y - hf.y));
+  hi = *reinterpret_cast<const uint32_t*>(&h);
+  lo = *reinterpret_cast<const uint32_t*>(&l);
+}
+
+// Matrix j >= 1: the accumulator of matrix j - 1 (its TMEM columns from tcol, this thread's row
+// offset rbase) into the B operand of matrix j, as four 16-byte chunks of hi and of lo.
+__device__ __forceinline__ void convert_next(uint32_t tcol, uint32_t rbase, const uint32_t (&cc)[4],
+                                             const uint32_t (&cm)[4], const uint32_t (&ce)[8],
+                                             uint8_t* __restrict__ b_hi, uint8_t* __restrict__ b_lo) {
 #pragma unroll
-  for (int q = 0; q < 32; ++q) {
-    const uint32_t off = (rbase ^ hoff) ^ uint32_t(p.ccol[J][q]);
-    __nv_bfloat16 h, l;
-    split_bf16(__uint_as_float(v[q]), h, l);
-    *reinterpret_cast<__nv_bfloat16*>(b_hi + off) = h;
-    *reinterpret_cast<__nv_bfloat16*>(b_lo + off) = l;
+  for (int m = 0; m < 4; ++m) {
+    uint32_t v[8];
+    tmem_ld_gather8(tcol + cm[m], ce, v);
+    uint32_t h[4], l[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) split2(v[2 * i], v[2 * i + 1], h[i], l[i]);
+    const uint32_t off = rbase ^ cc[m];
+    const uint32_t sh = smem_u32(b_hi + off), sl = smem_u32(b_lo + off);
+    asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(sh), "r"(h[0]), "r"(h[1]), "r"(h[2]), "r"(h[3])
+                 : "memory");
+    asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(sl), "r"(l[0]), "r"(l[1]), "r"(l[2]), "r"(l[3])
+                 : "memory");
   }
 }
 
@@ -357,6 +397,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_chain(float* __restrict__ re
     uint32_t rb1 = 0, rb2 = 0;                        // its byte offsets in the B of matrices 1 and 2
     if (nmat > 1) rb1 = p.crow[1][row];
     if (nmat > 2) rb2 = p.crow[2][row];
+    const uint32_t lane_base = tmem + ((quad * 32) << 16);
     uint32_t g = 0;
     uint32_t cph[2] = {0, 0};  // accumulators of each slot consumed so far (phases of dfull_c)
     bool stop = false;
@@ -390,12 +431,17 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_chain(float* __restrict__ re
             mbar_arrive(&ioempty[slot]);  // the staged tile has been read
           } else {
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            uint32_t v[32];
-            tmem_ld32_wait(tmem + ((quad * 32) << 16) + ds * 64u + half * 32u, v);
+            uint32_t cc[4], cmv[4], cev[8];
+#pragma unroll
+            for (int m = 0; m < 4; ++m) {
+              cc[m] = p.cchunk[j][half][m];
+              cmv[m] = p.cm[j][m];
+            }
+#pragma unroll
+            for (int e = 0; e < 8; ++e) cev[e] = p.ce[j][e];
+            convert_next(lane_base + ds * 64u + p.cw[j][half], j == 1 ? rb1 : rb2, cc, cmv, cev, b_hi, b_lo);
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-            mbar_arrive(&dfree[ds]);  // this thread's part of the accumulator is in registers
-            if (j == 1) convert_next<1>(v, half, rb1, b_hi, b_lo, p);
-            else convert_next<2>(v, half, rb2, b_hi, b_lo, p);
+            mbar_arrive(&dfree[ds]);  // this thread's part of the accumulator has been read
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             mbar_arrive(&bfull[bs]);
           }
@@ -422,7 +468,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_chain(float* __restrict__ re
               break;
             }
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const bool mn = j > 0 || BM == 0;
+            const bool mn = j > 0 ? p.bk[j] == 0 : BM == 0;
             const uint32_t idesc = mn ? idesc_mn : idesc_k;
             const uint32_t b_lbo = mn ? 128u * 128u : 16u;
             const uint32_t b_hi_s = smem_u32(bbuf + bs * 2 * kBBytes), b_lo_s = b_hi_s + kBBytes;
@@ -448,6 +494,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_chain(float* __restrict__ re
     const int et = tid - kEpiWarp0 * 32;
     const uint32_t row = uint32_t(quad * 32 + lane);
     const uint32_t frow = p.frow[row];
+    const bool evec = p.evec != 0;
     uint32_t g = 0;
     uint32_t eph[2] = {0, 0};  // final accumulators of each slot consumed so far (phases of dfull_e)
     bool stop = false;
@@ -471,11 +518,18 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_chain(float* __restrict__ re
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
         mbar_arrive_cnt(&dfree[ds], 2);  // 128 epilogue threads stand for the 256 converter arrivals
         char* st = reinterpret_cast<char*>(ostage);
+        if (evec) {
+          // columns 4k..4k+3 are four consecutive output positions: one 16-byte store each
 #pragma unroll
-        for (int cb = 0; cb < 4; ++cb)
+          for (int k = 0; k < 16; ++k)
+            *reinterpret_cast<float4*>(st + (frow ^ uint32_t(p.fcol[4 * k]))) =
+                make_float4(__uint_as_float(v[4 * k]), __uint_as_float(v[4 * k + 1]), __uint_as_float(v[4 * k + 2]),
+                            __uint_as_float(v[4 * k + 3]));
+        } else {
 #pragma unroll
-          for (int q = 0; q < 16; ++q)
-            *reinterpret_cast<float*>(st + (frow ^ uint32_t(p.fcol[cb * 16 + q]))) = __uint_as_float(v[cb * 16 + q]);
+          for (int q = 0; q < 64; ++q)
+            *reinterpret_cast<float*>(st + (frow ^ uint32_t(p.fcol[q]))) = __uint_as_float(v[q]);
+        }
         named_sync(1, kEpiThreads);  // the whole result is staged
         const uint64_t base = tile_base(blockIdx.x + (w0 + tt) * gridDim.x);
         const uint32_t s1 = p.sig_lo[1], s2 = p.sig_lo[2], s3 = p.sig_lo[3];
@@ -485,14 +539,19 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_chain(float* __restrict__ re
           const uint64_t a = base + s_hioff[thi] + uint64_t(tlo);
           const uint32_t w = uint32_t(s_sig[tlo]) ^ s_sig[64 + thi];
           float4 xr, xi;
-          xr.x = ostage[w];
-          xr.y = ostage[w ^ s1];
-          xr.z = ostage[w ^ s2];
-          xr.w = ostage[w ^ s3];
-          xi.x = ostage[kTileAmps + w];
-          xi.y = ostage[kTileAmps + (w ^ s1)];
-          xi.z = ostage[kTileAmps + (w ^ s2)];
-          xi.w = ostage[kTileAmps + (w ^ s3)];
+          if (evec) {  // the swizzle keeps bits 0, 1: positions t..t+3 are words w..w+3
+            xr = *reinterpret_cast<const float4*>(ostage + w);
+            xi = *reinterpret_cast<const float4*>(ostage + kTileAmps + w);
+          } else {
+            xr.x = ostage[w];
+            xr.y = ostage[w ^ s1];
+            xr.z = ostage[w ^ s2];
+            xr.w = ostage[w ^ s3];
+            xi.x = ostage[kTileAmps + w];
+            xi.y = ostage[kTileAmps + (w ^ s1)];
+            xi.z = ostage[kTileAmps + (w ^ s2)];
+            xi.w = ostage[kTileAmps + (w ^ s3)];
+          }
           __stcs(reinterpret_cast<float4*>(re + a), xr);
           __stcs(reinterpret_cast<float4*>(im + a), xi);
         }
@@ -606,13 +665,15 @@ int rank5(std::vector<uint32_t> v) {  // GF(2) rank of 5-bit vectors
   return r;
 }
 
-// The output staging swizzle: word index of position t = t ^ A(t >> 5), A a 7 -> 5 bit GF(2) map
-// (bits 5..11 stay, so it is a bijection), chosen so that the epilogue's 32 lanes (positions
-// lane_pos[0..4] for lane bits 0..4) and the write-back's 32 lanes (position bits 2..6) each hit
-// 32 distinct banks. Deterministic search; A = 0 (correct, with bank conflicts) if none is found.
-void staging_swizzle(const uint32_t (&lane_pos)[5], uint16_t (&sig_lo)[64], uint16_t (&sig_hi)[64]) {
+// The output staging swizzle: word index of position t = t ^ A(t >> 5), A a 7-bit -> 5-bit GF(2)
+// map (bits 5..11 stay, so it is a bijection). Scalar epilogue: the epilogue's 32 lanes (positions
+// lane_pos[0..4] for lane bits 0..4) and the write-back's 32 lanes (position bits 2..6) each hit 32
+// distinct banks. Vector epilogue (16-byte accesses, served 8 lanes at a time): A leaves bits 0, 1
+// alone, and the 8 lanes of each phase (lane bits 0..2) hit 8 distinct 16-byte bank groups in both
+// accesses. Deterministic search; A = 0 (correct, with bank conflicts) if none is found.
+void staging_swizzle(const uint32_t (&lane_pos)[5], bool vec, uint16_t (&sig_lo)[64], uint16_t (&sig_hi)[64]) {
   uint32_t A[7] = {0, 0, 0, 0, 0, 0, 0};
-  auto bank_of_bit = [&](uint32_t pos, const uint32_t (&a)[7]) { return pos < 5 ? (1u << pos) : a[pos - 5]; };
+  auto word_of_bit = [&](uint32_t pos, const uint32_t (&a)[7]) { return pos < 5 ? (1u << pos) : a[pos - 5]; };
   uint64_t rng = 0x9E3779B97F4A7C15ull;
   for (int attempt = 0; attempt < 20000; ++attempt) {
     uint32_t a[7];
@@ -620,14 +681,22 @@ void staging_swizzle(const uint32_t (&lane_pos)[5], uint16_t (&sig_lo)[64], uint
       rng ^= rng << 13;
       rng ^= rng >> 7;
       rng ^= rng << 17;
-      a[i] = uint32_t(rng) & 31u;
+      a[i] = vec ? (uint32_t(rng) & 7u) << 2 : uint32_t(rng) & 31u;
     }
     if (attempt == 0) std::fill(a, a + 7, 0u);
-    std::vector<uint32_t> w = {bank_of_bit(2, a), bank_of_bit(3, a), bank_of_bit(4, a), bank_of_bit(5, a),
-                               bank_of_bit(6, a)};
-    std::vector<uint32_t> e;
-    for (uint32_t b : lane_pos) e.push_back(bank_of_bit(b, a));
-    if (rank5(w) == 5 && rank5(e) == 5) {
+    bool ok;
+    if (vec) {
+      std::vector<uint32_t> e;
+      for (int b = 0; b < 3; ++b) e.push_back(word_of_bit(lane_pos[b], a) >> 2);
+      ok = rank5(e) == 3;  // the write-back's phases vary bits 2..4 of t only: always distinct
+    } else {
+      std::vector<uint32_t> w = {word_of_bit(2, a), word_of_bit(3, a), word_of_bit(4, a), word_of_bit(5, a),
+                                 word_of_bit(6, a)};
+      std::vector<uint32_t> e;
+      for (uint32_t b : lane_pos) e.push_back(word_of_bit(b, a));
+      ok = rank5(w) == 5 && rank5(e) == 5;
+    }
+    if (ok) {
       std::copy(a, a + 7, A);
       break;
     }
@@ -644,54 +713,28 @@ void staging_swizzle(const uint32_t (&lane_pos)[5], uint16_t (&sig_lo)[64], uint
   }
 }
 
-// Row and column orders of matrix j >= 1 (both internal to the pass) chosen so that the scattered
-// B stores of its conversion are bank-conflict free: the converter lanes carry matrix j-1's gate
-// rows 0..4; those that are rows of matrix j take row slots 0..2 (byte bits 7..9, swizzled into
-// bank bits), those that are its columns take column bits 0..2 first (one of them shares a 4-byte
-// word with its neighbour), then the column bits whose swizzle partner row bit is unused.
-void order_for_conversion(const uint8_t (&prev_rows)[6], uint64_t rows_set, uint8_t (&rows)[6], uint8_t (&cols)[6]) {
-  std::vector<uint8_t> lane_rows, lane_cols;
-  for (int b = 0; b < 5; ++b) {
-    if ((rows_set >> prev_rows[b]) & 1u) lane_rows.push_back(prev_rows[b]);
-    else lane_cols.push_back(prev_rows[b]);
-  }
-  int ri = 0;
-  bool row_used[6] = {false}, col_used[6] = {false};
-  uint8_t r_out[6], c_out[6];
-  for (uint8_t p : lane_rows) {
-    r_out[ri] = p;
-    row_used[ri] = true;
-    ++ri;
-  }
-  // column slots in preference order: 0, 1, 2, then 3 + k for row slots k that are unused
-  std::vector<int> cslots = {0, 1, 2};
-  for (int k = 0; k < 3; ++k)
-    if (k >= ri) cslots.push_back(3 + k);
-  for (int k = 0; k < 3; ++k)
-    if (k < ri) cslots.push_back(3 + k);
-  size_t ci = 0;
-  for (uint8_t p : lane_cols) {
-    c_out[cslots[ci]] = p;
-    col_used[cslots[ci]] = true;
-    ++ci;
-  }
-  // the remaining rows and columns in ascending tile position
-  std::vector<uint8_t> rest_rows, rest_cols;
-  for (int t = 0; t < 12; ++t) {
-    const bool in_lane = std::find(prev_rows, prev_rows + 5, uint8_t(t)) != prev_rows + 5;
-    if (in_lane) continue;
-    if ((rows_set >> t) & 1u) rest_rows.push_back(uint8_t(t));
-    else rest_cols.push_back(uint8_t(t));
-  }
-  size_t k = 0;
-  for (int i = 0; i < 6; ++i)
-    if (!row_used[i]) r_out[i] = rest_rows[k++];
-  k = 0;
-  for (int i = 0; i < 6; ++i)
-    if (!col_used[i]) c_out[i] = rest_cols[k++];
-  std::copy(r_out, r_out + 6, rows);
-  std::copy(c_out, c_out + 6, cols);
+// Layout class of the first matrix's B operand (the bmode of convert_first) from its rows.
+uint32_t first_bmode(const uint8_t (&rows0)[6], uint32_t* b2_bit0 = nullptr, uint32_t* pair_shift = nullptr) {
+  int rank0[12];
+  for (int t = 0; t < 12; ++t) rank0[t] = -1;
+  for (int i = 0; i < 6; ++i) rank0[rows0[i]] = i;
+  int row1_pos = -1;
+  for (int t = 0; t < 12; ++t)
+    if (rank0[t] == 1) row1_pos = t;
+  const bool low_cols = rank0[0] < 0 && rank0[1] < 0;
+  const bool low_rows = rank0[0] == 0 && rank0[1] == 1;
+  const bool lane_pair = rank0[0] < 0 && rank0[1] == 0 && row1_pos >= 2 && row1_pos <= 4;
+  if (b2_bit0) *b2_bit0 = rank0[0] == 0 ? 1u : 0u;
+  if (pair_shift) *pair_shift = lane_pair ? uint32_t(row1_pos - 2) : 0u;
+  return low_cols ? 0u : (low_rows ? 1u : (lane_pair ? 3u : 2u));
 }
+
+// Byte offset of element (kk, n) in a B operand of 128 K-rows x 64 columns, MN- or K-major (both
+// XOR-linear in the bits of kk and n).
+uint32_t b_off(bool kmajor, uint32_t kk, uint32_t n) { return kmajor ? kmaj_off(n, kk, 64) : mnmaj_off(kk, n); }
+
+bool contains6(const uint8_t (&a)[6], uint8_t v) { return std::find(a, a + 6, v) != a + 6; }
+int index6(const uint8_t (&a)[6], uint8_t v) { return int(std::find(a, a + 6, v) - a); }
 
 // Every table entry the kernel indexes shared memory with stays inside its buffer and maps its
 // domain one to one (a violated check is a planner or table bug, reported before any launch).
@@ -707,12 +750,21 @@ void check_chain_params(const ChainParams& p, uint32_t nm) {
     }
   for (uint32_t j = 1; j < nm; ++j) {
     reset();
-    for (uint32_t r = 0; r < 128; ++r)
-      for (uint32_t c = 0; c < 64; ++c) {
-        const uint32_t o = uint32_t(p.crow[j][r]) ^ p.ccol[j][c];
-        QSVB_REQUIRE(o < kBBytes && (o & 1u) == 0 && !seen[o], "chain pass: operand scatter table out of range");
-        seen[o] = 1;
-      }
+    std::vector<char> col_seen(64, 0);
+    for (uint32_t w = 0; w < 2; ++w)
+      for (uint32_t m = 0; m < 4; ++m)
+        for (uint32_t e = 0; e < 8; ++e) {
+          const uint32_t c = uint32_t(p.cw[j][w]) ^ p.cm[j][m] ^ p.ce[j][e];
+          QSVB_REQUIRE(c < 64 && !col_seen[c], "chain pass: accumulator column gather is not a bijection");
+          col_seen[c] = 1;
+          for (uint32_t r = 0; r < 128; ++r) {
+            const uint32_t chunk = uint32_t(p.crow[j][r]) ^ p.cchunk[j][w][m];
+            QSVB_REQUIRE((chunk & 15u) == 0, "chain pass: operand chunk not 16-byte aligned");
+            const uint32_t o = chunk + 2 * e;
+            QSVB_REQUIRE(o < kBBytes && !seen[o], "chain pass: operand scatter table out of range");
+            seen[o] = 1;
+          }
+        }
   }
   reset();
   for (uint32_t r = 0; r < 128; ++r)
@@ -721,12 +773,16 @@ void check_chain_params(const ChainParams& p, uint32_t nm) {
       QSVB_REQUIRE(o < 2u * kTileAmps * 4u && (o & 3u) == 0 && !seen[o >> 2],
                    "chain pass: output staging table out of range");
       seen[o >> 2] = 1;
+      if (p.evec && (c & 3u))
+        QSVB_REQUIRE(o == ((uint32_t(p.frow[r]) ^ p.fcol[c & ~3u]) + 4u * (c & 3u)),
+                     "chain pass: vector epilogue columns are not consecutive outputs");
     }
   reset();
   for (uint32_t h = 0; h < 64; ++h)
     for (uint32_t l = 0; l < 64; ++l) {
       const uint32_t w = uint32_t(p.sig_lo[l]) ^ p.sig_hi[h];
       QSVB_REQUIRE(w < 4096 && !seen[w], "chain pass: staging swizzle is not a bijection");
+      QSVB_REQUIRE(!p.evec || (w & 3u) == (l & 3u), "chain pass: vector staging swizzle moves bits 0, 1");
       seen[w] = 1;
     }
   reset();
@@ -737,8 +793,9 @@ void check_chain_params(const ChainParams& p, uint32_t nm) {
   }
 }
 
-// The kernel's parameter tables for one chain pass (tile addressing, operand scatter offsets,
-// output staging), checked to stay inside their buffers; returns the first matrix's B layout mode.
+// The kernel's parameter tables for one chain pass (tile addressing, operand gathers and chunk
+// offsets, output staging), checked to stay inside their buffers; returns the first matrix's B
+// layout mode.
 uint32_t build_chain_params(const Sweep& s, uint32_t n, float* re, float* im, ChainParams& p, TileLayout& lay) {
   QSVB_REQUIRE(n >= 12, "chain pass: state too small");
   QSVB_REQUIRE(s.chain_nmat >= 1 && s.chain_nmat <= uint32_t(kChainMaxMats), "chain pass: 1..3 matrices");
@@ -752,7 +809,6 @@ uint32_t build_chain_params(const Sweep& s, uint32_t n, float* re, float* im, Ch
   p.tm_rank = lay.tm_rank;
   std::copy(lay.tm_start, lay.tm_start + 5, p.tm_start);
   std::copy(lay.tm_len, lay.tm_len + 5, p.tm_len);
-  // matrix orders (tc_chain_prepare has put matrices 1.. in their conversion order)
   uint8_t rows[kChainMaxMats][6], cols[kChainMaxMats][6];
   for (uint32_t j = 0; j < nm; ++j) {
     std::copy(s.chain_rows[j], s.chain_rows[j] + 6, rows[j]);
@@ -761,30 +817,19 @@ uint32_t build_chain_params(const Sweep& s, uint32_t n, float* re, float* im, Ch
     for (int i = 0; i < 6; ++i) all |= (1u << rows[j][i]) | (1u << cols[j][i]);
     QSVB_REQUIRE(all == 0xFFFu, "chain pass: rows and columns must cover the 12 tile positions");
   }
-  // first matrix, read in address order
+  // first matrix, read in address order: rows ascend (the B layout modes rely on the lowest rows),
+  // and with bit 0 and 1 both columns (MN-major vectors) they are its columns 0 and 1
+  bool rows_ascending = true;
+  for (int i = 1; i < 6; ++i) rows_ascending = rows_ascending && rows[0][i] > rows[0][i - 1];
+  QSVB_REQUIRE(rows_ascending, "chain pass: the first matrix's rows must ascend");
+  const uint32_t bmode = first_bmode(rows[0], &p.b2_bit0, &p.pair_shift);
+  QSVB_REQUIRE(bmode != 0 || (cols[0][0] == 0 && cols[0][1] == 1),
+               "chain pass: state bits 0, 1 must be the first matrix's columns 0, 1");
   auto d_of = [&](uint32_t j, uint32_t t) { return (gather6(t, rows[j]) << 6) | gather6(t, cols[j]); };
   for (uint32_t l = 0; l < 64; ++l) {
     p.dstlo[l] = uint16_t(d_of(0, l));
     p.dsthi[l] = uint16_t(d_of(0, l << 6));
   }
-  int rank0[12];
-  for (int t = 0; t < 12; ++t) rank0[t] = -1;
-  for (int i = 0; i < 6; ++i) rank0[rows[0][i]] = i;
-  bool cols_ascending = true, rows_ascending = true;
-  for (int i = 1; i < 6; ++i) {
-    cols_ascending = cols_ascending && cols[0][i] > cols[0][i - 1];
-    rows_ascending = rows_ascending && rows[0][i] > rows[0][i - 1];
-  }
-  QSVB_REQUIRE(cols_ascending && rows_ascending, "chain pass: the first matrix's rows and columns must ascend");
-  const bool low_cols = rank0[0] < 0 && rank0[1] < 0;
-  const bool low_rows = rank0[0] == 0 && rank0[1] == 1;
-  int row1_pos = -1;
-  for (int t = 0; t < 12; ++t)
-    if (rank0[t] == 1) row1_pos = t;
-  const bool lane_pair = rank0[0] < 0 && rank0[1] == 0 && row1_pos >= 2 && row1_pos <= 4;
-  const uint32_t bmode = low_cols ? 0u : (low_rows ? 1u : (lane_pair ? 3u : 2u));
-  p.b2_bit0 = rank0[0] == 0 ? 1u : 0u;
-  p.pair_shift = lane_pair ? uint32_t(row1_pos - 2) : 0u;
   {
     // converter work order (as in tc_dense.cu): float4 index bits 0..2 stay; for K-major layouts the
     // lane bits 3 and 4 take the two float4 bits that spread the warp's B stores over most banks
@@ -835,24 +880,50 @@ uint32_t build_chain_params(const Sweep& s, uint32_t n, float* re, float* im, Ch
       p.tphi[u] = uint16_t(perm_t4(u << 5, best));
     }
   }
-  // later matrices: B byte offset of accumulator element (row r = part * 64 + gate row, column c)
-  // of matrix j - 1 = crow[j][r] ^ ccol[j][c] (the MN-major layout is XOR-linear in its bits)
+  // later matrices: the accumulator of matrix j - 1 into the B of matrix j. The B layout's three
+  // contiguous bits (column slots 0..2 when MN-major, row slots 0..2 when K-major) are columns of
+  // matrix j - 1: each converter thread gathers, per 16-byte chunk, the 8 accumulator columns that
+  // differ only in those three bits; the half of the columns a warp takes is fixed by one other
+  // column bit, and the chunk by the remaining two.
   auto pos_of = [&](uint32_t j, uint32_t srow, uint32_t col) { return deposit6(srow, rows[j]) | deposit6(col, cols[j]); };
   for (uint32_t j = 1; j < nm; ++j) {
-    for (uint32_t r = 0; r < 128; ++r) {
-      const uint32_t d = d_of(j, pos_of(j - 1, r & 63u, 0));
-      p.crow[j][r] = uint16_t(mnmaj_off((r >> 6) * 64u + (d >> 6), d & 63u));
+    const bool km = s.chain_bk[j] != 0;
+    p.bk[j] = km ? 1 : 0;
+    const uint8_t* vpos = km ? rows[j] : cols[j];  // positions of the contiguous bits 0..2
+    int vslot[3];
+    bool used[6] = {false, false, false, false, false, false};
+    for (int b = 0; b < 3; ++b) {
+      vslot[b] = index6(cols[j - 1], vpos[b]);
+      QSVB_REQUIRE(vslot[b] < 6, "chain pass: an operand's contiguous bits must be columns of the previous matrix");
+      used[vslot[b]] = true;
     }
-    for (uint32_t c = 0; c < 64; ++c) {
-      const uint32_t d = d_of(j, pos_of(j - 1, 0, c));
-      p.ccol[j][c] = uint16_t(mnmaj_off(d >> 6, d & 63u));
+    int free_slots[3], nf = 0;
+    for (int i = 0; i < 6; ++i)
+      if (!used[i]) free_slots[nf++] = i;
+    for (uint32_t e = 0; e < 8; ++e) {
+      uint32_t c = 0;
+      for (int b = 0; b < 3; ++b) c |= ((e >> b) & 1u) << vslot[b];
+      p.ce[j][e] = uint8_t(c);
     }
+    for (uint32_t m = 0; m < 4; ++m) p.cm[j][m] = uint8_t(((m & 1u) << free_slots[1]) | ((m >> 1) << free_slots[2]));
+    for (uint32_t w = 0; w < 2; ++w) p.cw[j][w] = uint8_t(w << free_slots[0]);
+    auto off_of = [&](uint32_t r, uint32_t c) {
+      const uint32_t d = d_of(j, pos_of(j - 1, r & 63u, c));
+      return b_off(km, (r >> 6) * 64u + (d >> 6), d & 63u);
+    };
+    for (uint32_t r = 0; r < 128; ++r) p.crow[j][r] = uint16_t(off_of(r, 0));
+    for (uint32_t w = 0; w < 2; ++w)
+      for (uint32_t m = 0; m < 4; ++m) p.cchunk[j][w][m] = uint16_t(off_of(0, uint32_t(p.cw[j][w]) | p.cm[j][m]));
   }
   // last matrix -> output staging at the permuted position, swizzled
+  p.evec = s.chain_evec ? 1u : 0u;
+  if (p.evec)
+    QSVB_REQUIRE(s.chain_perm[cols[nm - 1][0]] == 0 && s.chain_perm[cols[nm - 1][1]] == 1,
+                 "chain pass: vector epilogue needs the last matrix's columns 0, 1 on output bits 0, 1");
   uint32_t lane_pos[5];
   for (int b = 0; b < 5; ++b)
     lane_pos[b] = uint32_t(__builtin_ctz(permute12(1u << rows[nm - 1][b], s.chain_perm)));
-  staging_swizzle(lane_pos, p.sig_lo, p.sig_hi);
+  staging_swizzle(lane_pos, p.evec != 0, p.sig_lo, p.sig_hi);
   auto sig = [&](uint32_t t) { return uint32_t(p.sig_lo[t & 63u]) ^ p.sig_hi[t >> 6]; };
   for (uint32_t r = 0; r < 128; ++r)
     p.frow[r] =
@@ -864,18 +935,117 @@ uint32_t build_chain_params(const Sweep& s, uint32_t n, float* re, float* im, Ch
 
 }  // namespace
 
+// Operand layouts and orders of a pass (the planner has fixed its rows, columns and permutation):
+//  * the last matrix's columns 0, 1 are the positions the permutation sends to output bits 0, 1
+//    when both are its columns (vector epilogue; for a single matrix whose B is MN-major only if
+//    those are state bits 0, 1 themselves);
+//  * each later matrix j takes the B layout (MN- or K-major) whose contiguous bits can be three
+//    columns of matrix j - 1 (columns of both, or new rows of j: one set has at least three);
+//  * the three row bits of matrix j - 1 that select a converter lane within a 16-byte store phase
+//    go where they spread those stores over distinct bank groups;
+//  * matrix j's entries are permuted to its new row order (the column order is the kernel's own).
 void tc_chain_prepare(Sweep& s) {
   QSVB_REQUIRE(s.chain_nmat >= 1 && s.chain_nmat <= uint32_t(kChainMaxMats), "chain pass: 1..3 matrices");
-  for (uint32_t j = 0; j < s.chain_nmat; ++j)
+  const uint32_t nm = s.chain_nmat, L = nm - 1;
+  for (uint32_t j = 0; j < nm; ++j)
     QSVB_REQUIRE(s.chain_mats[j].size() == 64 * 64, "chain pass: matrices are 64 x 64");
-  for (uint32_t j = 1; j < s.chain_nmat; ++j) {
-    uint64_t rset = 0;
-    for (int i = 0; i < 6; ++i) rset |= 1ull << s.chain_rows[j][i];
+  uint8_t at_out[12];
+  for (int t = 0; t < 12; ++t) at_out[s.chain_perm[t]] = uint8_t(t);
+  const uint8_t q0 = at_out[0], q1 = at_out[1];
+  bool evec = !contains6(s.chain_rows[L], q0) && !contains6(s.chain_rows[L], q1);
+  const uint32_t bmode0 = first_bmode(s.chain_rows[0]);
+  if (evec && L == 0 && bmode0 == 0 && !(q0 == 0 && q1 == 1)) evec = false;
+  // first matrix: rows ascending; columns ascending, or [q0, q1, rest] for a vector epilogue
+  auto put_first = [](uint8_t (&a)[6], uint8_t x, uint8_t y) {
+    std::vector<uint8_t> rest;
+    for (int i = 0; i < 6; ++i)
+      if (a[i] != x && a[i] != y) rest.push_back(a[i]);
+    std::sort(rest.begin(), rest.end());
+    a[0] = x;
+    a[1] = y;
+    for (int i = 0; i < 4; ++i) a[2 + i] = rest[size_t(i)];
+  };
+  QSVB_REQUIRE(std::is_sorted(s.chain_rows[0], s.chain_rows[0] + 6), "chain pass: the first matrix's rows must ascend");
+  std::sort(s.chain_cols[0], s.chain_cols[0] + 6);
+  if (L == 0 && evec) put_first(s.chain_cols[0], q0, q1);
+  for (uint32_t j = 1; j < nm; ++j) {
+    const uint8_t(&pc)[6] = s.chain_cols[j - 1];
+    std::vector<uint8_t> both, newrows;  // columns of j - 1 that are columns / rows of j
+    for (int i = 0; i < 6; ++i) (contains6(s.chain_rows[j], pc[i]) ? newrows : both).push_back(pc[i]);
+    bool km;
+    std::vector<uint8_t> v;
+    const bool fix01 = j == L && evec;
+    if (fix01 && newrows.size() >= 3) {
+      km = true;
+      v.assign(newrows.begin(), newrows.begin() + 3);
+    } else if (fix01 && both.size() >= 3 && std::count(both.begin(), both.end(), q0) &&
+               std::count(both.begin(), both.end(), q1)) {
+      km = false;
+      v = {q0, q1};
+      for (uint8_t x : both)
+        if (x != q0 && x != q1 && v.size() < 3) v.push_back(x);
+    } else {
+      if (fix01) evec = false;
+      km = both.size() < 3;
+      const std::vector<uint8_t>& src = km ? newrows : both;
+      v.assign(src.begin(), src.begin() + 3);
+    }
+    // slot assignment: contiguous bits first, then the lane bits of matrix j - 1 (its rows 0..2) on
+    // the bits that pick the 16-byte bank group (K-major: row slots 3..5 and column slots 0..2;
+    // MN-major: column slots 3..5 and row slots 0..2), then the rest in ascending position
+    int rslot[12], cslot[12];
+    for (int t = 0; t < 12; ++t) rslot[t] = cslot[t] = -1;
+    bool rtaken[6] = {false}, ctaken[6] = {false};
+    auto place = [&](bool is_row, uint8_t pos, int slot) {
+      if (is_row) {
+        rslot[pos] = slot;
+        rtaken[slot] = true;
+      } else {
+        cslot[pos] = slot;
+        ctaken[slot] = true;
+      }
+    };
+    for (int b = 0; b < 3; ++b) place(km, v[size_t(b)], b);
+    if (j == L && evec && km) {  // the last matrix's columns 0, 1 for the vector epilogue
+      place(false, q0, 0);
+      place(false, q1, 1);
+    }
+    for (int b = 0; b < 3; ++b) {
+      const uint8_t pos = s.chain_rows[j - 1][b];
+      const bool is_row = contains6(s.chain_rows[j], pos);
+      if ((is_row ? rslot[pos] : cslot[pos]) >= 0) continue;
+      // the bank-group bits for this lane bit: index b, else any free one of the three
+      const int base = is_row ? (km ? 3 : 0) : (km ? 0 : 3);
+      bool* taken = is_row ? rtaken : ctaken;
+      int slot = -1;
+      for (int k = 0; k < 3 && slot < 0; ++k) {
+        const int cand = base + (b + k) % 3;
+        if (!taken[cand]) slot = cand;
+      }
+      if (slot >= 0) place(is_row, pos, slot);
+    }
     uint8_t nr[6], nc[6];
-    order_for_conversion(s.chain_rows[j - 1], rset, nr, nc);
+    {
+      std::vector<uint8_t> rest_r, rest_c;
+      for (int i = 0; i < 6; ++i) {
+        if (rslot[s.chain_rows[j][i]] < 0) rest_r.push_back(s.chain_rows[j][i]);
+        if (cslot[s.chain_cols[j][i]] < 0) rest_c.push_back(s.chain_cols[j][i]);
+      }
+      std::sort(rest_r.begin(), rest_r.end());
+      std::sort(rest_c.begin(), rest_c.end());
+      size_t kr = 0, kc = 0;
+      for (int i = 0; i < 6; ++i) {
+        if (!rtaken[i]) rslot[rest_r[kr++]] = i;
+        if (!ctaken[i]) cslot[rest_c[kc++]] = i;
+      }
+      for (int i = 0; i < 6; ++i) {
+        nr[rslot[s.chain_rows[j][i]]] = s.chain_rows[j][i];
+        nc[cslot[s.chain_cols[j][i]]] = s.chain_cols[j][i];
+      }
+    }
     // the matrix in the new row order: index bit i now means tile position nr[i]
     int from[6];
-    for (int i = 0; i < 6; ++i) from[i] = int(std::find(s.chain_rows[j], s.chain_rows[j] + 6, nr[i]) - s.chain_rows[j]);
+    for (int i = 0; i < 6; ++i) from[i] = index6(s.chain_rows[j], nr[i]);
     const std::vector<cd>& m = s.chain_mats[j];
     std::vector<cd> m2(64 * 64);
     for (uint32_t r = 0; r < 64; ++r)
@@ -890,7 +1060,9 @@ void tc_chain_prepare(Sweep& s) {
     s.chain_mats[j] = std::move(m2);
     std::copy(nr, nr + 6, s.chain_rows[j]);
     std::copy(nc, nc + 6, s.chain_cols[j]);
+    s.chain_bk[j] = km ? 1 : 0;
   }
+  s.chain_evec = evec ? 1 : 0;
 }
 
 size_t tc_chain_matrix_bytes(const Sweep& s) { return size_t(s.chain_nmat) * 2 * 128 * 128 * 2; }

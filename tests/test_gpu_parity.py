@@ -312,7 +312,8 @@ def test_qaoa_phase_sweeps_match_oracle(be, n):
     c = qaoa_maxcut(n, 3, 11 + n)
     st = be.alloc(n)
     be.init_basis(st, 0)
-    stats = be.run(st, c, opts(PLAN_LEARNED, 4))
+    # CUDA-core engine: the phase-polynomial sweep, not a tensor-core chain plan, is under test
+    stats = be.run(st, c, opts(PLAN_LEARNED, 4, ENGINE_CUDA_CORE))
     assert stats["by_kind"].get("phase", 0) >= 1, stats
     got = be.download(st).as_complex()
     err = max_abs_diff(ref_state(c), got)
