@@ -201,22 +201,45 @@ __device__ __forceinline__ void convert_first(const float* __restrict__ sre, con
   }
 }
 
-// Eight accumulator columns of this warp's 32 lanes, one column per load (addresses a0 + d[e]),
-// defined only once the loads have completed.
-__device__ __forceinline__ void tmem_ld_gather8(uint32_t a0, const uint32_t (&d)[8], uint32_t (&r)[8]) {
+// 32 accumulator columns of this warp's 32 lanes, one column per load (addresses a[k]), all in
+// flight at once, defined only once every load has completed.
+__device__ __forceinline__ void tmem_ld_gather32(const uint32_t (&a)[32], uint32_t (&r)[32]) {
   asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x1.b32 {%0}, [%8];\n\t"
-      "tcgen05.ld.sync.aligned.32x32b.x1.b32 {%1}, [%9];\n\t"
-      "tcgen05.ld.sync.aligned.32x32b.x1.b32 {%2}, [%10];\n\t"
-      "tcgen05.ld.sync.aligned.32x32b.x1.b32 {%3}, [%11];\n\t"
-      "tcgen05.ld.sync.aligned.32x32b.x1.b32 {%4}, [%12];\n\t"
-      "tcgen05.ld.sync.aligned.32x32b.x1.b32 {%5}, [%13];\n\t"
-      "tcgen05.ld.sync.aligned.32x32b.x1.b32 {%6}, [%14];\n\t"
-      "tcgen05.ld.sync.aligned.32x32b.x1.b32 {%7}, [%15];\n\t"
+      "tcgen05.ld.sync.aligned.32x32b.x1.b32 {%0}, [%32];\n\t"
+      "tcgen05.ld.sync.aligned.32x32b.x1.b32 {%1}, [%33];\n\t"
+      "tcgen05.ld.sync.aligned.32x32b.x1.b32 {%2}, [%34];\n\t"
+      "tcgen05.ld.sync.aligned.32x32b.x1.b32 {%3}, [%35];\n\t"
+      "tcgen05.ld.sync.aligned.32x32b.x1.b32 {%4}, [%36];\n\t"
+      "tcgen05.ld.sync.aligned.32x32b.x1.b32 {%5}, [%37];\n\t"
+      "tcgen05.ld.sync.aligned.32x32b.x1.b32 {%6}, [%38];\n\t"
+      "tcgen05.ld.sync.aligned.32x32b.x1.b32 {%7}, [%39];\n\t"
+      "tcgen05.ld.sync.aligned.32x32b.x1.b32 {%8}, [%40];\n\t"
+      "tcgen05.ld.sync.aligned.32x32b.x1.b32 {%9}, [%41];\n\t"
+      "tcgen05.ld.sync.aligned.32x32b.x1.b32 {%10}, [%42];\n\t"
+      "tcgen05.ld.sync.aligned.32x32b.x1.b32 {%11}, [%43];\n\t"
+      "tcgen05.ld.sync.aligned.32x32b.x1.b32 {%12}, [%44];\n\t"
+      "tcgen05.ld.sync.aligned.32x32b.x1.b32 {%13}, [%45];\n\t"
+      "tcgen05.ld.sync.aligned.32x32b.x1.b32 {%14}, [%46];\n\t"
+      "tcgen05.ld.sync.aligned.32x32b.x1.b32 {%15}, [%47];\n\t"
+      "tcgen05.ld.sync.aligned.32x32b.x1.b32 {%16}, [%48];\n\t"
+      "tcgen05.ld.sync.aligned.32x32b.x1.b32 {%17}, [%49];\n\t"
+      "tcgen05.ld.sync.aligned.32x32b.x1.b32 {%18}, [%50];\n\t"
+      "tcgen05.ld.sync.aligned.32x32b.x1.b32 {%19}, [%51];\n\t"
+      "tcgen05.ld.sync.aligned.32x32b.x1.b32 {%20}, [%52];\n\t"
+      "tcgen05.ld.sync.aligned.32x32b.x1.b32 {%21}, [%53];\n\t"
+      "tcgen05.ld.sync.aligned.32x32b.x1.b32 {%22}, [%54];\n\t"
+      "tcgen05.ld.sync.aligned.32x32b.x1.b32 {%23}, [%55];\n\t"
+      "tcgen05.ld.sync.aligned.32x32b.x1.b32 {%24}, [%56];\n\t"
+      "tcgen05.ld.sync.aligned.32x32b.x1.b32 {%25}, [%57];\n\t"
+      "tcgen05.ld.sync.aligned.32x32b.x1.b32 {%26}, [%58];\n\t"
+      "tcgen05.ld.sync.aligned.32x32b.x1.b32 {%27}, [%59];\n\t"
+      "tcgen05.ld.sync.aligned.32x32b.x1.b32 {%28}, [%60];\n\t"
+      "tcgen05.ld.sync.aligned.32x32b.x1.b32 {%29}, [%61];\n\t"
+      "tcgen05.ld.sync.aligned.32x32b.x1.b32 {%30}, [%62];\n\t"
+      "tcgen05.ld.sync.aligned.32x32b.x1.b32 {%31}, [%63];\n\t"
       "tcgen05.wait::ld.sync.aligned;\n"
-      : "=&r"(r[0]), "=&r"(r[1]), "=&r"(r[2]), "=&r"(r[3]), "=&r"(r[4]), "=&r"(r[5]), "=&r"(r[6]), "=&r"(r[7])
-      : "r"(a0 + d[0]), "r"(a0 + d[1]), "r"(a0 + d[2]), "r"(a0 + d[3]), "r"(a0 + d[4]), "r"(a0 + d[5]),
-        "r"(a0 + d[6]), "r"(a0 + d[7])
+      : "=&r"(r[0]), "=&r"(r[1]), "=&r"(r[2]), "=&r"(r[3]), "=&r"(r[4]), "=&r"(r[5]), "=&r"(r[6]), "=&r"(r[7]), "=&r"(r[8]), "=&r"(r[9]), "=&r"(r[10]), "=&r"(r[11]), "=&r"(r[12]), "=&r"(r[13]), "=&r"(r[14]), "=&r"(r[15]), "=&r"(r[16]), "=&r"(r[17]), "=&r"(r[18]), "=&r"(r[19]), "=&r"(r[20]), "=&r"(r[21]), "=&r"(r[22]), "=&r"(r[23]), "=&r"(r[24]), "=&r"(r[25]), "=&r"(r[26]), "=&r"(r[27]), "=&r"(r[28]), "=&r"(r[29]), "=&r"(r[30]), "=&r"(r[31])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(a[4]), "r"(a[5]), "r"(a[6]), "r"(a[7]), "r"(a[8]), "r"(a[9]), "r"(a[10]), "r"(a[11]), "r"(a[12]), "r"(a[13]), "r"(a[14]), "r"(a[15]), "r"(a[16]), "r"(a[17]), "r"(a[18]), "r"(a[19]), "r"(a[20]), "r"(a[21]), "r"(a[22]), "r"(a[23]), "r"(a[24]), "r"(a[25]), "r"(a[26]), "r"(a[27]), "r"(a[28]), "r"(a[29]), "r"(a[30]), "r"(a[31])
       : "memory");
 }
 
@@ -235,13 +258,17 @@ __device__ __forceinline__ void split2(uint32_t x0, uint32_t x1, uint32_t& hi, u
 __device__ __forceinline__ void convert_next(uint32_t tcol, uint32_t rbase, const uint32_t (&cc)[4],
                                              const uint32_t (&cm)[4], const uint32_t (&ce)[8],
                                              uint8_t* __restrict__ b_hi, uint8_t* __restrict__ b_lo) {
+  uint32_t a[32], v[32];
+#pragma unroll
+  for (int m = 0; m < 4; ++m)
+#pragma unroll
+    for (int e = 0; e < 8; ++e) a[8 * m + e] = tcol + cm[m] + ce[e];
+  tmem_ld_gather32(a, v);
 #pragma unroll
   for (int m = 0; m < 4; ++m) {
-    uint32_t v[8];
-    tmem_ld_gather8(tcol + cm[m], ce, v);
     uint32_t h[4], l[4];
 #pragma unroll
-    for (int i = 0; i < 4; ++i) split2(v[2 * i], v[2 * i + 1], h[i], l[i]);
+    for (int i = 0; i < 4; ++i) split2(v[8 * m + 2 * i], v[8 * m + 2 * i + 1], h[i], l[i]);
     const uint32_t off = rbase ^ cc[m];
     const uint32_t sh = smem_u32(b_hi + off), sl = smem_u32(b_lo + off);
     asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(sh), "r"(h[0]), "r"(h[1]), "r"(h[2]), "r"(h[3])

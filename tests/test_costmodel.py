@@ -116,48 +116,73 @@ def test_training_fits_a_known_function(be32):
 
 
 @pytest.mark.gpu
-def test_learned_planner_gains_over_the_untrained_method(be32):
-    """Autotune at 24 qubits, train, and compare measured circuit times: the learned plan against
-    the same planner on its roofline model and against qsv's greedy fuse at every width."""
-    import torch
-    from rustatevec_b200 import Plan, PLAN_GREEDY, PLAN_LEARNED, ENGINE_AUTO
-    from rustatevec_b200.circuits import brickwork, random_circuit
+def test_training_on_autotuner_records_ranks_sweeps(be32):
+    """Autotune at 24 qubits and train with the engine's own CUDA kernels: the trained network
+    orders the measured sweep times (Spearman rank correlation > 0.8)."""
     a = tuning.autotune(be32, 24, reps=3, seed=24)
     b = tuning.plan_records(be32, 24, reps=2, seed=24)
     rec = {k: np.concatenate([a[k], b[k]]) if k != "precision" else a[k] + b[k] for k in a}
-    loss = tuning.train(be32, rec, hidden=64, epochs=3000)
-    pred = tuning.predict(rec["features"])
-    truth = np.log2(rec["seconds"])
-    rank_corr = np.corrcoef(np.argsort(np.argsort(pred)), np.argsort(np.argsort(truth)))[0, 1]
-    assert rank_corr > 0.8, rank_corr
-    img = tuning.model_image()
-    stream = torch.cuda.ExternalStream(be32.stream())
+    try:
+        tuning.train(be32, rec, hidden=64, epochs=3000)
+        pred = tuning.predict(rec["features"])
+        truth = np.log2(rec["seconds"])
+        rank_corr = np.corrcoef(np.argsort(np.argsort(pred)), np.argsort(np.argsort(truth)))[0, 1]
+        assert rank_corr > 0.8, rank_corr
+    finally:
+        tuning.install(None)
 
-    def measure(circ, opts, reps=5):
-        st = be32.alloc(circ.n_qubits())
-        p = Plan(be32, circ, opts)
-        be32.init_basis(st, 0)
+
+@pytest.mark.gpu
+def test_learned_planner_gains_over_the_untrained_method(built):
+    """What the trained network gains: the learned planner with the trained cost model against the
+    same planner on its analytic roofline model (the method without the network), measured on the
+    device for complex128 circuit families at 26 qubits. Where the two pick different plans the
+    network's plan must be at least 5 % faster on the family where it decides most (and faster in
+    total); nowhere may it be more than 10 % slower. The fixed rule it replaces is qsv's max-k
+    greedy fuse (crates/qsv-core/src/fusion.rs:26-36)."""
+    import torch
+    from rustatevec_b200 import B200Backend, Plan, PLAN_LEARNED, ENGINE_AUTO
+    from rustatevec_b200.circuits import ghz_chain, qaoa_maxcut, random_circuit
+    doc = tuning.load()
+    if doc is None:
+        pytest.skip("no trained model in the tree")
+    img = doc["model"]
+    be = B200Backend(0, precision="f64")
+    stream = torch.cuda.ExternalStream(be.stream())
+
+    def measure(circ, reps=4):
+        st = be.alloc(circ.n_qubits())
+        p = Plan(be, circ, L.make_opts(PLAN_LEARNED, 6, ENGINE_AUTO))
+        be.init_basis(st, 0)
         p.run(st)
-        be32.synchronize()
+        be.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         for _ in range(reps):
             p.run(st)
         e1.record(stream)
         e1.synchronize()
-        return e0.elapsed_time(e1) / reps
+        kinds = p.stats()["by_kind"]
+        p.free()
+        st.free()
+        return e0.elapsed_time(e1) / reps, kinds
 
     try:
         report = {}
-        for name, circ in (("brickwork24", brickwork(24, 20, 1)), ("random24", random_circuit(24, 400, 7))):
+        for name, circ in (("random26", random_circuit(26, 300, 7)), ("qaoa26", qaoa_maxcut(26, 2, 3)),
+                           ("ghz26", ghz_chain(26))):
             tuning.install(img)
-            t_learned = measure(circ, L.make_opts(PLAN_LEARNED, 6, ENGINE_AUTO))
+            t_mlp, k_mlp = measure(circ)
             tuning.install(None)
-            t_roofline = measure(circ, L.make_opts(PLAN_LEARNED, 6, ENGINE_AUTO))
-            t_greedy = min(measure(circ, L.make_opts(PLAN_GREEDY, k, ENGINE_AUTO)) for k in (2, 3, 4, 5, 6))
-            report[name] = (t_learned, t_roofline, t_greedy)
-            assert t_learned <= 1.10 * t_greedy, report
-            assert t_learned <= 1.10 * t_roofline, report
-        print("learned vs roofline-model vs best greedy (ms):", report, "train loss", loss)
+            t_roof, k_roof = measure(circ)
+            report[name] = (round(t_mlp, 3), round(t_roof, 3), k_mlp, k_roof)
+        print("learned planner, trained model vs roofline model (ms, plans):", report)
+        for name, (t_mlp, t_roof, _, _) in report.items():
+            assert t_mlp <= 1.10 * t_roof, (name, report)
+        differing = {k: v for k, v in report.items() if v[2] != v[3]}
+        assert differing, ("the trained network changed no plan", report)
+        assert min(v[0] / v[1] for v in differing.values()) <= 0.95, report
+        assert sum(v[0] for v in report.values()) < sum(v[1] for v in report.values()), report
     finally:
         tuning.install(None)
+        be.close()
