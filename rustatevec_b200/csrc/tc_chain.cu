@@ -10,28 +10,31 @@
 // as the single-matrix sweep (tc_dense.cu) does.
 //
 // One persistent CTA per SM, warp-specialised:
-//   producer warp: one tiled TMA or bulk copies per component of each tile into one of four fp32
-//     input slots (address order);
+//   producer warp: one tiled TMA or bulk copies per component of each tile into one of four (three)
+//     fp32 input slots (address order);
 //   converter warps (8): for a tile's first matrix, split the staged fp32 tile into the bf16 hi/lo
-//     B operand (one of two B buffers; layout chosen by which matrix qubits are state bits 0, 1);
-//     for every later matrix, gather 32 of the previous matrix's accumulator columns straight from
-//     tensor memory (each warp its lane quadrant, one column per load, in the order the next
+//     B operand (one of two (three) B buffers; layout chosen by which matrix qubits are state bits
+//     0, 1); for every later matrix, gather 32 of the previous matrix's accumulator columns straight
+//     from tensor memory (each warp its lane quadrant, one column per load, in the order the next
 //     operand needs), split them and write them into the next B operand as 16-byte chunks of 8
 //     bf16: the operand is MN- or K-major, whichever has three of its contiguous bits among the
 //     previous matrix's columns (one of the two always does); chunk offsets are an XOR of a per-row
-//     and a per-chunk part, both precomputed on the host;
-//   MMA warp (one lane): 24 tcgen05.mma per matrix into one of two accumulators (64 columns each),
-//     the A operand (Whi, Wlo of matrix j) resident in tensor memory for the whole kernel;
+//     and a per-chunk part, both precomputed on the host; the hi/lo splits convert two values per
+//     instruction (packed bf16x2);
+//   MMA warps (one per B buffer, one lane each): 24 tcgen05.mma per matrix into the tile's
+//     accumulator (64 columns), the A operand (Whi, Wlo of matrix j) resident in tensor memory for
+//     the whole kernel; one thread issues a tcgen05.mma only every ~80 cycles while an N = 64 MMA
+//     occupies the tensor pipe ~32 cycles, so several items' MMAs are issued concurrently;
 //   epilogue warps (4): after the last matrix, read the accumulator, stage it in shared memory in
 //     the permuted address order (16-byte stores when the pass's permutation puts the last matrix's
 //     first two columns on output bits 0 and 1, which the planner arranges; scalar stores
 //     otherwise; a per-pass XOR swizzle keeps both the staging writes and the write-back's reads
 //     bank-conflict free) and write the tile back with 16-byte stores.
-// Work items are (tile, matrix) pairs. Two tiles are in flight at a time, and every role walks the
-// same item order: matrix 0 of tiles a and b, matrix 1 of tiles a and b, ..., so the MMA of one
-// tile overlaps the conversion of the other. Every item depends only on earlier items, so the
-// pipeline cannot deadlock; every mbarrier wait is bounded (a wait that runs out sets the context
-// error flag, the role stops and the host reports QSVB_E_TIMEOUT). No load uses cluster multicast.
+// Work items are (tile, matrix) pairs, walked by every role in the same order (walk_items). Up to
+// two matrices, four tiles are in flight (four accumulators, three B buffers, three MMA warps);
+// three matrices leave tensor memory for two accumulators, so two tiles are (two B buffers, two
+// MMA warps). Every mbarrier wait is bounded (a wait that runs out sets the context error flag,
+// the role stops and the host reports QSVB_E_TIMEOUT). No load uses cluster multicast.
 //
 // k_permute_tiles applies only a tile-qubit permutation (no arithmetic): the planner uses it to put
 // every qubit back on its own state bit after a run of chain passes.
@@ -61,22 +64,25 @@ constexpr int kEpiWarps = 4;
 constexpr int kCvtThreads = kCvtWarps * 32;
 constexpr int kEpiThreads = kEpiWarps * 32;
 constexpr int kProdWarp = kCvtWarps;       // warp 8
-constexpr int kMmaWarp = kCvtWarps + 1;    // warp 9
-constexpr int kEpiWarp0 = kCvtWarps + 2;   // warps 10..13
-constexpr int kThreads = (kCvtWarps + 2 + kEpiWarps) * 32;
-constexpr int kBSlots = 2;
-constexpr int kIoSlots = 4;
-constexpr int kWave = 2;                   // tiles in flight through the matrix stages
-constexpr int kTmemCols = 512;             // 2 accumulators (64 columns) + 3 x (Whi, Wlo) (64 each)
-constexpr uint32_t kTmemA0 = 128;          // matrix j: Whi at kTmemA0 + 128 j, Wlo 64 columns later
+constexpr int kMmaWarp = kCvtWarps + 1;    // warps 9..11: the MMAs of the items of B buffer 0, 1, 2
+constexpr int kMmaWarps = 3;
+constexpr int kEpiWarp0 = kMmaWarp + kMmaWarps;  // warps 12..15 (lane quadrants 0..3)
+constexpr int kThreads = (kEpiWarp0 + kEpiWarps) * 32;
+constexpr int kTmemCols = 512;             // DEPTH accumulators (64 columns) + (Whi, Wlo) of each matrix
+// Two configurations of the same kernel (template parameter DEPTH = accumulators = tiles in flight):
+//   DEPTH 2 (up to three matrices): 2 B buffers, 4 input slots, matrix j's Whi at column 128 + 128 j;
+//   DEPTH 4 (one or two matrices):  3 B buffers, 3 input slots, matrix j's Whi at column 256 + 128 j.
+// Both use the same shared memory: 2 x 2 + 5 = 3 x 2 + 4 buffers of 32 KB.
+constexpr int kBarBase = 26;               // iofull[4] ioempty[4] bfull[3] bfree[3] dfull_c[4] dfull_e[4] dfree[4]
 constexpr uint32_t kBBytes = 128u * 64u * 2u;  // one of Xhi / Xlo: K = 128 rows x N = 64 bf16
 constexpr uint32_t kIoBytes = kTileAmps * 8u;
 constexpr int kVC = kTileAmps / 4 / kCvtThreads;   // float4 per component per converter thread
 constexpr int kVE = kTileAmps / 4 / kEpiThreads;   // float4 per component per epilogue thread
-constexpr size_t kChainSmem = 1024 + kBSlots * 2 * size_t(kBBytes) + (kIoSlots + 1) * size_t(kIoBytes) +
-                              20 * 8 + 8 + 64 * 8 + 64 * 2 * 2 + 64 * 2 + 128 * 2;
+constexpr size_t kChainSmem = 1024 + 2 * 2 * size_t(kBBytes) + 5 * size_t(kIoBytes) + kBarBase * 8 + 8 + 64 * 8 +
+                              64 * 2 * 2 + 64 * 2 + 128 * 2;
+static_assert(2 * 2 * kBBytes + 5 * kIoBytes == 3 * 2 * kBBytes + 4 * kIoBytes, "chain pass: buffer budget");
 static_assert(kChainSmem <= 232448, "chain pass: shared memory above the 227 KB per-block limit");
-static_assert(kChainMaxMats * 128 + 128 <= kTmemCols, "chain pass: tensor memory");
+static_assert(kChainMaxMats * 128 + 2 * 64 <= kTmemCols && 2 * 128 + 4 * 64 <= kTmemCols, "chain pass: tensor memory");
 
 struct ChainParams {
   // tile addressing (tile_layout)
@@ -105,6 +111,20 @@ struct ChainParams {
   // sig_lo[t & 63] ^ sig_hi[t >> 6]
   uint16_t sig_lo[64], sig_hi[64];
 };
+
+// bf16 hi/lo split of two values, packed as bf16 pairs (the first value in the low half).
+__device__ __forceinline__ void split2(uint32_t x0, uint32_t x1, uint32_t& hi, uint32_t& lo) {
+  const float2 f = make_float2(__uint_as_float(x0), __uint_as_float(x1));
+  const __nv_bfloat162 h = __float22bfloat162_rn(f);
+  const float2 hf = __bfloat1622float2(h);
+  const __nv_bfloat162 l = __float22bfloat162_rn(make_float2(f.x - hf.x, f.y - hf.y));
+  hi = *reinterpret_cast<const uint32_t*>(&h);
+  lo = *reinterpret_cast<const uint32_t*>(&l);
+}
+
+__device__ __forceinline__ void split2f(float x0, float x1, uint32_t& hi, uint32_t& lo) {
+  split2(__float_as_uint(x0), __float_as_uint(x1), hi, lo);
+}
 
 // B layout of the first matrix (as in tc_dense.cu): 0 MN-major (state bits 0, 1 are columns),
 // 1 K-major vectors (they are the matrix's rows 0, 1), 2 K-major row pairs (exactly one is a row,
@@ -150,16 +170,15 @@ __device__ __forceinline__ void convert_first(const float* __restrict__ sre, con
       const uint32_t d = uint32_t(s_dlo[tg & 63]) + s_dhi[tg >> 6];
       const uint32_t s = d >> NCB, c = d & CMASK;
       const uint32_t o_re = kmaj_off(c, s, 64), o_im = kmaj_off(c, M2 + s, 64);
-      __nv_bfloat16 hr[4], lr[4], hm[4], lm[4];
-#pragma unroll
-      for (int e = 0; e < 4; ++e) {
-        split_bf16(wr[e], hr[e], lr[e]);
-        split_bf16(wi[e], hm[e], lm[e]);
-      }
-      *reinterpret_cast<uint2*>(b_hi + o_re) = pack4(hr);
-      *reinterpret_cast<uint2*>(b_lo + o_re) = pack4(lr);
-      *reinterpret_cast<uint2*>(b_hi + o_im) = pack4(hm);
-      *reinterpret_cast<uint2*>(b_lo + o_im) = pack4(lm);
+      uint2 hr, lr, hm, lm;
+      split2f(wr[0], wr[1], hr.x, lr.x);
+      split2f(wr[2], wr[3], hr.y, lr.y);
+      split2f(wi[0], wi[1], hm.x, lm.x);
+      split2f(wi[2], wi[3], hm.y, lm.y);
+      *reinterpret_cast<uint2*>(b_hi + o_re) = hr;
+      *reinterpret_cast<uint2*>(b_lo + o_re) = lr;
+      *reinterpret_cast<uint2*>(b_hi + o_im) = hm;
+      *reinterpret_cast<uint2*>(b_lo + o_im) = lm;
     } else if constexpr (BM == 2) {
       const int step = p.b2_bit0 ? 1 : 2;
 #pragma unroll
@@ -168,35 +187,28 @@ __device__ __forceinline__ void convert_first(const float* __restrict__ sre, con
         const uint32_t d = uint32_t(s_dlo[tlo + e]) + s_dhi[thi];
         const uint32_t s = d >> NCB, c = d & CMASK;
         const uint32_t o_re = kmaj_off(c, s, 64), o_im = kmaj_off(c, M2 + s, 64);
-        __nv_bfloat16 h0, l0, h1, l1;
-        split_bf16(vr[e], h0, l0);
-        split_bf16(vr[e + step], h1, l1);
-        *reinterpret_cast<uint32_t*>(b_hi + o_re) =
-            uint32_t(__bfloat16_as_ushort(h0)) | (uint32_t(__bfloat16_as_ushort(h1)) << 16);
-        *reinterpret_cast<uint32_t*>(b_lo + o_re) =
-            uint32_t(__bfloat16_as_ushort(l0)) | (uint32_t(__bfloat16_as_ushort(l1)) << 16);
-        split_bf16(vi[e], h0, l0);
-        split_bf16(vi[e + step], h1, l1);
-        *reinterpret_cast<uint32_t*>(b_hi + o_im) =
-            uint32_t(__bfloat16_as_ushort(h0)) | (uint32_t(__bfloat16_as_ushort(h1)) << 16);
-        *reinterpret_cast<uint32_t*>(b_lo + o_im) =
-            uint32_t(__bfloat16_as_ushort(l0)) | (uint32_t(__bfloat16_as_ushort(l1)) << 16);
+        uint32_t h, l;
+        split2f(vr[e], vr[e + step], h, l);
+        *reinterpret_cast<uint32_t*>(b_hi + o_re) = h;
+        *reinterpret_cast<uint32_t*>(b_lo + o_re) = l;
+        split2f(vi[e], vi[e + step], h, l);
+        *reinterpret_cast<uint32_t*>(b_hi + o_im) = h;
+        *reinterpret_cast<uint32_t*>(b_lo + o_im) = l;
       }
     } else {
       const uint32_t d = dda[j];
       const uint32_t s = d >> NCB, c = d & CMASK;
       const uint32_t o_re = b_mn ? mnmaj_off(s, c) : kmaj_off(c, s, 64);
       const uint32_t o_im = b_mn ? mnmaj_off(M2 + s, c) : kmaj_off(c, M2 + s, 64);
-      __nv_bfloat16 hr[4], lr[4], hm[4], lm[4];
-#pragma unroll
-      for (int e = 0; e < 4; ++e) {
-        split_bf16(vr[e], hr[e], lr[e]);
-        split_bf16(vi[e], hm[e], lm[e]);
-      }
-      *reinterpret_cast<uint2*>(b_hi + o_re) = pack4(hr);
-      *reinterpret_cast<uint2*>(b_lo + o_re) = pack4(lr);
-      *reinterpret_cast<uint2*>(b_hi + o_im) = pack4(hm);
-      *reinterpret_cast<uint2*>(b_lo + o_im) = pack4(lm);
+      uint2 hr, lr, hm, lm;
+      split2f(xr.x, xr.y, hr.x, lr.x);
+      split2f(xr.z, xr.w, hr.y, lr.y);
+      split2f(xi.x, xi.y, hm.x, lm.x);
+      split2f(xi.z, xi.w, hm.y, lm.y);
+      *reinterpret_cast<uint2*>(b_hi + o_re) = hr;
+      *reinterpret_cast<uint2*>(b_lo + o_re) = lr;
+      *reinterpret_cast<uint2*>(b_hi + o_im) = hm;
+      *reinterpret_cast<uint2*>(b_lo + o_im) = lm;
     }
   }
 }
@@ -243,16 +255,6 @@ __device__ __forceinline__ void tmem_ld_gather32(const uint32_t (&a)[32], uint32
       : "memory");
 }
 
-// bf16 hi/lo split of two values, packed as bf16 pairs (the first value in the low half).
-__device__ __forceinline__ void split2(uint32_t x0, uint32_t x1, uint32_t& hi, uint32_t& lo) {
-  const float2 f = make_float2(__uint_as_float(x0), __uint_as_float(x1));
-  const __nv_bfloat162 h = __float22bfloat162_rn(f);
-  const float2 hf = __bfloat1622float2(h);
-  const __nv_bfloat162 l = __float22bfloat162_rn(make_float2(f.x - hf.x, f.y - hf.y));
-  hi = *reinterpret_cast<const uint32_t*>(&h);
-  lo = *reinterpret_cast<const uint32_t*>(&l);
-}
-
 // Matrix j >= 1: the accumulator of matrix j - 1 (its TMEM columns from tcol, this thread's row
 // offset rbase) into the B operand of matrix j, as four 16-byte chunks of hi and of lo.
 __device__ __forceinline__ void convert_next(uint32_t tcol, uint32_t rbase, const uint32_t (&cc)[4],
@@ -278,30 +280,66 @@ __device__ __forceinline__ void convert_next(uint32_t tcol, uint32_t rbase, cons
   }
 }
 
-template <int BM>
+// The order in which every role walks the work items (tile k, matrix j). Item i uses B buffer
+// i % NB and accumulator k % DEPTH.
+//   DEPTH 2: waves of two tiles: matrix 0 of both, then matrix 1 of both, ... (the MMA of one tile
+//     overlaps the conversion of the other);
+//   DEPTH 4: a skewed stream: step s holds matrix 0 of tile s, then matrix 1 of tile s - 2, so two
+//     other conversions separate a tile's two conversions (covering its first MMA) and the staged
+//     tiles are consumed one per two items, evenly.
+// Every item depends only on earlier items of the same walk (its previous matrix, its B buffer's
+// previous item, the tile that last held its accumulator), so the pipeline cannot deadlock.
+// f(k, j, i) returns false to stop the walk.
+template <int DEPTH, class F>
+__device__ __forceinline__ void walk_items(uint32_t ntiles, uint32_t nmat, F&& f) {
+  uint32_t i = 0;
+  if constexpr (DEPTH == 2) {
+    for (uint32_t w0 = 0; w0 < ntiles; w0 += 2) {
+      const uint32_t nt = ntiles - w0 < 2u ? ntiles - w0 : 2u;
+      for (uint32_t j = 0; j < nmat; ++j)
+        for (uint32_t tt = 0; tt < nt; ++tt, ++i)
+          if (!f(w0 + tt, j, i)) return;
+    }
+  } else {
+    constexpr uint32_t L = 2;
+    const uint32_t steps = ntiles + (nmat - 1) * L;
+    for (uint32_t st = 0; st < steps; ++st)
+      for (uint32_t j = 0; j < nmat; ++j) {
+        if (st < j * L || st - j * L >= ntiles) continue;
+        if (!f(st - j * L, j, i)) return;
+        ++i;
+      }
+  }
+}
+
+template <int BM, int DEPTH>
 __global__ void __launch_bounds__(kThreads, 1) k_tc_chain(float* __restrict__ re, float* __restrict__ im,
                                                           uint64_t ntiles, const uint4* __restrict__ wpack,
                                                           const __grid_constant__ ChainParams p, int* err,
                                                           const __grid_constant__ CUtensorMap tm_re,
                                                           const __grid_constant__ CUtensorMap tm_im) {
+  constexpr int NB = DEPTH == 2 ? 2 : 3;       // B buffers (one MMA warp each)
+  constexpr int NIO = DEPTH == 2 ? 4 : 3;      // input slots
+  constexpr uint32_t A0 = 64u * DEPTH;         // tensor-memory column of matrix 0's Whi
+  static_assert(A0 + 128u * (DEPTH == 2 ? 3u : 2u) <= uint32_t(kTmemCols), "chain pass: tensor memory");
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  uint8_t* bbuf = smem;                                                    // slot s: hi, then lo
-  float* io = reinterpret_cast<float*>(bbuf + kBSlots * 2 * kBBytes);      // slot s: re [4096], im [4096]
-  float* ostage = io + kIoSlots * 2 * kTileAmps;                           // the epilogue's result
+  uint8_t* bbuf = smem;                                               // buffer b: hi, then lo
+  float* io = reinterpret_cast<float*>(bbuf + NB * 2 * kBBytes);      // slot s: re [4096], im [4096]
+  float* ostage = io + NIO * 2 * kTileAmps;                           // the epilogue's result
   uint64_t* bars = reinterpret_cast<uint64_t*>(ostage + 2 * kTileAmps);
-  uint64_t* iofull = bars;        // [4] TMA complete_tx -> converters
-  uint64_t* ioempty = bars + 4;   // [4] converters -> producer
-  uint64_t* bfull = bars + 8;     // [2] converters -> MMA
-  uint64_t* bfree = bars + 10;    // [2] MMA commit -> converters
+  uint64_t* iofull = bars;        // [NIO] TMA complete_tx -> converters
+  uint64_t* ioempty = bars + 4;   // [NIO] converters -> producer
+  uint64_t* bfull = bars + 8;     // [NB] converters -> MMA
+  uint64_t* bfree = bars + 11;    // [NB] MMA commit -> converters
   // accumulators: each barrier has one consumer role that waits on every one of its phases in
   // order (a parity wait cannot tell a completion from the one two phases later, so no role may
   // skip phases that belong to another)
-  uint64_t* dfull_c = bars + 12;  // [2] MMA commit -> converters (accumulators of matrices 0..nmat-2)
-  uint64_t* dfull_e = bars + 14;  // [2] MMA commit -> epilogue (accumulators of the last matrix)
-  uint64_t* dfree = bars + 16;    // [2] accumulator read -> MMA
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 20);
-  uint64_t* s_hioff = reinterpret_cast<uint64_t*>(bars + 21);
+  uint64_t* dfull_c = bars + 14;  // [DEPTH] MMA commit -> converters (accumulators of matrices 0..nmat-2)
+  uint64_t* dfull_e = bars + 18;  // [DEPTH] MMA commit -> epilogue (accumulators of the last matrix)
+  uint64_t* dfree = bars + 22;    // [DEPTH] accumulator read -> MMA
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + kBarBase);
+  uint64_t* s_hioff = reinterpret_cast<uint64_t*>(bars + kBarBase + 1);
   uint16_t* s_dlo = reinterpret_cast<uint16_t*>(s_hioff + 64);
   uint16_t* s_dhi = s_dlo + 64;
   uint16_t* s_tperm = s_dhi + 64;   // tplo [32], tphi [32]
@@ -326,13 +364,15 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_chain(float* __restrict__ re
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   if (tid == 0) {
-    for (int s = 0; s < kIoSlots; ++s) {
+    for (int s = 0; s < NIO; ++s) {
       mbar_init(&iofull[s], 1);
       mbar_init(&ioempty[s], kCvtThreads);
     }
-    for (int s = 0; s < 2; ++s) {
+    for (int s = 0; s < NB; ++s) {
       mbar_init(&bfull[s], kCvtThreads);
       mbar_init(&bfree[s], 1);
+    }
+    for (int s = 0; s < DEPTH; ++s) {
       mbar_init(&dfull_c[s], 1);
       mbar_init(&dfull_e[s], 1);
       // every converter thread (count 1) or every epilogue thread (count 2) once it has read the
@@ -363,7 +403,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_chain(float* __restrict__ re
           r[4 * q + 2] = u.z;
           r[4 * q + 3] = u.w;
         }
-        tmem_st64(tmem + ((quad * 32) << 16) + kTmemA0 + 128u * j + 64u * uint32_t(h), r);
+        tmem_st64(tmem + ((quad * 32) << 16) + A0 + 128u * j + 64u * uint32_t(h), r);
       }
     asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
   }
@@ -381,13 +421,14 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_chain(float* __restrict__ re
     }
     return base;
   };
-  const uint64_t my_tiles = uint64_t(blockIdx.x) < ntiles ? (ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+  const uint32_t my_tiles =
+      uint64_t(blockIdx.x) < ntiles ? uint32_t((ntiles - 1 - blockIdx.x) / gridDim.x + 1) : 0u;
 
   if (warp == kProdWarp) {
     // ============================ producer: the tile's runs into an input slot (address order)
     const uint32_t rb = p.runbits, nruns = uint32_t(kTileAmps) >> rb, run_bytes = 4u << rb;
-    for (uint64_t i = 0; i < my_tiles; ++i) {
-      const uint32_t slot = uint32_t(i % kIoSlots), par = uint32_t((i / kIoSlots) & 1);
+    for (uint32_t i = 0; i < my_tiles; ++i) {
+      const uint32_t slot = i % NIO, par = (i / NIO) & 1u;
       bool ok = true;
       if (lane == 0) {
         ok = mbar_wait(&ioempty[slot], par ^ 1u);
@@ -396,7 +437,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_chain(float* __restrict__ re
       }
       ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
       if (!ok) break;
-      const uint64_t base = tile_base(blockIdx.x + i * gridDim.x);
+      const uint64_t base = tile_base(blockIdx.x + uint64_t(i) * gridDim.x);
       float* dre = io + slot * 2 * kTileAmps;
       float* dim_ = dre + kTileAmps;
       if (p.tm_rank > 0) {
@@ -425,94 +466,93 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_chain(float* __restrict__ re
     if (nmat > 1) rb1 = p.crow[1][row];
     if (nmat > 2) rb2 = p.crow[2][row];
     const uint32_t lane_base = tmem + ((quad * 32) << 16);
-    uint32_t g = 0;
-    uint32_t cph[2] = {0, 0};  // accumulators of each slot consumed so far (phases of dfull_c)
-    bool stop = false;
-    for (uint64_t w0 = 0; w0 < my_tiles && !stop; w0 += kWave) {
-      const uint32_t nt = my_tiles - w0 < uint64_t(kWave) ? uint32_t(my_tiles - w0) : uint32_t(kWave);
-      for (uint32_t j = 0; j < nmat && !stop; ++j)
-        for (uint32_t tt = 0; tt < nt; ++tt, ++g) {
-          const uint64_t i = w0 + tt;
-          const uint32_t slot = uint32_t(i % kIoSlots);
-          const uint32_t bs = g & 1u, bpar = (g >> 1) & 1u;
-          // the input: the staged tile (matrix 0) or the accumulator of this tile's previous
-          // matrix, which the MMA wrote for item g - nt; the converters consume every
-          // intermediate accumulator, slot by slot in item order
-          const uint32_t ds = (g - nt) & 1u;
-          bool ready = j == 0 ? mbar_wait(&iofull[slot], uint32_t((i / kIoSlots) & 1))
-                              : mbar_wait(&dfull_c[ds], cph[ds] & 1u);
-          if (j > 0) ++cph[ds];
-          ready = ready && mbar_wait(&bfree[bs], bpar ^ 1u);
-          if (!__all_sync(0xffffffffu, ready)) {
-            atomicExch(err, 1);
-            stop = true;
-            break;
-          }
-          uint8_t* b_hi = bbuf + bs * 2 * kBBytes;
-          uint8_t* b_lo = b_hi + kBBytes;
-          if (j == 0) {
-            const float* sre = io + slot * 2 * kTileAmps;
-            convert_first<BM>(sre, sre + kTileAmps, b_hi, b_lo, s_dlo, s_dhi, s_tperm, p, tid, lane);
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            mbar_arrive(&bfull[bs]);
-            mbar_arrive(&ioempty[slot]);  // the staged tile has been read
-          } else {
-            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            uint32_t cc[4], cmv[4], cev[8];
+    uint32_t cpar = 0;  // bit a: parity of the intermediate accumulators of slot a consumed so far
+    walk_items<DEPTH>(my_tiles, nmat, [&](uint32_t k, uint32_t j, uint32_t i) -> bool {
+      const uint32_t slot = k % NIO, bs = i % NB, bpar = (i / NB) & 1u, a = k % DEPTH;
+      // the input: the staged tile (matrix 0) or the accumulator of this tile's previous matrix;
+      // the converters consume every intermediate accumulator, slot by slot in item order
+      bool ready = j == 0 ? mbar_wait(&iofull[slot], (k / NIO) & 1u) : mbar_wait(&dfull_c[a], (cpar >> a) & 1u);
+      if (j > 0) cpar ^= 1u << a;
+      ready = ready && mbar_wait(&bfree[bs], bpar ^ 1u);
+      if (!__all_sync(0xffffffffu, ready)) {
+        atomicExch(err, 1);
+        return false;
+      }
+      uint8_t* b_hi = bbuf + bs * 2 * kBBytes;
+      uint8_t* b_lo = b_hi + kBBytes;
+      if (j == 0) {
+        const float* sre = io + slot * 2 * kTileAmps;
+        convert_first<BM>(sre, sre + kTileAmps, b_hi, b_lo, s_dlo, s_dhi, s_tperm, p, tid, lane);
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        mbar_arrive(&bfull[bs]);
+        mbar_arrive(&ioempty[slot]);  // the staged tile has been read
+      } else {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        uint32_t cc[4], cmv[4], cev[8];
 #pragma unroll
-            for (int m = 0; m < 4; ++m) {
-              cc[m] = p.cchunk[j][half][m];
-              cmv[m] = p.cm[j][m];
-            }
-#pragma unroll
-            for (int e = 0; e < 8; ++e) cev[e] = p.ce[j][e];
-            convert_next(lane_base + ds * 64u + p.cw[j][half], j == 1 ? rb1 : rb2, cc, cmv, cev, b_hi, b_lo);
-            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-            mbar_arrive(&dfree[ds]);  // this thread's part of the accumulator has been read
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            mbar_arrive(&bfull[bs]);
-          }
+        for (int m = 0; m < 4; ++m) {
+          cc[m] = p.cchunk[j][half][m];
+          cmv[m] = p.cm[j][m];
         }
-    }
-  } else if (warp == kMmaWarp) {
-    // ============================ MMA issue: one lane
-    if (lane == 0) {
+#pragma unroll
+        for (int e = 0; e < 8; ++e) cev[e] = p.ce[j][e];
+        convert_next(lane_base + a * 64u + p.cw[j][half], j == 1 ? rb1 : rb2, cc, cmv, cev, b_hi, b_lo);
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        mbar_arrive(&dfree[a]);  // this thread's part of the accumulator has been read
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        mbar_arrive(&bfull[bs]);
+      }
+      return true;
+    });
+  } else if (warp < kMmaWarp + kMmaWarps) {
+    // ============================ MMA issue: one lane per warp, the items of one B buffer
+    const uint32_t own = uint32_t(warp - kMmaWarp);
+    if (own < uint32_t(NB) && lane == 0) {
       // idesc: f32 accumulate, bf16 A and B, K-major A; B MN-major (bit 16) for every matrix but
       // a K-major first one; N = 64, M = 128
       const uint32_t idesc_k =
           (1u << 4) | (1u << 7) | (1u << 10) | (uint32_t(64 >> 3) << 17) | (uint32_t(128 >> 4) << 24);
       const uint32_t idesc_mn = idesc_k | (1u << 16);
-      uint32_t g = 0;
-      bool stop = false;
-      for (uint64_t w0 = 0; w0 < my_tiles && !stop; w0 += kWave) {
-        const uint32_t nt = my_tiles - w0 < uint64_t(kWave) ? uint32_t(my_tiles - w0) : uint32_t(kWave);
-        for (uint32_t j = 0; j < nmat && !stop; ++j)
-          for (uint32_t tt = 0; tt < nt; ++tt, ++g) {
-            const uint32_t bs = g & 1u, par = (g >> 1) & 1u;
-            if (!mbar_wait(&bfull[bs], par) || !mbar_wait(&dfree[bs], par ^ 1u)) {
-              atomicExch(err, 1);
-              stop = true;
-              break;
-            }
-            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const bool mn = j > 0 ? p.bk[j] == 0 : BM == 0;
-            const uint32_t idesc = mn ? idesc_mn : idesc_k;
-            const uint32_t b_lbo = mn ? 128u * 128u : 16u;
-            const uint32_t b_hi_s = smem_u32(bbuf + bs * 2 * kBBytes), b_lo_s = b_hi_s + kBBytes;
-            const uint32_t d_tmem = tmem + bs * 64u;
-            const uint32_t a_hi = tmem + kTmemA0 + 128u * j, a_lo = a_hi + 64u;
-#pragma unroll 1
-            for (int s = 0; s < 8; ++s) {
-              const uint32_t bk = mn ? uint32_t(s) * 2048u : (s >> 2) * (64u * 128u) + (s & 3) * 32u;
-              const uint64_t dbh = sw128_desc(b_hi_s + bk, b_lbo, 1024u), dbl = sw128_desc(b_lo_s + bk, b_lbo, 1024u);
-              mma_bf16_ts(d_tmem, a_lo + uint32_t(s) * 8u, dbh, idesc, s > 0 ? 1u : 0u);
-              mma_bf16_ts(d_tmem, a_hi + uint32_t(s) * 8u, dbl, idesc, 1u);
-              mma_bf16_ts(d_tmem, a_hi + uint32_t(s) * 8u, dbh, idesc, 1u);
-            }
-            mma_commit(&bfree[bs]);  // B buffer consumed
-            mma_commit(j + 1 < nmat ? &dfull_c[bs] : &dfull_e[bs]);  // accumulator ready for its consumer
+      uint32_t upar = 0;  // bit a: parity of the MMAs into accumulator a so far (all warps' items)
+      walk_items<DEPTH>(my_tiles, nmat, [&](uint32_t k, uint32_t j, uint32_t i) -> bool {
+        const uint32_t a = k % DEPTH, u = (upar >> a) & 1u;
+        upar ^= 1u << a;
+        const uint32_t bs = i % NB;
+        if (bs != own) return true;
+        // the accumulator's previous content (consumed before this MMA can be issued, so the
+        // wait cannot see a phase two ahead)
+        if (!mbar_wait(&bfull[bs], (i / NB) & 1u) || !mbar_wait(&dfree[a], u ^ 1u)) {
+          atomicExch(err, 1);
+          return false;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const bool mn = j > 0 ? p.bk[j] == 0 : BM == 0;
+        const uint32_t d_tmem = tmem + a * 64u;
+        const uint32_t a_hi = tmem + A0 + 128u * j, a_lo = a_hi + 64u;
+        // descriptors of K step 0; step s adds its byte offset (>> 4) to the address field
+        const uint64_t dbh0 = sw128_desc(smem_u32(bbuf + bs * 2 * kBBytes), mn ? 128u * 128u : 16u, 1024u);
+        const uint64_t dbl0 = dbh0 + (kBBytes >> 4);
+        if (mn) {
+#pragma unroll
+          for (int s = 0; s < 8; ++s) {
+            const uint64_t o = uint64_t(s) * (2048u >> 4);
+            mma_bf16_ts(d_tmem, a_lo + uint32_t(s) * 8u, dbh0 + o, idesc_mn, s > 0 ? 1u : 0u);
+            mma_bf16_ts(d_tmem, a_hi + uint32_t(s) * 8u, dbl0 + o, idesc_mn, 1u);
+            mma_bf16_ts(d_tmem, a_hi + uint32_t(s) * 8u, dbh0 + o, idesc_mn, 1u);
           }
-      }
+        } else {
+#pragma unroll
+          for (int s = 0; s < 8; ++s) {
+            const uint64_t o = uint64_t((s >> 2) * (64 * 128) + (s & 3) * 32) >> 4;
+            mma_bf16_ts(d_tmem, a_lo + uint32_t(s) * 8u, dbh0 + o, idesc_k, s > 0 ? 1u : 0u);
+            mma_bf16_ts(d_tmem, a_hi + uint32_t(s) * 8u, dbl0 + o, idesc_k, 1u);
+            mma_bf16_ts(d_tmem, a_hi + uint32_t(s) * 8u, dbh0 + o, idesc_k, 1u);
+          }
+        }
+        mma_commit(&bfree[bs]);  // B buffer consumed
+        mma_commit(j + 1 < nmat ? &dfull_c[a] : &dfull_e[a]);  // accumulator ready for its consumer
+        return true;
+      });
     }
     __syncwarp();
   } else {
@@ -522,68 +562,63 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_chain(float* __restrict__ re
     const uint32_t row = uint32_t(quad * 32 + lane);
     const uint32_t frow = p.frow[row];
     const bool evec = p.evec != 0;
-    uint32_t g = 0;
-    uint32_t eph[2] = {0, 0};  // final accumulators of each slot consumed so far (phases of dfull_e)
-    bool stop = false;
-    for (uint64_t w0 = 0; w0 < my_tiles && !stop; w0 += kWave) {
-      const uint32_t nt = my_tiles - w0 < uint64_t(kWave) ? uint32_t(my_tiles - w0) : uint32_t(kWave);
-      g += (nmat - 1) * nt;  // items of the earlier matrices belong to the converters
-      for (uint32_t tt = 0; tt < nt; ++tt, ++g) {
-        const uint32_t ds = g & 1u;
-        const bool ready = mbar_wait(&dfull_e[ds], eph[ds] & 1u);
-        ++eph[ds];
-        // one decision for all epilogue threads; reaching this barrier also means every thread's
-        // reads of the previous tile's staging are done
-        if (!named_all(2, kEpiThreads, ready)) {
-          atomicExch(err, 1);
-          stop = true;
-          break;
-        }
-        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        uint32_t v[64];
-        tmem_ld64_wait(tmem + (uint32_t(quad * 32) << 16) + ds * 64u, v);
-        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-        mbar_arrive_cnt(&dfree[ds], 2);  // 128 epilogue threads stand for the 256 converter arrivals
-        char* st = reinterpret_cast<char*>(ostage);
-        if (evec) {
-          // columns 4k..4k+3 are four consecutive output positions: one 16-byte store each
-#pragma unroll
-          for (int k = 0; k < 16; ++k)
-            *reinterpret_cast<float4*>(st + (frow ^ uint32_t(p.fcol[4 * k]))) =
-                make_float4(__uint_as_float(v[4 * k]), __uint_as_float(v[4 * k + 1]), __uint_as_float(v[4 * k + 2]),
-                            __uint_as_float(v[4 * k + 3]));
-        } else {
-#pragma unroll
-          for (int q = 0; q < 64; ++q)
-            *reinterpret_cast<float*>(st + (frow ^ uint32_t(p.fcol[q]))) = __uint_as_float(v[q]);
-        }
-        named_sync(1, kEpiThreads);  // the whole result is staged
-        const uint64_t base = tile_base(blockIdx.x + (w0 + tt) * gridDim.x);
-        const uint32_t s1 = p.sig_lo[1], s2 = p.sig_lo[2], s3 = p.sig_lo[3];
-#pragma unroll
-        for (int j = 0; j < kVE; ++j) {
-          const int t = (et + j * kEpiThreads) * 4, tlo = t & 63, thi = t >> 6;
-          const uint64_t a = base + s_hioff[thi] + uint64_t(tlo);
-          const uint32_t w = uint32_t(s_sig[tlo]) ^ s_sig[64 + thi];
-          float4 xr, xi;
-          if (evec) {  // the swizzle keeps bits 0, 1: positions t..t+3 are words w..w+3
-            xr = *reinterpret_cast<const float4*>(ostage + w);
-            xi = *reinterpret_cast<const float4*>(ostage + kTileAmps + w);
-          } else {
-            xr.x = ostage[w];
-            xr.y = ostage[w ^ s1];
-            xr.z = ostage[w ^ s2];
-            xr.w = ostage[w ^ s3];
-            xi.x = ostage[kTileAmps + w];
-            xi.y = ostage[kTileAmps + (w ^ s1)];
-            xi.z = ostage[kTileAmps + (w ^ s2)];
-            xi.w = ostage[kTileAmps + (w ^ s3)];
-          }
-          __stcs(reinterpret_cast<float4*>(re + a), xr);
-          __stcs(reinterpret_cast<float4*>(im + a), xi);
-        }
+    uint32_t epar = 0;  // bit a: parity of the final accumulators of slot a consumed so far
+    walk_items<DEPTH>(my_tiles, nmat, [&](uint32_t k, uint32_t j, uint32_t) -> bool {
+      if (j + 1 != nmat) return true;  // items of the earlier matrices belong to the converters
+      const uint32_t a = k % DEPTH;
+      const bool ready = mbar_wait(&dfull_e[a], (epar >> a) & 1u);
+      epar ^= 1u << a;
+      // one decision for all epilogue threads; reaching this barrier also means every thread's
+      // reads of the previous tile's staging are done
+      if (!named_all(2, kEpiThreads, ready)) {
+        atomicExch(err, 1);
+        return false;
       }
-    }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      uint32_t v[64];
+      tmem_ld64_wait(tmem + (uint32_t(quad * 32) << 16) + a * 64u, v);
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      mbar_arrive_cnt(&dfree[a], 2);  // 128 epilogue threads stand for the 256 converter arrivals
+      char* st = reinterpret_cast<char*>(ostage);
+      if (evec) {
+        // columns 4k..4k+3 are four consecutive output positions: one 16-byte store each
+#pragma unroll
+        for (int q = 0; q < 16; ++q)
+          *reinterpret_cast<float4*>(st + (frow ^ uint32_t(p.fcol[4 * q]))) =
+              make_float4(__uint_as_float(v[4 * q]), __uint_as_float(v[4 * q + 1]), __uint_as_float(v[4 * q + 2]),
+                          __uint_as_float(v[4 * q + 3]));
+      } else {
+#pragma unroll
+        for (int q = 0; q < 64; ++q)
+          *reinterpret_cast<float*>(st + (frow ^ uint32_t(p.fcol[q]))) = __uint_as_float(v[q]);
+      }
+      named_sync(1, kEpiThreads);  // the whole result is staged
+      const uint64_t base = tile_base(blockIdx.x + uint64_t(k) * gridDim.x);
+      const uint32_t s1 = p.sig_lo[1], s2 = p.sig_lo[2], s3 = p.sig_lo[3];
+#pragma unroll
+      for (int q = 0; q < kVE; ++q) {
+        const int t = (et + q * kEpiThreads) * 4, tlo = t & 63, thi = t >> 6;
+        const uint64_t ad = base + s_hioff[thi] + uint64_t(tlo);
+        const uint32_t w = uint32_t(s_sig[tlo]) ^ s_sig[64 + thi];
+        float4 xr, xi;
+        if (evec) {  // the swizzle keeps bits 0, 1: positions t..t+3 are words w..w+3
+          xr = *reinterpret_cast<const float4*>(ostage + w);
+          xi = *reinterpret_cast<const float4*>(ostage + kTileAmps + w);
+        } else {
+          xr.x = ostage[w];
+          xr.y = ostage[w ^ s1];
+          xr.z = ostage[w ^ s2];
+          xr.w = ostage[w ^ s3];
+          xi.x = ostage[kTileAmps + w];
+          xi.y = ostage[kTileAmps + (w ^ s1)];
+          xi.z = ostage[kTileAmps + (w ^ s2)];
+          xi.w = ostage[kTileAmps + (w ^ s3)];
+        }
+        __stcs(reinterpret_cast<float4*>(re + ad), xr);
+        __stcs(reinterpret_cast<float4*>(im + ad), xi);
+      }
+      return true;
+    });
   }
   __syncwarp();  // roles may leave their loops at different iterations after a timeout
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -1118,7 +1153,11 @@ void launch_tc_chain(const LaunchEnv& env, float* re, float* im, uint32_t n, con
   TileLayout lay;
   const uint32_t bmode = build_chain_params(s, n, re, im, p, lay);
   const uint64_t ntiles = 1ull << (n - 12);
-  auto kern = bmode == 0 ? k_tc_chain<0> : bmode == 1 ? k_tc_chain<1> : bmode == 2 ? k_tc_chain<2> : k_tc_chain<3>;
+  // up to two matrices: four accumulators (tiles in flight); three matrices leave tensor memory for two
+  using Kern = decltype(&k_tc_chain<0, 2>);
+  static const Kern kerns[2][4] = {{k_tc_chain<0, 2>, k_tc_chain<1, 2>, k_tc_chain<2, 2>, k_tc_chain<3, 2>},
+                                   {k_tc_chain<0, 4>, k_tc_chain<1, 4>, k_tc_chain<2, 4>, k_tc_chain<3, 4>}};
+  const Kern kern = kerns[s.chain_nmat <= 2 ? 1 : 0][bmode];
   QSVB_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kChainSmem)));
   QSVB_CK(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
                                int(cudaSharedmemCarveoutMaxShared)));
