@@ -779,9 +779,11 @@ KERNEL_CASES = {
     "dense4_c128": ("f64", lambda n: [("u4", [0, 1, 2, 3])]),
     "dense5_c128": ("f64", lambda n: [("u5", [2, 3, 9, 10, 20])]),
     "dense4_c128": ("f64", lambda n: [("u4", [0, 1, 2, 3])]),
-    # tensor-core chain passes: one pass of 1 / 2 / 3 Haar 6-qubit matrices on the qubits 0..11
+    # tensor-core chain passes: one pass of 1 / 2 / 3 Haar 6-qubit matrices on the qubits 0..11; the
+    # last matrix leaves qubits 0 and 1 as columns, as the planner arranges in circuits (16-byte
+    # staging writes in the epilogue)
     "chain1": ("f32", lambda n: [("u6", list(range(6, 12)))]),
-    "chain2": ("f32", lambda n: [("u6", list(range(6, 12))), ("u6", list(range(6)))]),
+    "chain2": ("f32", lambda n: [("u6", list(range(6, 12))), ("u6", list(range(2, 8)))]),
     "chain3": ("f32", lambda n: [("u6", list(range(6, 12))), ("u6", list(range(6))), ("u6", list(range(3, 9)))]),
 }
 

@@ -21,10 +21,10 @@
 //     previous matrix's columns (one of the two always does); chunk offsets are an XOR of a per-row
 //     and a per-chunk part, both precomputed on the host; the hi/lo splits convert two values per
 //     instruction (packed bf16x2);
-//   MMA warps (one per B buffer, one lane each): 24 tcgen05.mma per matrix into the tile's
-//     accumulator (64 columns), the A operand (Whi, Wlo of matrix j) resident in tensor memory for
-//     the whole kernel; one thread issues a tcgen05.mma only every ~80 cycles while an N = 64 MMA
-//     occupies the tensor pipe ~32 cycles, so several items' MMAs are issued concurrently;
+//   MMA warps (one per B buffer; the warp walks the items on uniform control flow and one elected
+//     lane issues): 24 tcgen05.mma per matrix into the tile's accumulator (64 columns), the A
+//     operand (Whi, Wlo of matrix j) resident in tensor memory for the whole kernel; several items'
+//     MMAs are issued concurrently;
 //   epilogue warps (4): after the last matrix, read the accumulator, stage it in shared memory in
 //     the permuted address order (16-byte stores when the pass's permutation puts the last matrix's
 //     first two columns on output bits 0 and 1, which the planner arranges; scalar stores
@@ -130,32 +130,60 @@ __device__ __forceinline__ void split2f(float x0, float x1, uint32_t& hi, uint32
 // 1 K-major vectors (they are the matrix's rows 0, 1), 2 K-major row pairs (exactly one is a row,
 // the lowest), 3 K-major vectors assembled from a lane pair (bit 0 a column, bit 1 row 0, row 1 one
 // of state bits 2..4).
+//
+// What a converter thread does for a first matrix is the same for every tile of the pass, so it is
+// worked out once (first_plan): for each of its kVC float4 groups, the staged word index t in the
+// high half of plan[j] and the byte offset in B of its real parts in the low half (the imaginary
+// parts follow 8192 bytes later in both layouts); layout 2 stores two pairs per group, the second
+// offset in plan2[j]. Per tile, the conversion is then independent 16-byte loads, packed splits
+// and stores.
 template <int BM>
-__device__ __forceinline__ void convert_first(const float* __restrict__ sre, const float* __restrict__ sim,
-                                              uint8_t* __restrict__ b_hi, uint8_t* __restrict__ b_lo,
-                                              const uint16_t* __restrict__ s_dlo, const uint16_t* __restrict__ s_dhi,
-                                              const uint16_t* __restrict__ s_tperm, const ChainParams& p, int tid,
-                                              int lane) {
-  constexpr uint32_t M2 = 64, NCB = 6, CMASK = 63;
-  constexpr bool b_mn = BM == 0;
-  float4 xra[kVC], xia[kVC];
-  uint32_t dda[kVC];
-  int tt[kVC];
+__device__ __forceinline__ void first_plan(const uint16_t* __restrict__ s_dlo, const uint16_t* __restrict__ s_dhi,
+                                           const uint16_t* __restrict__ s_tperm, const ChainParams& p, int tid,
+                                           int lane, uint32_t (&plan)[kVC], uint32_t (&plan2)[kVC]) {
+  constexpr uint32_t NCB = 6, CMASK = 63;
 #pragma unroll
   for (int j = 0; j < kVC; ++j) {
     const uint32_t u = uint32_t(tid + j * kCvtThreads);
-    const int t = int(uint32_t(s_tperm[u & 31u]) | uint32_t(s_tperm[32 + (u >> 5)])) * 4;
-    tt[j] = t;
-    xra[j] = *reinterpret_cast<const float4*>(sre + t);
-    xia[j] = *reinterpret_cast<const float4*>(sim + t);
-    dda[j] = uint32_t(s_dlo[t & 63]) + s_dhi[t >> 6];
+    const uint32_t t = (uint32_t(s_tperm[u & 31u]) | uint32_t(s_tperm[32 + (u >> 5)])) * 4u;
+    uint32_t o = 0, o2 = 0;
+    if constexpr (BM == 3) {
+      const uint32_t sh = p.pair_shift;
+      const bool odd = ((uint32_t(lane) >> sh) & 1u) != 0;
+      const uint32_t tg = (t & ~(4u << sh)) | (odd ? 1u : 0u);
+      const uint32_t d = uint32_t(s_dlo[tg & 63]) + s_dhi[tg >> 6];
+      o = kmaj_off(d & CMASK, d >> NCB, 64);
+    } else if constexpr (BM == 2) {
+      const uint32_t e1 = p.b2_bit0 ? 2u : 1u;
+      const uint32_t d0 = uint32_t(s_dlo[t & 63]) + s_dhi[t >> 6];
+      const uint32_t d1 = uint32_t(s_dlo[(t & 63) + e1]) + s_dhi[t >> 6];
+      o = kmaj_off(d0 & CMASK, d0 >> NCB, 64);
+      o2 = kmaj_off(d1 & CMASK, d1 >> NCB, 64);
+    } else {
+      const uint32_t d = uint32_t(s_dlo[t & 63]) + s_dhi[t >> 6];
+      o = BM == 0 ? mnmaj_off(d >> NCB, d & CMASK) : kmaj_off(d & CMASK, d >> NCB, 64);
+    }
+    plan[j] = (t << 16) | o;
+    plan2[j] = o2;
+  }
+}
+
+template <int BM>
+__device__ __forceinline__ void convert_first(uint32_t sre, uint32_t sim, uint32_t b_hi, uint32_t b_lo,
+                                              const uint32_t (&plan)[kVC], const uint32_t (&plan2)[kVC],
+                                              const ChainParams& p, int lane) {
+  constexpr uint32_t kImOff = 8192;  // imaginary rows M2..2 M2-1: the second K half / 8 row groups later
+  float4 xra[kVC], xia[kVC];
+#pragma unroll
+  for (int j = 0; j < kVC; ++j) {
+    const uint32_t t4 = (plan[j] >> 16) * 4u;
+    xra[j] = lds128f(sre + t4);
+    xia[j] = lds128f(sim + t4);
   }
 #pragma unroll
   for (int j = 0; j < kVC; ++j) {
-    const int t = tt[j], tlo = t & 63, thi = t >> 6;
     const float4 xr = xra[j], xi = xia[j];
-    const float vr[4] = {xr.x, xr.y, xr.z, xr.w};
-    const float vi[4] = {xi.x, xi.y, xi.z, xi.w};
+    const uint32_t o = plan[j] & 0xFFFFu;
     if constexpr (BM == 3) {
       const uint32_t sh = p.pair_shift;
       const bool odd = ((uint32_t(lane) >> sh) & 1u) != 0;
@@ -164,51 +192,41 @@ __device__ __forceinline__ void convert_first(const float* __restrict__ sre, con
       const float rr1 = __shfl_xor_sync(0xffffffffu, odd ? xr.z : xr.w, pm);
       const float ri0 = __shfl_xor_sync(0xffffffffu, odd ? xi.x : xi.y, pm);
       const float ri1 = __shfl_xor_sync(0xffffffffu, odd ? xi.z : xi.w, pm);
-      const float wr[4] = {odd ? rr0 : xr.x, odd ? rr1 : xr.z, odd ? xr.y : rr0, odd ? xr.w : rr1};
-      const float wi[4] = {odd ? ri0 : xi.x, odd ? ri1 : xi.z, odd ? xi.y : ri0, odd ? xi.w : ri1};
-      const int tg = (t & ~(4 << sh)) | (odd ? 1 : 0);
-      const uint32_t d = uint32_t(s_dlo[tg & 63]) + s_dhi[tg >> 6];
-      const uint32_t s = d >> NCB, c = d & CMASK;
-      const uint32_t o_re = kmaj_off(c, s, 64), o_im = kmaj_off(c, M2 + s, 64);
-      uint2 hr, lr, hm, lm;
-      split2f(wr[0], wr[1], hr.x, lr.x);
-      split2f(wr[2], wr[3], hr.y, lr.y);
-      split2f(wi[0], wi[1], hm.x, lm.x);
-      split2f(wi[2], wi[3], hm.y, lm.y);
-      *reinterpret_cast<uint2*>(b_hi + o_re) = hr;
-      *reinterpret_cast<uint2*>(b_lo + o_re) = lr;
-      *reinterpret_cast<uint2*>(b_hi + o_im) = hm;
-      *reinterpret_cast<uint2*>(b_lo + o_im) = lm;
+      uint32_t h0, l0, h1, l1;
+      split2f(odd ? rr0 : xr.x, odd ? rr1 : xr.z, h0, l0);
+      split2f(odd ? xr.y : rr0, odd ? xr.w : rr1, h1, l1);
+      sts64(b_hi + o, h0, h1);
+      sts64(b_lo + o, l0, l1);
+      split2f(odd ? ri0 : xi.x, odd ? ri1 : xi.z, h0, l0);
+      split2f(odd ? xi.y : ri0, odd ? xi.w : ri1, h1, l1);
+      sts64(b_hi + o + kImOff, h0, h1);
+      sts64(b_lo + o + kImOff, l0, l1);
     } else if constexpr (BM == 2) {
+      const float vr[4] = {xr.x, xr.y, xr.z, xr.w};
+      const float vi[4] = {xi.x, xi.y, xi.z, xi.w};
       const int step = p.b2_bit0 ? 1 : 2;
 #pragma unroll
       for (int q = 0; q < 2; ++q) {
         const int e = p.b2_bit0 ? 2 * q : q;
-        const uint32_t d = uint32_t(s_dlo[tlo + e]) + s_dhi[thi];
-        const uint32_t s = d >> NCB, c = d & CMASK;
-        const uint32_t o_re = kmaj_off(c, s, 64), o_im = kmaj_off(c, M2 + s, 64);
+        const uint32_t oq = q == 0 ? o : plan2[j];
         uint32_t h, l;
         split2f(vr[e], vr[e + step], h, l);
-        *reinterpret_cast<uint32_t*>(b_hi + o_re) = h;
-        *reinterpret_cast<uint32_t*>(b_lo + o_re) = l;
+        sts32(b_hi + oq, h);
+        sts32(b_lo + oq, l);
         split2f(vi[e], vi[e + step], h, l);
-        *reinterpret_cast<uint32_t*>(b_hi + o_im) = h;
-        *reinterpret_cast<uint32_t*>(b_lo + o_im) = l;
+        sts32(b_hi + oq + kImOff, h);
+        sts32(b_lo + oq + kImOff, l);
       }
     } else {
-      const uint32_t d = dda[j];
-      const uint32_t s = d >> NCB, c = d & CMASK;
-      const uint32_t o_re = b_mn ? mnmaj_off(s, c) : kmaj_off(c, s, 64);
-      const uint32_t o_im = b_mn ? mnmaj_off(M2 + s, c) : kmaj_off(c, M2 + s, 64);
-      uint2 hr, lr, hm, lm;
-      split2f(xr.x, xr.y, hr.x, lr.x);
-      split2f(xr.z, xr.w, hr.y, lr.y);
-      split2f(xi.x, xi.y, hm.x, lm.x);
-      split2f(xi.z, xi.w, hm.y, lm.y);
-      *reinterpret_cast<uint2*>(b_hi + o_re) = hr;
-      *reinterpret_cast<uint2*>(b_lo + o_re) = lr;
-      *reinterpret_cast<uint2*>(b_hi + o_im) = hm;
-      *reinterpret_cast<uint2*>(b_lo + o_im) = lm;
+      uint32_t h0, l0, h1, l1;
+      split2f(xr.x, xr.y, h0, l0);
+      split2f(xr.z, xr.w, h1, l1);
+      sts64(b_hi + o, h0, h1);
+      sts64(b_lo + o, l0, l1);
+      split2f(xi.x, xi.y, h0, l0);
+      split2f(xi.z, xi.w, h1, l1);
+      sts64(b_hi + o + kImOff, h0, h1);
+      sts64(b_lo + o + kImOff, l0, l1);
     }
   }
 }
@@ -364,20 +382,23 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_chain(float* __restrict__ re
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   if (tid == 0) {
+    // converter and epilogue barriers take one arrival per warp (lane 0, after the warp's lanes
+    // have synchronised): 256 single-thread arrivals on one barrier word serialise for hundreds of
+    // cycles
     for (int s = 0; s < NIO; ++s) {
       mbar_init(&iofull[s], 1);
-      mbar_init(&ioempty[s], kCvtThreads);
+      mbar_init(&ioempty[s], kCvtWarps);
     }
     for (int s = 0; s < NB; ++s) {
-      mbar_init(&bfull[s], kCvtThreads);
+      mbar_init(&bfull[s], kCvtWarps);
       mbar_init(&bfree[s], 1);
     }
     for (int s = 0; s < DEPTH; ++s) {
       mbar_init(&dfull_c[s], 1);
       mbar_init(&dfull_e[s], 1);
-      // every converter thread (count 1) or every epilogue thread (count 2) once it has read the
+      // every converter warp (count 1) or every epilogue warp (count 2) once it has read the
       // accumulator
-      mbar_init(&dfree[s], kCvtThreads);
+      mbar_init(&dfree[s], kCvtWarps);
     }
     asm volatile("fence.mbarrier_init.release.cluster;");
   }
@@ -466,26 +487,38 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_chain(float* __restrict__ re
     if (nmat > 1) rb1 = p.crow[1][row];
     if (nmat > 2) rb2 = p.crow[2][row];
     const uint32_t lane_base = tmem + ((quad * 32) << 16);
+    uint32_t plan[kVC], plan2[kVC];
+    first_plan<BM>(s_dlo, s_dhi, s_tperm, p, tid, lane, plan, plan2);
     uint32_t cpar = 0;  // bit a: parity of the intermediate accumulators of slot a consumed so far
     walk_items<DEPTH>(my_tiles, nmat, [&](uint32_t k, uint32_t j, uint32_t i) -> bool {
       const uint32_t slot = k % NIO, bs = i % NB, bpar = (i / NB) & 1u, a = k % DEPTH;
       // the input: the staged tile (matrix 0) or the accumulator of this tile's previous matrix;
-      // the converters consume every intermediate accumulator, slot by slot in item order
-      bool ready = j == 0 ? mbar_wait(&iofull[slot], (k / NIO) & 1u) : mbar_wait(&dfull_c[a], (cpar >> a) & 1u);
+      // the converters consume every intermediate accumulator, slot by slot in item order. Lane 0
+      // waits for the warp (a barrier polled by all 32 lanes costs hundreds of cycles); the warp
+      // synchronisation after it orders the other lanes' reads after its acquire.
+      bool ready = true;
+      if (lane == 0) {
+        ready = j == 0 ? mbar_wait(&iofull[slot], (k / NIO) & 1u) : mbar_wait(&dfull_c[a], (cpar >> a) & 1u);
+        ready = ready && mbar_wait(&bfree[bs], bpar ^ 1u);
+      }
       if (j > 0) cpar ^= 1u << a;
-      ready = ready && mbar_wait(&bfree[bs], bpar ^ 1u);
-      if (!__all_sync(0xffffffffu, ready)) {
+      ready = __shfl_sync(0xffffffffu, ready ? 1 : 0, 0) != 0;
+      __syncwarp();
+      if (!ready) {
         atomicExch(err, 1);
         return false;
       }
       uint8_t* b_hi = bbuf + bs * 2 * kBBytes;
       uint8_t* b_lo = b_hi + kBBytes;
       if (j == 0) {
-        const float* sre = io + slot * 2 * kTileAmps;
-        convert_first<BM>(sre, sre + kTileAmps, b_hi, b_lo, s_dlo, s_dhi, s_tperm, p, tid, lane);
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        mbar_arrive(&bfull[bs]);
-        mbar_arrive(&ioempty[slot]);  // the staged tile has been read
+        const uint32_t sre = smem_u32(io + slot * 2 * kTileAmps);
+        convert_first<BM>(sre, sre + kTileAmps * 4u, smem_u32(b_hi), smem_u32(b_lo), plan, plan2, p, lane);
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // B writes -> the MMA's reads
+        __syncwarp();
+        if (lane == 0) {
+          mbar_arrive(&bfull[bs]);
+          mbar_arrive(&ioempty[slot]);  // the staged tile has been read
+        }
       } else {
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         uint32_t cc[4], cmv[4], cev[8];
@@ -498,16 +531,21 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_chain(float* __restrict__ re
         for (int e = 0; e < 8; ++e) cev[e] = p.ce[j][e];
         convert_next(lane_base + a * 64u + p.cw[j][half], j == 1 ? rb1 : rb2, cc, cmv, cev, b_hi, b_lo);
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-        mbar_arrive(&dfree[a]);  // this thread's part of the accumulator has been read
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        mbar_arrive(&bfull[bs]);
+        __syncwarp();
+        if (lane == 0) {
+          mbar_arrive(&dfree[a]);  // the warp's part of the accumulator has been read
+          mbar_arrive(&bfull[bs]);
+        }
       }
       return true;
     });
   } else if (warp < kMmaWarp + kMmaWarps) {
-    // ============================ MMA issue: one lane per warp, the items of one B buffer
+    // ============================ MMA issue: the items of one B buffer; the whole warp walks them
+    // (uniform operands), one elected lane issues
     const uint32_t own = uint32_t(warp - kMmaWarp);
-    if (own < uint32_t(NB) && lane == 0) {
+    if (own < uint32_t(NB)) {
+      const uint32_t leader = elect_one();
       // idesc: f32 accumulate, bf16 A and B, K-major A; B MN-major (bit 16) for every matrix but
       // a K-major first one; N = 64, M = 128
       const uint32_t idesc_k =
@@ -521,8 +559,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_chain(float* __restrict__ re
         if (bs != own) return true;
         // the accumulator's previous content (consumed before this MMA can be issued, so the
         // wait cannot see a phase two ahead)
-        if (!mbar_wait(&bfull[bs], (i / NB) & 1u) || !mbar_wait(&dfree[a], u ^ 1u)) {
-          atomicExch(err, 1);
+        const bool ok = mbar_wait(&bfull[bs], (i / NB) & 1u) && mbar_wait(&dfree[a], u ^ 1u);
+        if (!__all_sync(0xffffffffu, ok)) {
+          if (leader) atomicExch(err, 1);
           return false;
         }
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -536,21 +575,21 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_chain(float* __restrict__ re
 #pragma unroll
           for (int s = 0; s < 8; ++s) {
             const uint64_t o = uint64_t(s) * (2048u >> 4);
-            mma_bf16_ts(d_tmem, a_lo + uint32_t(s) * 8u, dbh0 + o, idesc_mn, s > 0 ? 1u : 0u);
-            mma_bf16_ts(d_tmem, a_hi + uint32_t(s) * 8u, dbl0 + o, idesc_mn, 1u);
-            mma_bf16_ts(d_tmem, a_hi + uint32_t(s) * 8u, dbh0 + o, idesc_mn, 1u);
+            mma_bf16_ts_by(leader, d_tmem, a_lo + uint32_t(s) * 8u, dbh0 + o, idesc_mn, s > 0 ? 1u : 0u);
+            mma_bf16_ts_by(leader, d_tmem, a_hi + uint32_t(s) * 8u, dbl0 + o, idesc_mn, 1u);
+            mma_bf16_ts_by(leader, d_tmem, a_hi + uint32_t(s) * 8u, dbh0 + o, idesc_mn, 1u);
           }
         } else {
 #pragma unroll
           for (int s = 0; s < 8; ++s) {
             const uint64_t o = uint64_t((s >> 2) * (64 * 128) + (s & 3) * 32) >> 4;
-            mma_bf16_ts(d_tmem, a_lo + uint32_t(s) * 8u, dbh0 + o, idesc_k, s > 0 ? 1u : 0u);
-            mma_bf16_ts(d_tmem, a_hi + uint32_t(s) * 8u, dbl0 + o, idesc_k, 1u);
-            mma_bf16_ts(d_tmem, a_hi + uint32_t(s) * 8u, dbh0 + o, idesc_k, 1u);
+            mma_bf16_ts_by(leader, d_tmem, a_lo + uint32_t(s) * 8u, dbh0 + o, idesc_k, s > 0 ? 1u : 0u);
+            mma_bf16_ts_by(leader, d_tmem, a_hi + uint32_t(s) * 8u, dbl0 + o, idesc_k, 1u);
+            mma_bf16_ts_by(leader, d_tmem, a_hi + uint32_t(s) * 8u, dbh0 + o, idesc_k, 1u);
           }
         }
-        mma_commit(&bfree[bs]);  // B buffer consumed
-        mma_commit(j + 1 < nmat ? &dfull_c[a] : &dfull_e[a]);  // accumulator ready for its consumer
+        mma_commit_by(leader, &bfree[bs]);  // B buffer consumed
+        mma_commit_by(leader, j + 1 < nmat ? &dfull_c[a] : &dfull_e[a]);  // accumulator ready for its consumer
         return true;
       });
     }
@@ -566,10 +605,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_chain(float* __restrict__ re
     walk_items<DEPTH>(my_tiles, nmat, [&](uint32_t k, uint32_t j, uint32_t) -> bool {
       if (j + 1 != nmat) return true;  // items of the earlier matrices belong to the converters
       const uint32_t a = k % DEPTH;
-      const bool ready = mbar_wait(&dfull_e[a], (epar >> a) & 1u);
+      const bool ready = lane != 0 || mbar_wait(&dfull_e[a], (epar >> a) & 1u);  // lane 0 waits for the warp
       epar ^= 1u << a;
-      // one decision for all epilogue threads; reaching this barrier also means every thread's
-      // reads of the previous tile's staging are done
+      // one decision for all epilogue threads (the barrier also orders every lane after its warp's
+      // acquire); reaching it also means every thread's reads of the previous tile's staging are done
       if (!named_all(2, kEpiThreads, ready)) {
         atomicExch(err, 1);
         return false;
@@ -578,19 +617,19 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_chain(float* __restrict__ re
       uint32_t v[64];
       tmem_ld64_wait(tmem + (uint32_t(quad * 32) << 16) + a * 64u, v);
       asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-      mbar_arrive_cnt(&dfree[a], 2);  // 128 epilogue threads stand for the 256 converter arrivals
-      char* st = reinterpret_cast<char*>(ostage);
+      __syncwarp();
+      if (lane == 0) mbar_arrive_cnt(&dfree[a], 2);  // 4 epilogue warps stand for the 8 converter warps
+      const uint32_t st = smem_u32(ostage);
       if (evec) {
         // columns 4k..4k+3 are four consecutive output positions: one 16-byte store each
 #pragma unroll
         for (int q = 0; q < 16; ++q)
-          *reinterpret_cast<float4*>(st + (frow ^ uint32_t(p.fcol[4 * q]))) =
-              make_float4(__uint_as_float(v[4 * q]), __uint_as_float(v[4 * q + 1]), __uint_as_float(v[4 * q + 2]),
-                          __uint_as_float(v[4 * q + 3]));
+          sts128f(st + (frow ^ uint32_t(p.fcol[4 * q])),
+                  make_float4(__uint_as_float(v[4 * q]), __uint_as_float(v[4 * q + 1]), __uint_as_float(v[4 * q + 2]),
+                              __uint_as_float(v[4 * q + 3])));
       } else {
 #pragma unroll
-        for (int q = 0; q < 64; ++q)
-          *reinterpret_cast<float*>(st + (frow ^ uint32_t(p.fcol[q]))) = __uint_as_float(v[q]);
+        for (int q = 0; q < 64; ++q) sts32(st + (frow ^ uint32_t(p.fcol[q])), v[q]);
       }
       named_sync(1, kEpiThreads);  // the whole result is staged
       const uint64_t base = tile_base(blockIdx.x + uint64_t(k) * gridDim.x);
@@ -602,8 +641,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_chain(float* __restrict__ re
         const uint32_t w = uint32_t(s_sig[tlo]) ^ s_sig[64 + thi];
         float4 xr, xi;
         if (evec) {  // the swizzle keeps bits 0, 1: positions t..t+3 are words w..w+3
-          xr = *reinterpret_cast<const float4*>(ostage + w);
-          xi = *reinterpret_cast<const float4*>(ostage + kTileAmps + w);
+          xr = lds128f(st + w * 4u);
+          xi = lds128f(st + (kTileAmps + w) * 4u);
         } else {
           xr.x = ostage[w];
           xr.y = ostage[w ^ s1];

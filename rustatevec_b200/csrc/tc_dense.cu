@@ -355,31 +355,35 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_dense(float* __restrict__ 
       mbar_arrive(&ioempty[slot]);  // this thread's reads of the input slot are done (fenced above)
     }
   } else if (warp == kMmaWarp) {
-    // ============================ MMA issue: one lane
-    if (lane == 0) {
+    // ============================ MMA issue: the whole warp walks the tiles (uniform operands), one
+    // elected lane issues
+    {
+      const uint32_t leader = elect_one();
       const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | (b_mn << 16) | (uint32_t(kMmaN >> 3) << 17) |
                              (uint32_t(128 >> 4) << 24);
       const uint32_t b_lbo = b_mn ? uint32_t(kMmaK) * 128u : 16u;
       for (uint64_t i = 0; i < my_tiles; ++i) {
         const uint32_t bs = uint32_t(i & 1), par = uint32_t((i >> 1) & 1);
-        if (!mbar_wait_t(&bfull[bs], par, w0) || !mbar_wait_t(&dfree[bs], par ^ 1u, w1)) {
-          atomicExch(err, 1);
+        const bool ok = mbar_wait_t(&bfull[bs], par, w0) && mbar_wait_t(&dfree[bs], par ^ 1u, w1);
+        if (!__all_sync(0xffffffffu, ok)) {
+          if (leader) atomicExch(err, 1);
           break;
         }
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        const uint32_t b_hi_s = smem_u32(bbuf + bs * 2 * kBBytes), b_lo_s = b_hi_s + kBBytes;
         const uint32_t d_tmem = tmem + bs * kMmaN;
-#pragma unroll 1
+        // descriptors of K step 0; step s adds its byte offset (>> 4) to the address field
+        const uint64_t dbh0 = sw128_desc(smem_u32(bbuf + bs * 2 * kBBytes), b_lbo, 1024u);
+        const uint64_t dbl0 = dbh0 + (kBBytes >> 4);
+#pragma unroll
         for (int s = 0; s < kMmaK / 16; ++s) {
-          const uint32_t bk = b_mn ? uint32_t(s) * 2048u : (s >> 2) * (64u * 128u) + (s & 3) * 32u;
+          const uint64_t o = (b_mn ? uint64_t(s) * 2048u : uint64_t((s >> 2) * (64 * 128) + (s & 3) * 32)) >> 4;
           const uint32_t tah = tmem + kTmemAHi + uint32_t(s) * 8u, tal = tmem + kTmemALo + uint32_t(s) * 8u;
-          const uint64_t dbh = sw128_desc(b_hi_s + bk, b_lbo, 1024u), dbl = sw128_desc(b_lo_s + bk, b_lbo, 1024u);
-          mma_bf16_ts(d_tmem, tal, dbh, idesc, s > 0 ? 1u : 0u);
-          mma_bf16_ts(d_tmem, tah, dbl, idesc, 1u);
-          mma_bf16_ts(d_tmem, tah, dbh, idesc, 1u);
+          mma_bf16_ts_by(leader, d_tmem, tal, dbh0 + o, idesc, s > 0 ? 1u : 0u);
+          mma_bf16_ts_by(leader, d_tmem, tah, dbl0 + o, idesc, 1u);
+          mma_bf16_ts_by(leader, d_tmem, tah, dbh0 + o, idesc, 1u);
         }
-        mma_commit(&bfree[bs]);  // B buffer consumed
-        mma_commit(&dfull[bs]);  // accumulator ready
+        mma_commit_by(leader, &bfree[bs]);  // B buffer consumed
+        mma_commit_by(leader, &dfull[bs]);  // accumulator ready
       }
     }
     __syncwarp();
