@@ -89,7 +89,7 @@ struct ChainParams {
   uint32_t hibits[6];
   uint64_t hioff[64];
   uint32_t runbits;
-  uint32_t tm_rank, tm_start[5], tm_len[5];
+  uint32_t tm_rank, tm_start[5], tm_len[5], tm_outer, tm_obit[3];
   uint32_t nmat;
   // first matrix, read from the staged tile in address order: (row << 6 | column) of each value
   // of the low / high six tile positions, the converters' work order, and the B layout details
@@ -462,14 +462,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_chain(float* __restrict__ re
       float* dre = io + slot * 2 * kTileAmps;
       float* dim_ = dre + kTileAmps;
       if (p.tm_rank > 0) {
-        if (lane == 0) {
-          int c[5];
-#pragma unroll
-          for (uint32_t d = 0; d < 5; ++d)
-            c[d] = d < p.tm_rank ? int((base >> p.tm_start[d]) & ((1ull << p.tm_len[d]) - 1ull)) : 0;
-          tma_tensor_g2s(dre, &tm_re, c, p.tm_rank, &iofull[slot]);
-          tma_tensor_g2s(dim_, &tm_im, c, p.tm_rank, &iofull[slot]);
-        }
+        if (lane == 0)
+          tma_tile_g2s(dre, dim_, &tm_re, &tm_im, base, p.tm_rank, p.tm_start, p.tm_len, p.tm_outer, p.tm_obit,
+                       &iofull[slot]);
         continue;
       }
       for (uint32_t j = lane; j < nruns; j += 32) {
@@ -910,6 +905,8 @@ uint32_t build_chain_params(const Sweep& s, uint32_t n, float* re, float* im, Ch
   p.tm_rank = lay.tm_rank;
   std::copy(lay.tm_start, lay.tm_start + 5, p.tm_start);
   std::copy(lay.tm_len, lay.tm_len + 5, p.tm_len);
+  p.tm_outer = lay.tm_outer;
+  std::copy(lay.tm_obit, lay.tm_obit + 3, p.tm_obit);
   uint8_t rows[kChainMaxMats][6], cols[kChainMaxMats][6];
   for (uint32_t j = 0; j < nm; ++j) {
     std::copy(s.chain_rows[j], s.chain_rows[j] + 6, rows[j]);

@@ -254,6 +254,25 @@ __device__ __forceinline__ void tma_tensor_g2s(void* dst, const CUtensorMap* map
   }
 }
 
+// A whole tile in address order by tiled tensor-map copies (no multicast): one per value of the
+// `nouter` tile bits folded into the last dimension's coordinate (bit positions obit), each filling
+// the next 4096 >> nouter amplitudes of the slot. `base` is the tile's first state index.
+__device__ __forceinline__ void tma_tile_g2s(float* dre, float* dim, const CUtensorMap* mre, const CUtensorMap* mim,
+                                             uint64_t base, uint32_t rank, const uint32_t (&start)[5],
+                                             const uint32_t (&len)[5], uint32_t nouter, const uint32_t (&obit)[3],
+                                             uint64_t* bar) {
+  int c[5];
+#pragma unroll
+  for (uint32_t d = 0; d < 5; ++d) c[d] = d < rank ? int((base >> start[d]) & ((1ull << len[d]) - 1ull)) : 0;
+  const uint32_t chunk = 4096u >> nouter;
+  for (uint32_t o = 0; o < (1u << nouter); ++o) {
+    int cc[5] = {c[0], c[1], c[2], c[3], c[4]};
+    for (uint32_t k = 0; k < nouter; ++k) cc[rank - 1] |= int(((o >> k) & 1u) << obit[k]);
+    tma_tensor_g2s(dre + o * chunk, mre, cc, rank, bar);
+    tma_tensor_g2s(dim + o * chunk, mim, cc, rank, bar);
+  }
+}
+
 // One bulk copy global -> this CTA's shared memory, completing on `bar` (no multicast).
 __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
   asm volatile(
@@ -288,8 +307,11 @@ struct TileLayout {
   uint32_t hibits[6];
   uint64_t hioff[64];     // address offset of each value of the high six tile bits
   uint32_t runbits;       // log2 of the contiguous run length (>= 6)
-  uint32_t tm_rank;       // > 0: one tiled tensor-map copy per component fetches the tile
+  uint32_t tm_rank;       // > 0: tiled tensor-map copies fetch the tile (2^tm_outer per component)
   uint32_t tm_start[5], tm_len[5];
+  uint32_t tm_box[5];     // log2 of each dimension's box extent (its run of tile bits)
+  uint32_t tm_outer;      // tile bits folded into the last dimension's coordinate (0..3)
+  uint32_t tm_obit[3];    // their bit positions in that coordinate
   CUtensorMap maps[2];
 };
 void tile_layout(uint32_t n, const uint32_t (&tbits)[12], float* re, float* im, TileLayout& out);

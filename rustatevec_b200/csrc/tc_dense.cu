@@ -99,6 +99,8 @@ struct TcParams {
   uint32_t tm_rank;        // > 0: the producer uses one tensor-map TMA per component per tile
   uint32_t tm_start[5];    // first state bit of each tensor dimension
   uint32_t tm_len[5];      // bits of that dimension (a run of tile bits plus the run of non-tile bits above it)
+  uint32_t tm_outer;       // tile bits folded into the last dimension (one copy per value)
+  uint32_t tm_obit[3];     // their bit positions in that dimension's coordinate
 };
 
 // BM: the B-operand layout mode (TcParams::bmode), fixed at compile time so that each
@@ -224,14 +226,9 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_dense(float* __restrict__ 
       float* dre = io + slot * 2 * kTileAmps;
       float* dim_ = dre + kTileAmps;
       if (p.tm_rank > 0) {
-        if (lane == 0) {
-          int c[5];
-#pragma unroll
-          for (uint32_t d = 0; d < 5; ++d)
-            c[d] = d < p.tm_rank ? int((base >> p.tm_start[d]) & ((1ull << p.tm_len[d]) - 1ull)) : 0;
-          tma_tensor_g2s(dre, &tm_re, c, p.tm_rank, &iofull[slot]);
-          tma_tensor_g2s(dim_, &tm_im, c, p.tm_rank, &iofull[slot]);
-        }
+        if (lane == 0)
+          tma_tile_g2s(dre, dim_, &tm_re, &tm_im, base, p.tm_rank, p.tm_start, p.tm_len, p.tm_outer, p.tm_obit,
+                       &iofull[slot]);
         continue;
       }
       for (uint32_t j = lane; j < nruns; j += 32) {
@@ -552,10 +549,32 @@ void tile_layout(uint32_t n, const uint32_t (&tbits)[12], float* re, float* im, 
     dims.push_back({b, e - b, f - b});
     b = f;
   }
-  bool ok = dims.size() <= 5;
+  // A tensor map has at most five dimensions: fold every dimension above the fifth into it. Their
+  // tile bits become bits of the fifth coordinate, fetched by one copy per value (at most two bits:
+  // seven dimensions mean six single-bit runs of high tile bits).
+  uint32_t obits[3] = {0, 0, 0}, nob = 0;
+  bool ok = true;
+  if (dims.size() > 5) {
+    for (size_t d = 5; d < dims.size(); ++d)
+      for (uint32_t t = 0; t < dims[d].tile_len; ++t) {
+        if (nob < 3) obits[nob] = dims[d].start + t - dims[4].start;
+        ++nob;
+      }
+    dims[4].len = n - dims[4].start;
+    dims.resize(5);
+    ok = nob <= 3;
+  }
   for (const Dim& d : dims) ok = ok && d.tile_len <= 8 && d.len <= 31;  // box <= 256, extent < 2^32
   for (size_t d = 1; d < dims.size(); ++d) ok = ok && dims[d].start >= 2;  // 16-byte strides
-  if (!ok || re == nullptr || im == nullptr) return;
+  if (!ok) return;
+  for (size_t d = 0; d < dims.size(); ++d) {
+    out.tm_start[d] = dims[d].start;
+    out.tm_len[d] = dims[d].len;
+    out.tm_box[d] = dims[d].tile_len;
+  }
+  out.tm_outer = nob;
+  std::copy(obits, obits + 3, out.tm_obit);
+  if (re == nullptr || im == nullptr) return;  // layout only (no tensor maps)
   static PFN_cuTensorMapEncodeTiled_v12000 encode = [] {
     void* fn = nullptr;
     cudaDriverEntryPointQueryResult q;
@@ -572,8 +591,6 @@ void tile_layout(uint32_t n, const uint32_t (&tbits)[12], float* re, float* im, 
     box[d] = cuuint32_t(1) << dims[d].tile_len;
     estr[d] = 1;
     if (d > 0) strides[d - 1] = (cuuint64_t(1) << dims[d].start) * sizeof(float);
-    out.tm_start[d] = dims[d].start;
-    out.tm_len[d] = dims[d].len;
   }
   float* bases[2] = {re, im};
   bool enc_ok = true;
@@ -620,6 +637,8 @@ static void launch_tc_k(const LaunchEnv& env, float* re, float* im, uint32_t n, 
   }
   p.runbits = lay.runbits;
   p.tm_rank = lay.tm_rank;
+  p.tm_outer = lay.tm_outer;
+  std::copy(lay.tm_obit, lay.tm_obit + 3, p.tm_obit);
   for (int d = 0; d < 5; ++d) {
     p.tm_start[d] = lay.tm_start[d];
     p.tm_len[d] = lay.tm_len[d];
