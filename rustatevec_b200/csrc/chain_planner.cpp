@@ -83,8 +83,11 @@ int tile_pos(const uint32_t (&tb)[12], uint32_t bit) {
 // take the state bits of the tile those vacate: a qubit whose own state bit is among them goes home,
 // qubits already in place stay. State bits 0 and 1 take two qubits of `low` that are columns of
 // the pass's last matrix (`lastcols`) when there are two, so that the kernel's epilogue writes
-// 16-byte vectors. Returns the tile permutation (tile position i -> perm[i]) and updates the layout.
-void relabel(Layout& lay, const uint32_t (&tb)[12], uint64_t low, uint64_t lastcols, uint8_t (&perm)[12]) {
+// 16-byte vectors; among those, preferably two that are both qubits of the next pass's first
+// matrix (`nextfirst`) or both not, so that its operand takes one of the two faster layouts.
+// Returns the tile permutation (tile position i -> perm[i]) and updates the layout.
+void relabel(Layout& lay, const uint32_t (&tb)[12], uint64_t low, uint64_t lastcols, uint64_t nextfirst,
+             uint8_t (&perm)[12]) {
   std::vector<uint32_t> occ(12);
   for (int i = 0; i < 12; ++i) occ[size_t(i)] = lay.log_at[tb[i]];
   std::vector<int> dest(12, -1);
@@ -95,6 +98,15 @@ void relabel(Layout& lay, const uint32_t (&tb)[12], uint64_t low, uint64_t lastc
     if (want_low(i) && ((lastcols >> occ[size_t(i)]) & 1u)) pref.push_back(i);
   for (int i = 2; i < 12; ++i)
     if (want_low(i) && ((lastcols >> occ[size_t(i)]) & 1u)) pref.push_back(i);
+  {
+    std::vector<int> in_first, not_first;
+    for (int i : pref) (((nextfirst >> occ[size_t(i)]) & 1u) ? in_first : not_first).push_back(i);
+    if (in_first.size() >= 2 || not_first.size() >= 2) {
+      // the side whose first pair keeps more qubits already on bits 0, 1 in place
+      auto kept = [](const std::vector<int>& v) { return v.size() >= 2 ? int(v[0] < 2) + int(v[1] < 2) : -1; };
+      pref = kept(in_first) >= kept(not_first) ? in_first : not_first;
+    }
+  }
   if (pref.size() >= 2) {
     for (int k = 0; k < 2; ++k)  // a preferred qubit already on bit 0 or 1 keeps it
       if (pref[size_t(k)] < 2) {
@@ -250,24 +262,23 @@ std::vector<Sweep> plan_chain(const std::vector<Gate>& in, uint32_t n, uint32_t 
   std::vector<size_t> pending(in.size());
   std::iota(pending.begin(), pending.end(), size_t(0));
   std::vector<Sweep> out;
-  while (!pending.empty()) {
-    uint64_t low = 0;
-    for (uint32_t b = 0; b < 6; ++b) low |= 1ull << lay.log_at[b];
-    uint64_t S = low;
+  // A pass's twelve qubits S (the six on state bits 0..5, `low`, then the qubits the pending gates
+  // use soonest, then the lowest state bits), the pending gates it may take (`absorbed`) and its
+  // matrices (window groups, at most max_mats).
+  auto pass_of = [&](uint64_t low, uint64_t& S, std::vector<size_t>& absorbed) {
+    S = low;
     for (size_t i : pending) {
       const uint64_t m = gate_mask(in[i]);
       if (popc(S | m) <= 12) S |= m;
       if (popc(S) == 12) break;
     }
-    // fill: qubits used soonest, then the lowest state bits
     for (size_t i : pending) {
       if (popc(S) == 12) break;
       const Gate& g = in[i];
       for (uint32_t j = 0; j < g.m && popc(S) < 12; ++j) S |= 1ull << g.q[j];
     }
     for (uint32_t b = 6; b < n && popc(S) < 12; ++b) S |= 1ull << lay.log_at[b];
-    // the gates this pass may take, then its matrices
-    std::vector<size_t> absorbed;
+    absorbed.clear();
     uint64_t blocked = 0;
     for (size_t i : pending) {
       const uint64_t m = gate_mask(in[i]);
@@ -276,6 +287,14 @@ std::vector<Sweep> plan_chain(const std::vector<Gate>& in, uint32_t n, uint32_t 
     }
     std::vector<std::vector<size_t>> groups = window_groups(in, absorbed);
     if (groups.size() > max_mats) groups.resize(max_mats);
+    return groups;
+  };
+  while (!pending.empty()) {
+    uint64_t low = 0;
+    for (uint32_t b = 0; b < 6; ++b) low |= 1ull << lay.log_at[b];
+    uint64_t S = 0;
+    std::vector<size_t> absorbed;
+    std::vector<std::vector<size_t>> groups = pass_of(low, S, absorbed);
     std::vector<char> kept(in.size(), 0);
     uint64_t n_gates = 0;
     for (const auto& g : groups)
@@ -345,8 +364,18 @@ std::vector<Sweep> plan_chain(const std::vector<Gate>& in, uint32_t n, uint32_t 
       for (int i = 0; i < 6; ++i) lastrows |= 1ull << lay.log_at[tb[s.chain_rows[s.chain_nmat - 1][i]]];
       lastcols = S & ~lastrows;
     }
-    if (pending.empty()) assign_home(lay, tb, s.chain_perm);  // last pass: towards the identity
-    else relabel(lay, tb, next_low, lastcols, s.chain_perm);
+    if (pending.empty()) {
+      assign_home(lay, tb, s.chain_perm);  // last pass: towards the identity
+    } else {
+      // the next pass's first matrix (before padding), which depends only on next_low and the
+      // pending gates
+      uint64_t S2 = 0, nextfirst = 0;
+      std::vector<size_t> absorbed2;
+      const std::vector<std::vector<size_t>> g2 = pass_of(next_low, S2, absorbed2);
+      if (!g2.empty())
+        for (size_t i : g2[0]) nextfirst |= gate_mask(in[i]);
+      relabel(lay, tb, next_low, lastcols, nextfirst, s.chain_perm);
+    }
     tc_chain_prepare(s);
     out.push_back(std::move(s));
   }
