@@ -38,7 +38,8 @@ WORKLOAD = f"random brickwork {N_QUBITS}q depth {DEPTH}, complex64, Haar SU(2) +
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum, one ncu capture of one launch at 26
 # qubits, scaled by the amplitudes a launch processes) per algorithmic byte, for the kernels the
 # roofline object can name
-TRAFFIC_PER_ALGORITHMIC_BYTE = {"dense_tc": (536.995584 + 477.506560) / 1073.741824,
+TRAFFIC_PER_ALGORITHMIC_BYTE = {"dense_tc": (537.161472 + 476.718592) / 1073.741824,
+                                "tc_chain": (537.134848 + 477.886720) / 1073.741824,
                                 "1q": (536.916992 + 479.222272) / 1073.741824}
 
 
