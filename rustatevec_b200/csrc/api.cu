@@ -110,7 +110,12 @@ void run_sweep(qsvb_ctx* c, qsvb_state* st, const Sweep& s, const void* dev_mat)
   });
 }
 
-qsvb_plan* build_plan(qsvb_ctx* c, const qsvb_circuit* circ, int dtype, const qsvb_plan_opts* opts) {
+// exec_block: the plan is run once and freed by the caller before the context's next call (one-shot
+// execute); its matrices then go into the context's reusable block instead of an allocation of
+// their own, so a one-shot call allocates and frees nothing on the device once the block is large
+// enough (a cudaFree can stall the host for tens to hundreds of milliseconds).
+qsvb_plan* build_plan(qsvb_ctx* c, const qsvb_circuit* circ, int dtype, const qsvb_plan_opts* opts,
+                      bool exec_block) {
   validate_circuit(circ);
   QSVB_REQUIRE(dtype == QSVB_C64 || dtype == QSVB_C128, "dtype must be QSVB_C64 or QSVB_C128");
   std::unique_ptr<qsvb_plan> p(new qsvb_plan);
@@ -131,10 +136,25 @@ qsvb_plan* build_plan(qsvb_ctx* c, const qsvb_circuit* circ, int dtype, const qs
     std::vector<char> host(total, 0);
     for (size_t i = 0; i < p->sweeps.size(); ++i)
       if (sweep_matrix_bytes(p->sweeps[i], dtype)) pack_sweep_matrix(p->sweeps[i], dtype, host.data() + p->mat_offset[i]);
-    QSVB_CK(cudaMalloc(&p->d_mats, total));
-    QSVB_CK(cudaMemcpy(p->d_mats, host.data(), total, cudaMemcpyHostToDevice));
+    if (exec_block) {
+      if (c->exec_mats_cap < total) {
+        QSVB_CK(cudaStreamSynchronize(c->stream));  // the previous call's kernels may still read it
+        if (c->d_exec_mats) QSVB_CK(cudaFree(c->d_exec_mats));
+        c->d_exec_mats = nullptr;
+        c->exec_mats_cap = 0;
+        QSVB_CK(cudaMalloc(&c->d_exec_mats, total));
+        c->exec_mats_cap = total;
+      }
+      p->d_mats = c->d_exec_mats;
+      p->owns_mats = false;
+      // stream-ordered after every earlier use of the block on this context's stream
+      QSVB_CK(cudaMemcpyAsync(p->d_mats, host.data(), total, cudaMemcpyHostToDevice, c->stream));
+      QSVB_CK(cudaStreamSynchronize(c->stream));  // `host` is pageable and about to go away
+    } else {
+      QSVB_CK(cudaMalloc(&p->d_mats, total));
+      QSVB_CK(cudaMemcpy(p->d_mats, host.data(), total, cudaMemcpyHostToDevice));
+    }
   }
-  (void)c;
   return p.release();
 }
 
@@ -179,7 +199,7 @@ void run_plan(qsvb_ctx* c, qsvb_plan* p, qsvb_state* st) {
 void free_plan(qsvb_plan* p) {
   if (!p) return;
   if (p->graph) cudaGraphExecDestroy(p->graph);
-  if (p->d_mats) cudaFree(p->d_mats);
+  if (p->d_mats && p->owns_mats) cudaFree(p->d_mats);
   delete p;
 }
 
@@ -239,6 +259,7 @@ int qsvb_destroy(qsvb_ctx* c) {
     if (c->d_partials) cudaFree(c->d_partials);
     if (c->d_result) cudaFree(c->d_result);
     if (c->d_mat_ring) cudaFree(c->d_mat_ring);
+    if (c->d_exec_mats) cudaFree(c->d_exec_mats);
     if (c->d_prob) cudaFree(c->d_prob);
     if (c->d_err) cudaFree(c->d_err);
     for (int i = 0; i < 2; ++i) {
@@ -382,7 +403,7 @@ int qsvb_plan_create(qsvb_ctx* c, const qsvb_circuit* circ, int dtype, const qsv
     check_ctx(c);
     QSVB_REQUIRE(out != nullptr, "null output pointer");
     DeviceGuard dg(c->device);
-    *out = build_plan(c, circ, dtype, opts);
+    *out = build_plan(c, circ, dtype, opts, false);
   });
 }
 
@@ -479,7 +500,7 @@ int qsvb_execute(qsvb_ctx* c, qsvb_state* s, const qsvb_circuit* circ, const qsv
     QSVB_REQUIRE(circ != nullptr, "null circuit");
     QSVB_REQUIRE(circ->n_qubits == s->n_qubits, "circuit and state qubit counts differ");
     DeviceGuard dg(c->device);
-    std::unique_ptr<qsvb_plan, void (*)(qsvb_plan*)> p(build_plan(c, circ, s->dtype, opts), free_plan);
+    std::unique_ptr<qsvb_plan, void (*)(qsvb_plan*)> p(build_plan(c, circ, s->dtype, opts, true), free_plan);
     run_plan(c, p.get(), s);
     if (stats) *stats = p->stats;
     // the plan's device matrices and graph must outlive the queued work

@@ -195,6 +195,8 @@ struct qsvb_ctx {
   char* d_mat_ring = nullptr;     // per-apply matrix uploads
   size_t mat_ring_cap = 0;
   size_t mat_ring_pos = 0;
+  char* d_exec_mats = nullptr;    // matrix block of one-shot execute calls (grow-only, reused)
+  size_t exec_mats_cap = 0;
   void* d_prob = nullptr;         // probability staging chunk
   size_t prob_cap = 0;
   int* d_err = nullptr;           // device error flag (bounded waits)
@@ -237,6 +239,7 @@ struct qsvb_plan {
   std::vector<size_t> mat_offset;   // byte offset of each sweep's matrix block in d_mats
   char* d_mats = nullptr;
   size_t mats_bytes = 0;
+  bool owns_mats = true;            // false: d_mats is the context's execute block
   qsvb_plan_stats stats{};
   cudaGraphExec_t graph = nullptr;
   void* graph_re = nullptr;         // state the graph was captured for
