@@ -104,11 +104,15 @@ __device__ __forceinline__ uint64_t gstride() { return (uint64_t)gridDim.x * blo
 // ---------------------------------------------------------------------------------------------
 
 // Target bit inside one 16-byte vector: pairs are formed in registers.
-template <class R>
+template <class R, int T>
 __global__ void __launch_bounds__(kThreads) k_pair_invec(R* __restrict__ re, R* __restrict__ im,
-                                                         uint64_t nwork, Enum en, uint32_t t,
-                                                         uint32_t ctrl_low, M2<R> g) {
+                                                         uint64_t nwork, Enum en, uint32_t ctrl_low,
+                                                         M2<R> g) {
+  // the target bit T is a template parameter: with a run-time bit the partner index e | 1 << t
+  // indexes the register array dynamically, which puts it in local memory
   constexpr int N = VecT<R>::N, LOG = VecT<R>::LOG;
+  static_assert(T < LOG, "in-vector target");
+  constexpr uint32_t t = T;
   for (uint64_t w = gtid(); w < nwork; w += gstride()) {
     const uint64_t b = enum_base(w, LOG, en);
     R xr[N], xi[N];
@@ -833,8 +837,9 @@ void launch_pair(const LaunchEnv& env, R* re, R* im, uint32_t n, uint32_t t, con
     if (t < LOG) {
       const uint64_t set = split(LOG, fixed, low);
       const uint64_t nwork = 1ull << (n - LOG - fixed.size());
-      k_pair_invec<R><<<grid_for(nwork, kThreads, env.num_sms), kThreads, 0, env.stream>>>(
-          re, im, nwork, make_enum(fixed, set), t, low, g);
+      auto kern = t == 0 ? k_pair_invec<R, 0> : k_pair_invec<R, LOG - 1>;  // LOG is 1 or 2
+      kern<<<grid_for(nwork, kThreads, env.num_sms), kThreads, 0, env.stream>>>(re, im, nwork, make_enum(fixed, set),
+                                                                             low, g);
     } else if (t < LOG + 5) {
       const uint64_t set = split(LOG + 5, fixed, low);
       const uint64_t nwork = 1ull << (n - LOG - 5 - fixed.size());
