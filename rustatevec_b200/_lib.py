@@ -12,7 +12,9 @@ import os
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libqsvb.so")
+# QSVB_LIBRARY selects another build of the engine, e.g. the bounds-checked libqsvb_checked.so
+# (`make -C rustatevec_b200/csrc BOUNDS=1`)
+LIB_PATH = os.environ.get("QSVB_LIBRARY") or os.path.join(_HERE, "libqsvb.so")
 
 QSVB_OK = 0
 QSVB_E_INVALID = -1

@@ -69,6 +69,8 @@ void sync_and_check(qsvb_ctx* c) {
   QSVB_CK(cudaMemcpy(&flag, c->d_err, sizeof(int), cudaMemcpyDeviceToHost));
   if (flag) {
     QSVB_CK(cudaMemset(c->d_err, 0, sizeof(int)));
+    if (flag & kErrBounds)
+      throw Error(QSVB_E_CUDA, "a device bounds check failed (an index out of its buffer); results are invalid");
     throw Error(QSVB_E_TIMEOUT, "a device-side wait ran out of its iteration budget; results are invalid");
   }
 }
@@ -563,7 +565,7 @@ int qsvb_download(qsvb_ctx* c, const qsvb_state* s, void* re, void* im) {
     const size_t b = state_bytes(s);
     QSVB_CK(cudaMemcpyAsync(re, s->re, b, cudaMemcpyDeviceToHost, c->stream));
     QSVB_CK(cudaMemcpyAsync(im, s->im, b, cudaMemcpyDeviceToHost, c->stream));
-    QSVB_CK(cudaStreamSynchronize(c->stream));
+    sync_and_check(c);  // also reports a failure flagged by earlier device work
   });
 }
 
@@ -576,12 +578,12 @@ int qsvb_amplitude(qsvb_ctx* c, const qsvb_state* s, uint64_t index, double out[
     if (s->dtype == QSVB_C128) {
       QSVB_CK(cudaMemcpyAsync(&out[0], static_cast<double*>(s->re) + index, 8, cudaMemcpyDeviceToHost, c->stream));
       QSVB_CK(cudaMemcpyAsync(&out[1], static_cast<double*>(s->im) + index, 8, cudaMemcpyDeviceToHost, c->stream));
-      QSVB_CK(cudaStreamSynchronize(c->stream));
+      sync_and_check(c);  // also reports a failure flagged by earlier device work
     } else {
       float v[2];
       QSVB_CK(cudaMemcpyAsync(&v[0], static_cast<float*>(s->re) + index, 4, cudaMemcpyDeviceToHost, c->stream));
       QSVB_CK(cudaMemcpyAsync(&v[1], static_cast<float*>(s->im) + index, 4, cudaMemcpyDeviceToHost, c->stream));
-      QSVB_CK(cudaStreamSynchronize(c->stream));
+      sync_and_check(c);  // also reports a failure flagged by earlier device work
       out[0] = v[0];
       out[1] = v[1];
     }
@@ -731,7 +733,7 @@ int qsvb_inner_product(qsvb_ctx* c, const qsvb_state* a, const qsvb_state* b, do
                                         static_cast<const float*>(b->re), static_cast<const float*>(b->im),
                                         a->n_qubits, c->d_partials, c->d_result);
     QSVB_CK(cudaMemcpyAsync(out, c->d_result, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-    QSVB_CK(cudaStreamSynchronize(c->stream));
+    sync_and_check(c);  // also reports a failure flagged by earlier device work
   });
 }
 

@@ -739,6 +739,7 @@ __global__ void __launch_bounds__(NT, MINB)
     const Item item = fixed ? Item{0u, it} : items[it];
     const PassDev& P = passes[item.pass];
     const uint32_t L = P.nlocal, T = 1u << L;
+    [[maybe_unused]] const uint64_t gsize = 1ull << (L + P.nnon);  // the circuit's amplitudes (checked builds)
     if (tid == 0) {
       int ok = *reinterpret_cast<volatile int*>(err) == 0;
       if (ok && P.prev != ~0u) {
@@ -749,7 +750,7 @@ __global__ void __launch_bounds__(NT, MINB)
           while (d.load(cuda::memory_order_acquire) < need) {
             if (clock64() - t0 > budget) {
               ok = 0;
-              atomicExch(err, 1);
+              atomicOr(err, kErrTimeout);
               break;
             }
             if (*reinterpret_cast<volatile int*>(err)) {  // an earlier wait gave up: abandon fast
@@ -781,7 +782,8 @@ __global__ void __launch_bounds__(NT, MINB)
     // item is a tile of the same pass), overlapped with the tile fill
     const uint32_t ph_bytes = P.prog_len * uint32_t(sizeof(Instr));
     const uint32_t co_bytes = (ph_bytes + P.nphase * uint32_t(sizeof(PhaseDev)) + 7u) & ~7u;
-    if (P.staged && staged_pass != item.pass) {
+    if (P.staged && staged_pass != item.pass &&
+        QSVB_BC(co_bytes + P.ncoef * 2u * uint32_t(sizeof(R)) <= (fixed ? kTileStageBytes : kStageBytes), err)) {
       const uint32_t* src0 = reinterpret_cast<const uint32_t*>(prog + P.prog_off);
       const uint32_t* src1 = reinterpret_cast<const uint32_t*>(phases + P.phase_off);
       const uint32_t* src2 = reinterpret_cast<const uint32_t*>(coef + 2 * size_t(P.coef_off));
@@ -821,6 +823,7 @@ __global__ void __launch_bounds__(NT, MINB)
           const uint32_t x = xb + uint32_t(u) * NT * VN;
           if (x < T) {
             const uint64_t a = s_gaddr[x >> 5] | (x & 31u);
+            if (!QSVB_BC(a + VN <= gsize, err)) continue;
             vr[u] = __ldcg(reinterpret_cast<const VT*>(gre + a));
             vi[u] = __ldcg(reinterpret_cast<const VT*>(gim + a));
           }
@@ -830,6 +833,7 @@ __global__ void __launch_bounds__(NT, MINB)
           const uint32_t x = xb + uint32_t(u) * NT * VN;
           if (x < T) {
             const uint32_t y = x ^ s_swz[x >> W];
+            if (!QSVB_BC((y | uint32_t(VN - 1)) < T, err)) continue;
 #pragma unroll
             for (int e = 0; e < VN; ++e) {
               xr[y ^ uint32_t(e)] = Vec16<R>::get(vr[u], e);
@@ -842,6 +846,7 @@ __global__ void __launch_bounds__(NT, MINB)
       for (uint32_t x = tid; x < T; x += NT) {
         const uint64_t a = s_gaddr[x >> 5] | (x & lowmask);
         const uint32_t y = x ^ s_swz[x >> W];
+        if (!QSVB_BC(a < gsize && y < T, err)) continue;
         cp_async_elem(xr + y, gre + a);
         cp_async_elem(xi + y, gim + a);
       }
@@ -910,18 +915,25 @@ __global__ void __launch_bounds__(NT, MINB)
       uint32_t rp[RB];
 #pragma unroll
       for (int j = 0; j < RB; ++j) rp[j] = D.rphys[j];
+      // (checked builds) a group's offsets are XORs of these and of its two table entries, so each
+      // below T keeps every offset in the tile
+      bool rp_ok = true;
+#pragma unroll
+      for (int j = 0; j < RB; ++j) rp_ok = rp_ok && (uint32_t(j) >= D.r || QSVB_BC(rp[j] < T, err));  // bits in use
+      auto grp_ok = [&](uint32_t gi) { return rp_ok && QSVB_BC((uint32_t(D.lo[gi & 31u]) ^ uint32_t(D.hi[gi >> 5])) < T, err); };
       // two groups at a time where the thread has two (independent updates interleave), then one
       const uint32_t ngrp = 1u << nt;
       uint32_t grp = tid;
       if constexpr (GP == 2) {
         for (; grp + NT < ngrp; grp += 2 * NT) {
           const uint32_t gg[2] = {grp, grp + NT};
-          phase_groups<R, RB, 2>(gg, D, rp, xr, xi, pprog, kbeg, kend, pcoef, item.tile, tcoef);
+          if (grp_ok(gg[0]) && grp_ok(gg[1]))
+            phase_groups<R, RB, 2>(gg, D, rp, xr, xi, pprog, kbeg, kend, pcoef, item.tile, tcoef);
         }
       }
       for (; grp < ngrp; grp += NT) {
         const uint32_t gg[1] = {grp};
-        phase_groups<R, RB, 1>(gg, D, rp, xr, xi, pprog, kbeg, kend, pcoef, item.tile, tcoef);
+        if (grp_ok(gg[0])) phase_groups<R, RB, 1>(gg, D, rp, xr, xi, pprog, kbeg, kend, pcoef, item.tile, tcoef);
       }
       k = kend;
       __syncthreads();
@@ -933,8 +945,10 @@ __global__ void __launch_bounds__(NT, MINB)
       double* pout = probs + P.prob_off;
       for (uint32_t x = tid; x < T; x += NT) {
         const uint32_t y = x ^ s_swz[x >> W];
+        const uint64_t pa = s_gaddr[x >> 5] | (x & lowmask);
+        if (!QSVB_BC(pa < gsize && y < T, err)) continue;
         const double p = double(xr[y]) * double(xr[y]) + double(xi[y]) * double(xi[y]);
-        __stcs(pout + (s_gaddr[x >> 5] | (x & lowmask)), p);
+        __stcs(pout + pa, p);
         z += (x & 1u) ? -p : p;
       }
 #pragma unroll
@@ -952,6 +966,7 @@ __global__ void __launch_bounds__(NT, MINB)
       for (uint32_t x = tid * VN; x < T; x += NT * VN) {
         const uint64_t a = s_gaddr[x >> 5] | (x & 31u);
         const uint32_t y = x ^ s_swz[x >> W];
+        if (!QSVB_BC(a + VN <= gsize && (y | uint32_t(VN - 1)) < T, err)) continue;
         VT vr, vi;
 #pragma unroll
         for (int e = 0; e < VN; ++e) {
@@ -965,6 +980,7 @@ __global__ void __launch_bounds__(NT, MINB)
       for (uint32_t x = tid; x < T; x += NT) {
         const uint64_t a = s_gaddr[x >> 5] | (x & lowmask);
         const uint32_t y = x ^ s_swz[x >> W];
+        if (!QSVB_BC(a < gsize && y < T, err)) continue;
         __stcg(gre + a, xr[y]);
         __stcg(gim + a, xi[y]);
       }
@@ -1950,6 +1966,8 @@ void batch_run(qsvb_ctx* c, qsvb_batch* b, double* z0_out, double* probs_out, co
   QSVB_CK(cudaMemcpy(&flag, c->d_err, sizeof(int), cudaMemcpyDeviceToHost));
   if (flag) {
     QSVB_CK(cudaMemset(c->d_err, 0, sizeof(int)));
+    if (flag & kErrBounds)
+      throw Error(QSVB_E_CUDA, "a device bounds check failed (an index out of its buffer); results are invalid");
     throw Error(QSVB_E_TIMEOUT, "a batched-runner dependency wait ran out of its budget; results are invalid");
   }
   if (probs_out) {

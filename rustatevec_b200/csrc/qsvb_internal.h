@@ -15,6 +15,27 @@ namespace qsvb {
 
 using cd = std::complex<double>;
 
+// ------------------------------------------------------------------ device bounds checks
+// The context error flag (int, device memory) collects device-side failures as bits:
+constexpr int kErrTimeout = 1;  // a bounded wait ran out (QSVB_E_TIMEOUT)
+constexpr int kErrBounds = 2;   // a bounds check failed (checked builds only; QSVB_E_CUDA)
+// A build with -DQSVB_BOUNDS_CHECK (`make -C rustatevec_b200/csrc BOUNDS=1`, which writes
+// libqsvb_checked.so) range-checks the table-driven indices of the index-heavy kernels before each
+// access: a failing check sets kErrBounds in the flag and the access is skipped, so a bad index
+// is reported by the next synchronising call instead of touching memory it should not. In the
+// ordinary build QSVB_BC(cond, err) is `true` and `cond` is not evaluated.
+#if defined(__CUDACC__)
+#ifdef QSVB_BOUNDS_CHECK
+__device__ __forceinline__ bool bounds_ok(bool ok, int* err) {
+  if (!ok) atomicOr(err, kErrBounds);
+  return ok;
+}
+#define QSVB_BC(cond, err) ::qsvb::bounds_ok((cond), (err))
+#else
+#define QSVB_BC(cond, err) true
+#endif
+#endif
+
 // ------------------------------------------------------------------ errors
 struct Error : std::runtime_error {
   int code;

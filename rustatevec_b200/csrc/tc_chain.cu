@@ -442,7 +442,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_chain(float* __restrict__ re
     }
     return base;
   };
-  const uint32_t my_tiles =
+  uint32_t my_tiles =  // this CTA's tiles (a role whose checked tables fail sets it to 0)
       uint64_t(blockIdx.x) < ntiles ? uint32_t((ntiles - 1 - blockIdx.x) / gridDim.x + 1) : 0u;
 
   if (warp == kProdWarp) {
@@ -454,7 +454,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_chain(float* __restrict__ re
       if (lane == 0) {
         ok = mbar_wait(&ioempty[slot], par ^ 1u);
         if (ok) mbar_arrive_expect_tx(&iofull[slot], kIoBytes);
-        else atomicExch(err, 1);
+        else atomicOr(err, kErrTimeout);
       }
       ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
       if (!ok) break;
@@ -470,6 +470,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_chain(float* __restrict__ re
       for (uint32_t j = lane; j < nruns; j += 32) {
         const uint32_t t0 = j << rb;
         const uint64_t a = base + s_hioff[t0 >> 6];
+        if (!QSVB_BC(a + (1ull << rb) <= (ntiles << 12), err)) continue;
         bulk_g2s(dre + t0, re + a, run_bytes, &iofull[slot]);
         bulk_g2s(dim_ + t0, im + a, run_bytes, &iofull[slot]);
       }
@@ -484,6 +485,23 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_chain(float* __restrict__ re
     const uint32_t lane_base = tmem + ((quad * 32) << 16);
     uint32_t plan[kVC], plan2[kVC];
     first_plan<BM>(s_dlo, s_dhi, s_tperm, p, tid, lane, plan, plan2);
+    // (checked builds) every staged word, operand offset and accumulator column this thread will
+    // use, once: a converter warp whose tables fail stops, and the pass ends through its bounded
+    // waits
+    bool tables_ok = true;
+#pragma unroll
+    for (int v = 0; v < kVC; ++v)
+      tables_ok = tables_ok && QSVB_BC((plan[v] >> 16) + 4 <= uint32_t(kTileAmps) &&
+                                           (plan[v] & 0xFFFFu) + 8192u + (BM == 2 ? 4u : 8u) <= kBBytes &&
+                                           (BM != 2 || plan2[v] + 8192u + 4u <= kBBytes),
+                                       err);
+    for (uint32_t j = 1; j < nmat; ++j)
+      for (int m = 0; m < 4; ++m) {
+        tables_ok = tables_ok && QSVB_BC(((j == 1 ? rb1 : rb2) ^ p.cchunk[j][half][m]) + 16u <= kBBytes, err);
+        for (int e = 0; e < 8; ++e)
+          tables_ok = tables_ok && QSVB_BC(uint32_t(p.cw[j][half]) + p.cm[j][m] + p.ce[j][e] < 64u, err);
+      }
+    if (!__all_sync(0xffffffffu, tables_ok)) my_tiles = 0;
     uint32_t cpar = 0;  // bit a: parity of the intermediate accumulators of slot a consumed so far
     walk_items<DEPTH>(my_tiles, nmat, [&](uint32_t k, uint32_t j, uint32_t i) -> bool {
       const uint32_t slot = k % NIO, bs = i % NB, bpar = (i / NB) & 1u, a = k % DEPTH;
@@ -500,7 +518,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_chain(float* __restrict__ re
       ready = __shfl_sync(0xffffffffu, ready ? 1 : 0, 0) != 0;
       __syncwarp();
       if (!ready) {
-        atomicExch(err, 1);
+        atomicOr(err, kErrTimeout);
         return false;
       }
       uint8_t* b_hi = bbuf + bs * 2 * kBBytes;
@@ -556,7 +574,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_chain(float* __restrict__ re
         // wait cannot see a phase two ahead)
         const bool ok = mbar_wait(&bfull[bs], (i / NB) & 1u) && mbar_wait(&dfree[a], u ^ 1u);
         if (!__all_sync(0xffffffffu, ok)) {
-          if (leader) atomicExch(err, 1);
+          if (leader) atomicOr(err, kErrTimeout);
           return false;
         }
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -596,6 +614,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_chain(float* __restrict__ re
     const uint32_t row = uint32_t(quad * 32 + lane);
     const uint32_t frow = p.frow[row];
     const bool evec = p.evec != 0;
+    bool tables_ok = true;  // (checked builds) the staging offsets of this thread's row, once
+    for (int q = 0; q < 64; q += evec ? 4 : 1)
+      tables_ok = tables_ok && QSVB_BC((frow ^ uint32_t(p.fcol[q])) + (evec ? 16u : 4u) <= 2u * kTileAmps * 4u, err);
+    if (!named_all(3, kEpiThreads, tables_ok)) my_tiles = 0;
     uint32_t epar = 0;  // bit a: parity of the final accumulators of slot a consumed so far
     walk_items<DEPTH>(my_tiles, nmat, [&](uint32_t k, uint32_t j, uint32_t) -> bool {
       if (j + 1 != nmat) return true;  // items of the earlier matrices belong to the converters
@@ -605,7 +627,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_chain(float* __restrict__ re
       // one decision for all epilogue threads (the barrier also orders every lane after its warp's
       // acquire); reaching it also means every thread's reads of the previous tile's staging are done
       if (!named_all(2, kEpiThreads, ready)) {
-        atomicExch(err, 1);
+        atomicOr(err, kErrTimeout);
         return false;
       }
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -634,6 +656,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_chain(float* __restrict__ re
         const int t = (et + q * kEpiThreads) * 4, tlo = t & 63, thi = t >> 6;
         const uint64_t ad = base + s_hioff[thi] + uint64_t(tlo);
         const uint32_t w = uint32_t(s_sig[tlo]) ^ s_sig[64 + thi];
+        if (!QSVB_BC((evec ? w + 4 <= uint32_t(kTileAmps) : w < uint32_t(kTileAmps)) && ad + 4 <= (ntiles << 12), err))
+          continue;
         float4 xr, xi;
         if (evec) {  // the swizzle keeps bits 0, 1: positions t..t+3 are words w..w+3
           xr = lds128f(st + w * 4u);

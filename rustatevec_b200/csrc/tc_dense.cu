@@ -207,7 +207,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_dense(float* __restrict__ 
     }
     return base;
   };
-  const uint64_t my_tiles = uint64_t(blockIdx.x) < ntiles ? (ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+  // this CTA's tiles (an epilogue whose checked tables fail sets it to 0)
+  uint64_t my_tiles = uint64_t(blockIdx.x) < ntiles ? (ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
 
   if (warp == kProdWarp) {
     // ============================ producer: TMA bulk copies of the tile's contiguous runs
@@ -218,7 +219,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_dense(float* __restrict__ 
       if (lane == 0) {
         ok = mbar_wait_t(&ioempty[slot], par ^ 1u, w0);
         if (ok) mbar_arrive_expect_tx(&iofull[slot], kIoBytes);
-        else atomicExch(err, 1);
+        else atomicOr(err, kErrTimeout);
       }
       ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
       if (!ok) break;
@@ -234,6 +235,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_dense(float* __restrict__ 
       for (uint32_t j = lane; j < nruns; j += 32) {
         const uint32_t t0 = j << rb;
         const uint64_t a = base + s_hioff[t0 >> 6];
+        if (!QSVB_BC(a + (1ull << rb) <= (ntiles << 12), err)) continue;
         bulk_g2s(dre + t0, re + a, run_bytes, &iofull[slot]);
         bulk_g2s(dim_ + t0, im + a, run_bytes, &iofull[slot]);
       }
@@ -245,7 +247,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_dense(float* __restrict__ 
       const uint32_t bs = uint32_t(i & 1), bpar = uint32_t((i >> 1) & 1);
       const bool ready = mbar_wait_t(&iofull[slot], par, w0) && mbar_wait_t(&bfree[bs], bpar ^ 1u, w1);
       if (!__all_sync(0xffffffffu, ready)) {  // warp-uniform exit: the lane-pair mode shuffles
-        atomicExch(err, 1);
+        atomicOr(err, kErrTimeout);
         break;
       }
       const float* sre = io + slot * 2 * kTileAmps;
@@ -259,7 +261,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_dense(float* __restrict__ 
 #pragma unroll
       for (int j = 0; j < kVC; ++j) {
         const uint32_t u = uint32_t(tid + j * kCvtThreads);
-        const int t = int(uint32_t(s_tperm[u & 31u]) | uint32_t(s_tperm[32 + (u >> 5)])) * 4;
+        const int t0 = int(uint32_t(s_tperm[u & 31u]) | uint32_t(s_tperm[32 + (u >> 5)])) * 4;
+        const int t = QSVB_BC(t0 + 4 <= kTileAmps, err) ? t0 : 0;
         tt[j] = t;
         xra[j] = *reinterpret_cast<const float4*>(sre + t);
         xia[j] = *reinterpret_cast<const float4*>(sim + t);
@@ -298,10 +301,12 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_dense(float* __restrict__ 
             split_bf16(wr[e], hr[e], lr[e]);
             split_bf16(wi[e], hm[e], lm[e]);
           }
-          *reinterpret_cast<uint2*>(b_hi + o_re) = pack4(hr);
-          *reinterpret_cast<uint2*>(b_lo + o_re) = pack4(lr);
-          *reinterpret_cast<uint2*>(b_hi + o_im) = pack4(hm);
-          *reinterpret_cast<uint2*>(b_lo + o_im) = pack4(lm);
+          if (QSVB_BC(o_re + 8 <= kBBytes && o_im + 8 <= kBBytes, err)) {
+            *reinterpret_cast<uint2*>(b_hi + o_re) = pack4(hr);
+            *reinterpret_cast<uint2*>(b_lo + o_re) = pack4(lr);
+            *reinterpret_cast<uint2*>(b_hi + o_im) = pack4(hm);
+            *reinterpret_cast<uint2*>(b_lo + o_im) = pack4(lm);
+          }
         } else if constexpr (BM == 2) {
           // exactly one of state bits 0, 1 is a gate bit (the gate's lowest, so row parity): the
           // four amplitudes are two pairs of adjacent rows (K) in two columns, stored as bf16 pairs
@@ -314,6 +319,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_dense(float* __restrict__ 
             const uint32_t kb = (c >> 6) * KR, cl = c & 63u;
             const uint32_t o_re = kmaj_off(cl, kb + s, 64);
             const uint32_t o_im = kmaj_off(cl, kb + M2 + s, 64);
+            if (!QSVB_BC(o_re + 4 <= kBBytes && o_im + 4 <= kBBytes, err)) continue;
             __nv_bfloat16 h0, l0, h1, l1;
             split_bf16(vr[e], h0, l0);
             split_bf16(vr[e + step], h1, l1);
@@ -341,10 +347,12 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_dense(float* __restrict__ 
             split_bf16(vr[e], hr[e], lr[e]);
             split_bf16(vi[e], hm[e], lm[e]);
           }
-          *reinterpret_cast<uint2*>(b_hi + o_re) = pack4(hr);
-          *reinterpret_cast<uint2*>(b_lo + o_re) = pack4(lr);
-          *reinterpret_cast<uint2*>(b_hi + o_im) = pack4(hm);
-          *reinterpret_cast<uint2*>(b_lo + o_im) = pack4(lm);
+          if (QSVB_BC(o_re + 8 <= kBBytes && o_im + 8 <= kBBytes, err)) {
+            *reinterpret_cast<uint2*>(b_hi + o_re) = pack4(hr);
+            *reinterpret_cast<uint2*>(b_lo + o_re) = pack4(lr);
+            *reinterpret_cast<uint2*>(b_hi + o_im) = pack4(hm);
+            *reinterpret_cast<uint2*>(b_lo + o_im) = pack4(lm);
+          }
         }
       }
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -363,7 +371,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_dense(float* __restrict__ 
         const uint32_t bs = uint32_t(i & 1), par = uint32_t((i >> 1) & 1);
         const bool ok = mbar_wait_t(&bfull[bs], par, w0) && mbar_wait_t(&dfree[bs], par ^ 1u, w1);
         if (!__all_sync(0xffffffffu, ok)) {
-          if (leader) atomicExch(err, 1);
+          if (leader) atomicOr(err, kErrTimeout);
           break;
         }
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -401,13 +409,24 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_dense(float* __restrict__ 
     // scalar store, measured 3-6 % faster there; the MN-major instantiations spill with them)
     for (int cb = 0; cb < 4; ++cb)
       sch[cb] = (BM == 0 ? 1u : 4u) * stage_idx(tr ^ uint32_t(s_tcol[blk * 64 + cb * 16]));
+    {
+      // (checked builds) every staging offset of this thread, once; a failing epilogue stops and
+      // the sweep ends through the other roles' bounded waits
+      bool tables_ok = true;
+      for (int cb = 0; cb < 4; ++cb)
+        for (int q = 0; q < 16; ++q)
+          tables_ok = tables_ok && QSVB_BC(BM == 0 ? (q % 4 == 0 ? (sch[cb] ^ p.tcl[q]) + 4 <= uint32_t(kTileAmps) : true)
+                                                   : (sch[cb] ^ p.tclb[q]) + 4 <= uint32_t(kTileAmps) * 4u,
+                                           err);
+      if (!named_all(3, kEpiThreads, tables_ok)) my_tiles = 0;
+    }
     for (uint64_t i = 0; i < my_tiles; ++i) {
       const uint32_t ds = uint32_t(i & 1), dpar = uint32_t((i >> 1) & 1);
       const bool ready = mbar_wait_t(&dfull[ds], dpar, w0);
       // one decision for all epilogue threads (they meet at named barriers below); reaching this
       // barrier also means every thread's reads of the previous tile's staging are done
       if (!named_all(2, kEpiThreads, ready)) {
-        atomicExch(err, 1);
+        atomicOr(err, kErrTimeout);
         break;
       }
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -447,6 +466,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc_dense(float* __restrict__ 
         const int t = (et + j * kEpiThreads) * 4, tlo = t & 63, thi = t >> 6;
         const uint64_t a = base + s_hioff[thi] + uint64_t(tlo);
         const uint32_t si = stage_idx(uint32_t(t));
+        if (!QSVB_BC(a + 4 <= (ntiles << 12), err)) continue;
         __stcs(reinterpret_cast<float4*>(re + a), *reinterpret_cast<const float4*>(sre + si));
         __stcs(reinterpret_cast<float4*>(im + a), *reinterpret_cast<const float4*>(sre + kTileAmps + si));
       }
