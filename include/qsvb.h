@@ -183,6 +183,10 @@ int qsvb_plan_dry_run(const qsvb_circuit* circuit, int dtype, const qsvb_plan_op
                       qsvb_plan_stats* stats);
 
 /* ---------------------------------------------------------------- read-out */
+/* Every read-out call below waits for the context's queued work and reports a failure that work
+ * flagged on the device (a bounded wait that ran out: QSVB_E_TIMEOUT; a failed range check of the
+ * bounds-checked build: QSVB_E_CUDA), as qsvb_synchronize does; the state's contents are then
+ * invalid. */
 /* Backend::download (mod.rs:62; lib.rs:218-227): SoA copy into host buffers of the state's
  * precision. */
 int qsvb_download(qsvb_ctx* ctx, const qsvb_state* st, void* re, void* im);

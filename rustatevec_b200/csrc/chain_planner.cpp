@@ -87,7 +87,7 @@ int tile_pos(const uint32_t (&tb)[12], uint32_t bit) {
 // matrix (`nextfirst`) or both not, so that its operand takes one of the two faster layouts.
 // Returns the tile permutation (tile position i -> perm[i]) and updates the layout.
 void relabel(Layout& lay, const uint32_t (&tb)[12], uint64_t low, uint64_t lastcols, uint64_t nextfirst,
-             uint8_t (&perm)[12]) {
+             uint64_t finished, uint8_t (&perm)[12]) {
   std::vector<uint32_t> occ(12);
   for (int i = 0; i < 12; ++i) occ[size_t(i)] = lay.log_at[tb[i]];
   std::vector<int> dest(12, -1);
@@ -121,6 +121,18 @@ void relabel(Layout& lay, const uint32_t (&tb)[12], uint64_t low, uint64_t lastc
       taken[size_t(t)] = 1;
     }
   }
+  // qubits bound for the high side go to their own state bit when it is a free tile position
+  // (fewer permutation passes at the end): those no pending gate touches first, then the others
+  for (int pass = 0; pass < 2; ++pass)
+    for (int i = 0; i < 12; ++i) {
+      if (dest[size_t(i)] >= 0 || want_low(i)) continue;
+      if ((((finished >> occ[size_t(i)]) & 1u) != 0) != (pass == 0)) continue;
+      const int home = tile_pos(tb, occ[size_t(i)]);
+      if (home >= 6 && !taken[size_t(home)]) {
+        dest[size_t(i)] = home;
+        taken[size_t(home)] = 1;
+      }
+    }
   // qubits already on the right side stay
   for (int i = 0; i < 12; ++i)
     if (dest[size_t(i)] < 0 && want_low(i) == (i < 6) && !taken[size_t(i)]) {
@@ -374,7 +386,9 @@ std::vector<Sweep> plan_chain(const std::vector<Gate>& in, uint32_t n, uint32_t 
       const std::vector<std::vector<size_t>> g2 = pass_of(next_low, S2, absorbed2);
       if (!g2.empty())
         for (size_t i : g2[0]) nextfirst |= gate_mask(in[i]);
-      relabel(lay, tb, next_low, lastcols, nextfirst, s.chain_perm);
+      uint64_t future = 0;  // qubits some pending gate touches
+      for (size_t i : pending) future |= gate_mask(in[i]);
+      relabel(lay, tb, next_low, lastcols, nextfirst, ~future, s.chain_perm);
     }
     tc_chain_prepare(s);
     out.push_back(std::move(s));
