@@ -10,10 +10,10 @@
 // as the single-matrix sweep (tc_dense.cu) does.
 //
 // One persistent CTA per SM, warp-specialised:
-//   producer warp: one tiled TMA or bulk copies per component of each tile into one of four (three)
-//     fp32 input slots (address order);
+//   producer warp: tiled TMA or bulk copies of each tile into one of three fp32 input slots
+//     (address order);
 //   converter warps (8): for a tile's first matrix, split the staged fp32 tile into the bf16 hi/lo
-//     B operand (one of two (three) B buffers; layout chosen by which matrix qubits are state bits
+//     B operand (one of three B buffers; layout chosen by which matrix qubits are state bits
 //     0, 1); for every later matrix, gather 32 of the previous matrix's accumulator columns straight
 //     from tensor memory (each warp its lane quadrant, one column per load, in the order the next
 //     operand needs), split them and write them into the next B operand as 16-byte chunks of 8
@@ -31,9 +31,9 @@
 //     otherwise; a per-pass XOR swizzle keeps both the staging writes and the write-back's reads
 //     bank-conflict free) and write the tile back with 16-byte stores.
 // Work items are (tile, matrix) pairs, walked by every role in the same order (walk_items). Up to
-// two matrices, four tiles are in flight (four accumulators, three B buffers, three MMA warps);
-// three matrices leave tensor memory for two accumulators, so two tiles are (two B buffers, two
-// MMA warps). Every mbarrier wait is bounded (a wait that runs out sets the context error flag,
+// two matrices, four tiles are in flight (four accumulators); three matrices leave tensor memory
+// for two accumulators, so two tiles are. Either way three B buffers rotate over the items, each
+// with its own MMA warp. Every mbarrier wait is bounded (a wait that runs out sets the context error flag,
 // the role stops and the host reports QSVB_E_TIMEOUT). No load uses cluster multicast.
 //
 // k_permute_tiles applies only a tile-qubit permutation (no arithmetic): the planner uses it to put
@@ -70,17 +70,18 @@ constexpr int kEpiWarp0 = kMmaWarp + kMmaWarps;  // warps 12..15 (lane quadrants
 constexpr int kThreads = (kEpiWarp0 + kEpiWarps) * 32;
 constexpr int kTmemCols = 512;             // DEPTH accumulators (64 columns) + (Whi, Wlo) of each matrix
 // Two configurations of the same kernel (template parameter DEPTH = accumulators = tiles in flight):
-//   DEPTH 2 (up to three matrices): 2 B buffers, 4 input slots, matrix j's Whi at column 128 + 128 j;
-//   DEPTH 4 (one or two matrices):  3 B buffers, 3 input slots, matrix j's Whi at column 256 + 128 j.
-// Both use the same shared memory: 2 x 2 + 5 = 3 x 2 + 4 buffers of 32 KB.
+//   DEPTH 2 (up to three matrices): matrix j's Whi at column 128 + 128 j;
+//   DEPTH 4 (one or two matrices):  matrix j's Whi at column 256 + 128 j.
+// Both have 3 B buffers (one MMA warp each) and 3 input slots: 3 x 2 + 3 + 1 buffers of 32 KB with
+// the output staging. With two tiles in flight the third B buffer lets the next wave's first
+// conversion run while the current wave's last MMAs still read the other two.
 constexpr int kBarBase = 26;               // iofull[4] ioempty[4] bfull[3] bfree[3] dfull_c[4] dfull_e[4] dfree[4]
 constexpr uint32_t kBBytes = 128u * 64u * 2u;  // one of Xhi / Xlo: K = 128 rows x N = 64 bf16
 constexpr uint32_t kIoBytes = kTileAmps * 8u;
 constexpr int kVC = kTileAmps / 4 / kCvtThreads;   // float4 per component per converter thread
 constexpr int kVE = kTileAmps / 4 / kEpiThreads;   // float4 per component per epilogue thread
-constexpr size_t kChainSmem = 1024 + 2 * 2 * size_t(kBBytes) + 5 * size_t(kIoBytes) + kBarBase * 8 + 8 + 64 * 8 +
+constexpr size_t kChainSmem = 1024 + 3 * 2 * size_t(kBBytes) + 4 * size_t(kIoBytes) + kBarBase * 8 + 8 + 64 * 8 +
                               64 * 2 * 2 + 64 * 2 + 128 * 2;
-static_assert(2 * 2 * kBBytes + 5 * kIoBytes == 3 * 2 * kBBytes + 4 * kIoBytes, "chain pass: buffer budget");
 static_assert(kChainSmem <= 232448, "chain pass: shared memory above the 227 KB per-block limit");
 static_assert(kChainMaxMats * 128 + 2 * 64 <= kTmemCols && 2 * 128 + 4 * 64 <= kTmemCols, "chain pass: tensor memory");
 
@@ -336,8 +337,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_chain(float* __restrict__ re
                                                           const __grid_constant__ ChainParams p, int* err,
                                                           const __grid_constant__ CUtensorMap tm_re,
                                                           const __grid_constant__ CUtensorMap tm_im) {
-  constexpr int NB = DEPTH == 2 ? 2 : 3;       // B buffers (one MMA warp each)
-  constexpr int NIO = DEPTH == 2 ? 4 : 3;      // input slots
+  constexpr int NB = 3;                        // B buffers (one MMA warp each)
+  constexpr int NIO = 3;                       // input slots
   constexpr uint32_t A0 = 64u * DEPTH;         // tensor-memory column of matrix 0's Whi
   static_assert(A0 + 128u * (DEPTH == 2 ? 3u : 2u) <= uint32_t(kTmemCols), "chain pass: tensor memory");
   extern __shared__ uint8_t smem_raw[];
