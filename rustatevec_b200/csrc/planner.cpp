@@ -91,16 +91,22 @@ bool is_diag(const Gate& g) {
 // Compose `ops` (applied in order) onto the sorted qubit list `q` in FP64: new = E(g) * mat, the
 // embedding qsv's build_fused uses (fusion.rs:102-140). Each gate updates, in place, the 2^m rows
 // it mixes (rows whose indices differ only in the gate's bits), with real and imaginary parts in
-// separate arrays so the column loops vectorise; every product is summed in gate-column order
-// from zero, skipping zero entries.
+// separate arrays; every product is summed in gate-column order from zero, skipping zero entries.
+// A new row is accumulated 8 columns at a time in registers over all of the gate's nonzero
+// entries of that row (the same sums in the same order as one pass per entry, with a third of the
+// loads and stores). An AVX2 clone is chosen at load time where the host has it (no FMA: the
+// same roundings as the baseline build).
+__attribute__((target_clones("avx2", "default")))
 Gate compose(const std::vector<uint32_t>& q, const std::vector<const Gate*>& ops) {
   const size_t m = q.size(), dim = size_t(1) << m;
   std::vector<double> re(dim * dim, 0.0), im(dim * dim, 0.0);  // row-major
   for (size_t i = 0; i < dim; ++i) re[i * dim + i] = 1.0;
   std::vector<double> ore, oim;  // the old values of the rows one gate block mixes
+  std::vector<double> ger, gei;  // per gate row: the nonzero entries, in column order
+  std::vector<uint8_t> gks;      // ... and their columns
   for (const Gate* g : ops) {
     const size_t nsub = size_t(1) << g->m;
-    size_t off[64], gmask = 0;
+    size_t off[64], gmask = 0, nnz[64];
     uint32_t local[6];
     for (uint32_t j = 0; j < g->m; ++j) {
       local[j] = uint32_t(std::find(q.begin(), q.end(), g->q[j]) - q.begin());
@@ -110,6 +116,19 @@ Gate compose(const std::vector<uint32_t>& q, const std::vector<const Gate*>& ops
       size_t o = 0;
       for (uint32_t j = 0; j < g->m; ++j) o |= ((ks >> j) & 1u) << local[j];
       off[ks] = o;
+    }
+    ger.resize(nsub * nsub);
+    gei.resize(nsub * nsub);
+    gks.resize(nsub * nsub);
+    for (size_t rs = 0; rs < nsub; ++rs) {
+      nnz[rs] = 0;
+      for (size_t ks = 0; ks < nsub; ++ks) {
+        const cd e = g->a[rs * nsub + ks];
+        if (e == cd(0, 0)) continue;
+        ger[rs * nsub + nnz[rs]] = e.real();
+        gei[rs * nsub + nnz[rs]] = e.imag();
+        gks[rs * nsub + nnz[rs]++] = uint8_t(ks);
+      }
     }
     ore.resize(nsub * dim);
     oim.resize(nsub * dim);
@@ -122,17 +141,35 @@ Gate compose(const std::vector<uint32_t>& q, const std::vector<const Gate*>& ops
       for (size_t rs = 0; rs < nsub; ++rs) {
         double* __restrict__ dr = &re[(b | off[rs]) * dim];
         double* __restrict__ di = &im[(b | off[rs]) * dim];
-        std::fill_n(dr, dim, 0.0);
-        std::fill_n(di, dim, 0.0);
-        for (size_t ks = 0; ks < nsub; ++ks) {
-          const cd e = g->a[rs * nsub + ks];
-          if (e == cd(0, 0)) continue;
-          const double er = e.real(), ei = e.imag();
-          const double* __restrict__ sr = &ore[ks * dim];
-          const double* __restrict__ si = &oim[ks * dim];
+        const double* er = &ger[rs * nsub];
+        const double* ei = &gei[rs * nsub];
+        const uint8_t* kk = &gks[rs * nsub];
+        if (dim >= 8) {
+          for (size_t c0 = 0; c0 < dim; c0 += 8) {
+            double ar[8] = {}, ai[8] = {};
+            for (size_t t = 0; t < nnz[rs]; ++t) {
+              const double* __restrict__ sr = &ore[kk[t] * dim + c0];
+              const double* __restrict__ si = &oim[kk[t] * dim + c0];
+              const double xr = er[t], xi = ei[t];
+              for (int j = 0; j < 8; ++j) {
+                ar[j] += xr * sr[j] - xi * si[j];
+                ai[j] += xr * si[j] + xi * sr[j];
+              }
+            }
+            for (int j = 0; j < 8; ++j) {
+              dr[c0 + j] = ar[j];
+              di[c0 + j] = ai[j];
+            }
+          }
+        } else {
           for (size_t c = 0; c < dim; ++c) {
-            dr[c] += er * sr[c] - ei * si[c];
-            di[c] += er * si[c] + ei * sr[c];
+            double ar = 0.0, ai = 0.0;
+            for (size_t t = 0; t < nnz[rs]; ++t) {
+              ar += er[t] * ore[kk[t] * dim + c] - ei[t] * oim[kk[t] * dim + c];
+              ai += er[t] * oim[kk[t] * dim + c] + ei[t] * ore[kk[t] * dim + c];
+            }
+            dr[c] = ar;
+            di[c] = ai;
           }
         }
       }
@@ -382,14 +419,15 @@ Sweep classify_gate(const Gate& g) {
   for (uint32_t i = 0; i < g.m; ++i) order[i] = i;
   std::sort(order, order + g.m, [&](uint32_t a, uint32_t b) { return g.q[a] < g.q[b]; });
   for (uint32_t i = 0; i < g.m; ++i) s.q[i] = g.q[order[i]];
-  auto remap = [&](size_t sidx) {  // sorted-order index -> gate-order index
+  size_t remap[64];  // sorted-order index -> gate-order index
+  for (size_t sidx = 0; sidx < d; ++sidx) {
     size_t o = 0;
     for (uint32_t i = 0; i < g.m; ++i) o |= ((sidx >> i) & 1u) << order[i];
-    return o;
-  };
+    remap[sidx] = o;
+  }
   s.mat.resize(d * d);
   for (size_t r = 0; r < d; ++r)
-    for (size_t c = 0; c < d; ++c) s.mat[r * d + c] = at(remap(r), remap(c));
+    for (size_t c = 0; c < d; ++c) s.mat[r * d + c] = at(remap[r], remap[c]);
   return s;
 }
 
