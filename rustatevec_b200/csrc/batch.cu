@@ -55,7 +55,10 @@ constexpr int kMaxLocal = 14;
 constexpr int kMaxHi = 512;                   // 2^(kMaxLocal - 5): entries of the address / swizzle tables
 constexpr long long kSpinBudget = 1ll << 32;  // default dependency-wait budget, clock64 cycles (about 2 s)
 constexpr uint32_t kStageBytes = 32768;       // shared memory for one pass's program
-constexpr uint32_t kTileStageBytes = 16384;   // the same for tile sweeps (four blocks per SM)
+// The same for tile sweeps: small enough for five blocks per SM (larger programs are read from
+// global memory through L1).
+constexpr uint32_t kTileStageBytes = 8192;
+constexpr int kTileHi = 128;  // address / swizzle table entries of tile sweeps (<= 12 local bits)
 
 // OP_D1T: a diagonal on one register bit whose two entries depend on one bit of the tile index
 // (a 2-qubit diagonal with one qubit outside the tile); OP_DT: a phase that depends only on tile
@@ -698,7 +701,9 @@ __device__ __forceinline__ void phase_groups(const uint32_t* grp, const PhaseDev
   }
 }
 
-template <class R, int RB, int W, int NT, int MINB = 1, int GP = 1>
+// HI: entries of the address and swizzle tables (2^(lbits - 5) and 2^(lbits - W) at most); tile
+// sweeps take a smaller table, which leaves room for one more block per SM.
+template <class R, int RB, int W, int NT, int MINB = 1, int GP = 1, int HI = kMaxHi>
 __global__ void __launch_bounds__(NT, MINB)
     k_batch(const Item* __restrict__ items, uint32_t nitems, const PassDev* __restrict__ passes,
             const PhaseDev* __restrict__ phases, const Instr* __restrict__ prog, const R* __restrict__ coef,
@@ -711,8 +716,8 @@ __global__ void __launch_bounds__(NT, MINB)
   uint8_t* stage = reinterpret_cast<uint8_t*>(xi + (size_t(1) << lbits));  // the pass's program
   // per-tile phase coefficients (tile sweeps; sits right after the program staging area)
   R* tcoef = reinterpret_cast<R*>(stage + (fixed ? kTileStageBytes : kStageBytes));
-  __shared__ uint64_t s_gaddr[kMaxHi];
-  __shared__ uint16_t s_swz[kMaxHi];
+  __shared__ uint64_t s_gaddr[HI];
+  __shared__ uint16_t s_swz[HI];
   __shared__ uint32_t s_item;
   __shared__ double s_red[NT / 32];
   __shared__ int s_ok;
@@ -725,7 +730,7 @@ __global__ void __launch_bounds__(NT, MINB)
     uint32_t v = 0;
     for (int i = 0; i < int(lbits) - W; ++i)
       if ((h >> i) & 1u) v ^= swz_col(W + i, W);
-    s_swz[h] = uint16_t(v);
+    if (QSVB_BC(h < uint32_t(HI), err)) s_swz[h] = uint16_t(v);
   }
   long long t_wait = 0, t_fill = 0, t_gates = 0, t_out = 0, n_items = 0, t_mark = prof ? clock64() : 0;
   uint32_t staged_pass = ~0u;
@@ -772,7 +777,7 @@ __global__ void __launch_bounds__(NT, MINB)
       for (uint32_t h = tid; h < (1u << nhi); h += NT) {
         uint64_t a = base;
         for (uint32_t j = 0; j < nhi; ++j) a |= uint64_t((h >> j) & 1u) << P.local[5 + j];
-        s_gaddr[h] = a;
+        if (QSVB_BC(h < uint32_t(HI), err)) s_gaddr[h] = a;
       }
     }
     __syncthreads();
@@ -2043,7 +2048,7 @@ void free_batch(qsvb_batch* b) { delete b; }
 namespace qsvb {
 
 uint32_t tile_local_bits(int dtype, uint32_t n) {
-  const uint32_t lmax = batch_max_local_bits(dtype) - 2;  // a quarter of the shared memory: four blocks per SM
+  const uint32_t lmax = batch_max_local_bits(dtype) - 2;  // a 32 KB tile: five blocks per SM
   if (n >= lmax + 8) return lmax;  // at least 256 tiles to spread over the SMs
   if (n >= 15) return n - 8;
   return 0;
@@ -2056,7 +2061,10 @@ constexpr size_t kTileSmemMax = (size_t(2) * 4 << 12) + kTileStageBytes + kTphSl
 
 template <class R, int RB, int NT, int MINB, int GP>
 void launch_tile_variant(const LaunchEnv& e, R* re, R* im, const Sweep& s, const uint8_t* base) {
-  auto fn = k_batch<R, RB, sizeof(R) == 8 ? 4 : 5, NT, MINB, GP>;
+  constexpr int W = sizeof(R) == 8 ? 4 : 5;
+  auto fn = k_batch<R, RB, W, NT, MINB, GP, kTileHi>;
+  QSVB_REQUIRE(s.tile_lbits <= 12 && (1u << (s.tile_lbits - uint32_t(W))) <= uint32_t(kTileHi),
+               "tile sweep wider than its address tables");
   static std::once_flag once;
   std::call_once(once, [&] {
     QSVB_CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kTileSmemMax)));
@@ -2324,9 +2332,11 @@ void launch_tile(const LaunchEnv& e, R* re, R* im, uint32_t n, const Sweep& s, c
   QSVB_REQUIRE(dev_blob != nullptr && !s.tile_blob.empty(), "tile sweep without a program");
   QSVB_REQUIRE(n >= s.tile_lbits, "tile sweep larger than the state");
   const uint8_t* base = static_cast<const uint8_t*>(dev_blob);
-  // four blocks per SM (some stream their tiles while others compute): <= 128 registers a thread
-  if constexpr (sizeof(R) == 8) launch_tile_variant<double, 3, 128, 4, 1>(e, re, im, s, base);
-  else launch_tile_variant<float, 4, 128, 4, 1>(e, re, im, s, base);
+  // five blocks per SM (some stream their tiles while others compute; the gates' register phases
+  // and shared-memory round trips are latency-bound, so warps per SM set the pace): <= 102
+  // registers a thread, the 8 KB program stage and 128-entry address tables
+  if constexpr (sizeof(R) == 8) launch_tile_variant<double, 3, 128, 5, 1>(e, re, im, s, base);
+  else launch_tile_variant<float, 4, 128, 5, 1>(e, re, im, s, base);
 }
 
 template void launch_tile<float>(const LaunchEnv&, float*, float*, uint32_t, const Sweep&, const void*);
