@@ -6,11 +6,11 @@
 
 #include <algorithm>
 #include <cstring>
-#include <thread>
-#include <cstring>
+#include <future>
 #include <memory>
 #include <new>
 #include <string>
+#include <thread>
 
 #include "cost_model.h"
 #include "qsvb_internal.h"
@@ -136,8 +136,22 @@ qsvb_plan* build_plan(qsvb_ctx* c, const qsvb_circuit* circ, int dtype, const qs
   p->mats_bytes = total;
   if (total) {
     std::vector<char> host(total, 0);
-    for (size_t i = 0; i < p->sweeps.size(); ++i)
-      if (sweep_matrix_bytes(p->sweeps[i], dtype)) pack_sweep_matrix(p->sweeps[i], dtype, host.data() + p->mat_offset[i]);
+    // each sweep packs into its own range (the tensor-core bf16 hi/lo images take about 50 us a
+    // matrix): large plans pack on several host threads
+    auto pack_range = [&](size_t lo, size_t hi) {
+      for (size_t i = lo; i < hi; ++i)
+        if (sweep_matrix_bytes(p->sweeps[i], dtype)) pack_sweep_matrix(p->sweeps[i], dtype, host.data() + p->mat_offset[i]);
+    };
+    const size_t ns = p->sweeps.size();
+    const size_t nth = std::min<size_t>({size_t(std::max(1u, std::thread::hardware_concurrency())), size_t(8), ns});
+    if (total < (size_t(1) << 20) || nth < 2) {
+      pack_range(0, ns);
+    } else {
+      std::vector<std::future<void>> fut;
+      for (size_t t = 1; t < nth; ++t) fut.push_back(std::async(std::launch::async, pack_range, ns * t / nth, ns * (t + 1) / nth));
+      pack_range(0, ns / nth);
+      for (auto& f : fut) f.get();
+    }
     if (exec_block) {
       if (c->exec_mats_cap < total) {
         QSVB_CK(cudaStreamSynchronize(c->stream));  // the previous call's kernels may still read it

@@ -183,7 +183,8 @@ Gate compose(const std::vector<uint32_t>& q, const std::vector<const Gate*>& ops
   return out;
 }
 
-// A group of diagonal gates composed as the product of their diagonals (O(2^m) per gate).
+// A group of diagonal gates composed as the product of their diagonals (O(2^m) per gate), kept as
+// the diagonal alone (candidate costing only needs its classification).
 Gate compose_diag(const std::vector<uint32_t>& q, const std::vector<const Gate*>& ops) {
   const size_t m = q.size(), dim = size_t(1) << m;
   std::vector<cd> d(dim, cd(1, 0));
@@ -201,8 +202,8 @@ Gate compose_diag(const std::vector<uint32_t>& q, const std::vector<const Gate*>
   Gate out;
   out.m = uint32_t(m);
   for (size_t j = 0; j < m; ++j) out.q[j] = q[j];
-  out.a.assign(dim * dim, cd(0, 0));
-  for (size_t r = 0; r < dim; ++r) out.a[r * dim + r] = d[r];
+  out.a = std::move(d);
+  out.diag_only = true;
   return out;
 }
 
@@ -364,20 +365,21 @@ Sweep classify_gate(const Gate& g) {
   s.n_gates = 1;
   const size_t d = size_t(1) << g.m;
   auto at = [&](size_t r, size_t c) { return g.a[r * d + c]; };
-  if (is_diag(g)) {
+  if (g.diag_only || is_diag(g)) {
+    auto dg = [&](size_t i) { return g.diag_only ? g.a[i] : at(i, i); };
     bool ident = true;
-    for (size_t i = 0; i < d; ++i) ident = ident && at(i, i) == cd(1, 0);
+    for (size_t i = 0; i < d; ++i) ident = ident && dg(i) == cd(1, 0);
     if (ident) {
       s.kind = SK_NONE;
       return s;
     }
     s.kind = SK_DIAG;
     s.mat.resize(d);
-    for (size_t i = 0; i < d; ++i) s.mat[i] = at(i, i);
+    for (size_t i = 0; i < d; ++i) s.mat[i] = dg(i);
     for (uint32_t j = 0; j < g.m; ++j) {  // qubit j is skippable when its 0-half is all ones
       bool ok = true;
       for (size_t i = 0; i < d && ok; ++i)
-        if (((i >> j) & 1) == 0 && at(i, i) != cd(1, 0)) ok = false;
+        if (((i >> j) & 1) == 0 && dg(i) != cd(1, 0)) ok = false;
       if (ok) s.ctrl[s.nctrl++] = g.q[j];
     }
     return s;

@@ -74,7 +74,8 @@ constexpr int kChainMaxMats = 3;
 struct Gate {  // host copy of an input gate, FP64
   uint32_t m = 0;
   uint32_t q[6] = {0, 0, 0, 0, 0, 0};
-  std::vector<cd> a;  // row-major 2^m x 2^m
+  std::vector<cd> a;  // row-major 2^m x 2^m (diag_only: the 2^m diagonal entries)
+  bool diag_only = false;  // a diagonal group composed only for costing (classify_gate reads it)
 };
 
 struct PhaseTerm {
