@@ -398,7 +398,7 @@ def run_gpu(args):
             "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": {"value": round(e2e, 6), "unit": "s", "h2d_bytes_per_step": pc_bytes, "d2h_bytes_per_step": 16,
-                    "path": "B200Backend.run(host circuit) -> qsvb_execute (plan + matrix upload + graph) -> "
+                    "path": "B200Backend.run(host circuit) -> qsvb_execute (plan + matrix upload + sweeps) -> "
                             "expectation_z(mask=1) read back"},
             "gpu_launches": n_launch,
             "clocks": clk,

@@ -88,7 +88,7 @@ typedef struct qsvb_plan_opts {
   uint32_t planner;          /* qsvb_planner */
   uint32_t max_fused_qubits; /* fusion width cap, 1..6 (ignored by AS_GIVEN) */
   uint32_t engine;           /* qsvb_engine */
-  uint32_t use_graph;        /* capture the sweep sequence in a CUDA graph */
+  uint32_t use_graph;        /* reusable plans: capture the sweep sequence in a CUDA graph */
   uint32_t chain_max_matrices; /* QSVB_PLAN_CHAIN: matrices per pass, 1..3 (0: chosen by cost) */
   uint32_t reserved[3];
 } qsvb_plan_opts;
@@ -138,8 +138,9 @@ int qsvb_init_gaussian(qsvb_ctx* ctx, qsvb_state* st, uint64_t seed);
 int qsvb_apply(qsvb_ctx* ctx, qsvb_state* st, const double* matrix, const uint32_t* qubits,
                uint32_t n_qubits);
 /* Backend::execute (mod.rs:66-73) on an initialised state: plans, uploads matrices once, and
- * queues every sweep (as one CUDA graph when opts->use_graph). opts may be NULL (greedy, k=4,
- * auto engine, graph on). stats may be NULL. */
+ * launches every sweep directly (use_graph applies to reusable plans: a graph instantiated for a
+ * single run would only hold back the first kernel). opts may be NULL (greedy, k=4, auto
+ * engine). stats may be NULL. */
 int qsvb_execute(qsvb_ctx* ctx, qsvb_state* st, const qsvb_circuit* circuit,
                  const qsvb_plan_opts* opts, qsvb_plan_stats* stats);
 

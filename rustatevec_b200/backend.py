@@ -10,10 +10,10 @@ trait method              here
 ``apply(s, gate, qs)``    ``qsvb_apply`` (diagonal / butterfly / controlled / dense fast paths)
 ``amplitude(s, i)``       ``qsvb_amplitude`` (one element, not the whole state)
 ``probabilities(s)``      ``qsvb_probabilities`` (FP64 on device, returned in R)
-``sample(s, shots, rng)`` trait default: host alias table over ``probabilities`` (sample.rs:107-111)
+``sample(s, shots, rng)`` ``qsvb_sample``: inverse-CDF draws on the device (cdf_sample, sample.rs:163-172)
 ``expectation_z(s, m)``   ``qsvb_expectation_z`` (FP64 on device)
 ``download(s)``           ``qsvb_download`` -> host ``StateVector``
-``execute(circuit)``      alloc + init_basis(0) + ``qsvb_execute`` (planned, CUDA graph)
+``execute(circuit)``      alloc + init_basis(0) + ``qsvb_execute`` (planned, sweeps launched directly)
 ========================  ============================================================
 
 ``R`` is chosen per backend instance: ``B200Backend(precision="f64")`` serves complex128 states

@@ -517,6 +517,8 @@ int qsvb_execute(qsvb_ctx* c, qsvb_state* s, const qsvb_circuit* circ, const qsv
     QSVB_REQUIRE(circ->n_qubits == s->n_qubits, "circuit and state qubit counts differ");
     DeviceGuard dg(c->device);
     std::unique_ptr<qsvb_plan, void (*)(qsvb_plan*)> p(build_plan(c, circ, s->dtype, opts, true), free_plan);
+    // one run: launched directly, so the first sweep starts while later ones are still queued
+    p->opts.use_graph = 0;
     run_plan(c, p.get(), s);
     if (stats) *stats = p->stats;
     // the plan's device matrices and graph must outlive the queued work
