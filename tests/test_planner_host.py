@@ -80,17 +80,20 @@ def test_dry_run_rejects_bad_input(built):
 
 def test_chain_planner_passes(built):
     """PLAN_CHAIN: brickwork 30q depth 20 in far fewer passes than one sweep per fused 6-qubit
-    block; the layout is restored by a few permutation passes; other states plan as WINDOW."""
+    block; the layout is restored by a few permutation passes; other states plan as WINDOW.
+    The pass counts are those of the current planner (qubits bound for a tile's high side go to
+    their own state bit when it is free): 63 + 3, 37 + 2 and 27 + 3 chain + permutation passes
+    at one, two and three matrices a pass."""
     c = brickwork(30, 20, 0)
     win = dry(c, L.PLAN_WINDOW, 6)
-    for mats, most in ((1, 70), (2, 45), (3, 35)):
+    for mats, most, perm in ((1, 63, 3), (2, 37, 2), (3, 27, 3)):
         st = L.PlanStats()
         pc = L.PackedCircuit(c)
         o = L.make_opts(L.PLAN_CHAIN, 6, L.ENGINE_AUTO, chain_max_matrices=mats)
         L.check(L.lib().qsvb_plan_dry_run(pc.ref(), L.C64, C.byref(o), C.byref(st)))
         d = st.to_dict()
         assert set(d["by_kind"]) <= {"tc_chain", "permute"}, d
-        assert d["by_kind"]["tc_chain"] <= most and d["by_kind"].get("permute", 0) <= 6, d
+        assert d["by_kind"]["tc_chain"] <= most and d["by_kind"].get("permute", 0) <= perm, d
         assert d["n_sweeps"] < win["n_sweeps"] or mats == 1
     assert "tc_chain" not in dry(c, L.PLAN_CHAIN, 6, dtype=L.C128)["by_kind"]
     assert "tc_chain" not in dry(random_circuit(11, 60, 1), L.PLAN_CHAIN, 6)["by_kind"]
