@@ -288,14 +288,9 @@ std::vector<Gate> learned_fuse(const std::vector<Gate>& seg, uint32_t n, const q
   };
   const size_t ncand = 2 * size_t(cap);
   std::vector<double> secs(ncand, 1e300);
-  if (seg.size() >= 64) {
-    std::vector<std::future<double>> fut;
-    for (size_t c = 0; c < ncand; ++c)
-      fut.push_back(std::async(std::launch::async, candidate, int(c / cap), uint32_t(c % cap) + 1));
-    for (size_t c = 0; c < ncand; ++c) secs[c] = fut[c].get();
-  } else {
-    for (size_t c = 0; c < ncand; ++c) secs[c] = candidate(int(c / cap), uint32_t(c % cap) + 1);
-  }
+  parallel_ranges(ncand, seg.size() >= 64 ? 1 : SIZE_MAX, [&](size_t lo, size_t hi) {
+    for (size_t c = lo; c < hi; ++c) secs[c] = candidate(int(c / cap), uint32_t(c % cap) + 1);
+  });
   size_t best = 0;
   for (size_t c = 1; c < ncand; ++c)
     if (secs[c] < secs[best]) best = c;  // ties keep the earlier (greedy, narrower) candidate

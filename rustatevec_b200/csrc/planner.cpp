@@ -29,6 +29,8 @@
 
 namespace qsvb {
 
+thread_local uint32_t g_plan_threads = 0;
+
 qsvb_plan_opts default_opts() {
   qsvb_plan_opts o{};
   o.planner = QSVB_PLAN_GREEDY;
@@ -239,15 +241,7 @@ std::vector<Gate> emit_groups(const std::vector<std::vector<const Gate*>>& group
   auto range = [&](size_t lo, size_t hi) {
     for (size_t i = lo; i < hi; ++i) out[i] = make_group(groups[i], cost_only);
   };
-  const size_t nth = std::min<size_t>(std::max(1u, std::thread::hardware_concurrency()), 16);
-  if (cost_only || groups.size() < 32 || nth == 1) {
-    range(0, groups.size());
-    return out;
-  }
-  std::vector<std::future<void>> fut;
-  for (size_t t = 0; t < nth; ++t)
-    fut.push_back(std::async(std::launch::async, range, groups.size() * t / nth, groups.size() * (t + 1) / nth));
-  for (auto& f : fut) f.get();
+  parallel_ranges(groups.size(), cost_only ? SIZE_MAX : 32, range);
   return out;
 }
 
@@ -468,16 +462,24 @@ std::vector<Sweep> plan_sweeps(const std::vector<Gate>& in, uint32_t n, const qs
   if (o.planner != QSVB_PLAN_LEARNED) return plan_with(in, n, o, dtype, false, TILE_NO);
   // learned: merging long diagonal runs into phase-polynomial sweeps, and running gate runs as
   // tile passes, are candidate choices weighed by predicted time
-  // the four candidates are independent: plan them on separate host threads
+  // the candidates are independent: plan them on separate host threads, each with its share of
+  // the host's threads for its own parallel loops
+  const bool with_chain = chain_ok && n >= 14;
+  const size_t ncand = 4 + (with_chain ? size_t(kChainMaxMats) - 1 : 0);
+  const uint32_t share = uint32_t(std::max<size_t>(1, plan_thread_budget() / ncand));
   std::vector<std::future<std::vector<Sweep>>> fut;
   for (int c = 0; c < 4; ++c)
     fut.push_back(std::async(std::launch::async, [&, c] {
+      g_plan_threads = share;
       return plan_with(in, n, o, dtype, (c & 1) == 0, c < 2 ? TILE_NO : TILE_CHOOSE);
     }));
   // chain passes (complex64 on the tensor cores, states of >= 14 qubits) at 2 and 3 matrices a pass
-  if (chain_ok && n >= 14)
+  if (with_chain)
     for (uint32_t m = 2; m <= uint32_t(kChainMaxMats); ++m)
-      fut.push_back(std::async(std::launch::async, [&, m] { return plan_chain(in, n, m); }));
+      fut.push_back(std::async(std::launch::async, [&, m] {
+        g_plan_threads = share;
+        return plan_chain(in, n, m);
+      }));
   std::vector<Sweep> best;
   double best_t = 1e300;
   for (size_t c = 0; c < fut.size(); ++c) {
@@ -528,6 +530,7 @@ void tile_segment(const std::vector<Gate>& seg, uint32_t n, const qsvb_plan_opts
     return;
   }
   std::vector<Gate> pend;
+  std::vector<Sweep> passes;  // the tile passes of one run of gates, in order
   auto flush = [&] {
     std::vector<char> done(pend.size(), 0);
     size_t first = 0;
@@ -560,20 +563,33 @@ void tile_segment(const std::vector<Gate>& seg, uint32_t n, const qsvb_plan_opts
           blocked |= m;
         }
       }
-      if (mode == TILE_CHOOSE) {
-        std::vector<Sweep> alt = fused_sweeps(t.tile_gates, n, o, dtype);
-        select_engines(alt, n, o, dtype);
-        tile_prepare(t, n, dtype);
-        if (predict_plan_seconds(alt, n, dtype) <= predict_sweep_seconds(t, n, dtype)) {
-          append(std::move(alt));
-          continue;
-        }
-      } else {
-        tile_prepare(t, n, dtype);
-      }
-      out.push_back(std::move(t));
+      passes.push_back(std::move(t));
     }
     pend.clear();
+    // A pass's gates do not depend on how earlier passes were run, so each pass is prepared (and,
+    // with TILE_CHOOSE, weighed against the fused sweeps of its gates) on its own: long runs of
+    // passes spread over host threads, and the results are appended in pass order.
+    std::vector<std::vector<Sweep>> res(passes.size());
+    auto work = [&](size_t lo, size_t hi) {
+      for (size_t i = lo; i < hi; ++i) {
+        Sweep& t = passes[i];
+        if (mode == TILE_CHOOSE) {
+          std::vector<Sweep> alt = fused_sweeps(t.tile_gates, n, o, dtype);
+          select_engines(alt, n, o, dtype);
+          tile_prepare(t, n, dtype);
+          if (predict_plan_seconds(alt, n, dtype) <= predict_sweep_seconds(t, n, dtype)) {
+            res[i] = std::move(alt);
+            continue;
+          }
+        } else {
+          tile_prepare(t, n, dtype);
+        }
+        res[i].push_back(std::move(t));
+      }
+    };
+    parallel_ranges(passes.size(), 4, work);
+    passes.clear();
+    for (auto& r : res) append(std::move(r));
   };
   for (const Gate& g : seg) {
     if (g.m <= 2) {
@@ -589,15 +605,17 @@ void tile_segment(const std::vector<Gate>& seg, uint32_t n, const qsvb_plan_opts
 std::vector<Sweep> plan_with(const std::vector<Gate>& in, uint32_t n, const qsvb_plan_opts& o, int dtype,
                              bool phase_runs, TileMode tile) {
 
-  // split into segments: phase-polynomial runs vs ordinary gates
-  std::vector<Sweep> out;
+  // split into segments: phase-polynomial runs vs ordinary gates. Segments are planned
+  // independently (on several host threads when there are many) and concatenated in order.
+  struct Part {
+    std::vector<Gate> seg;  // gates to fuse / tile, or
+    Sweep phase;            // a ready phase-polynomial sweep (seg empty)
+  };
+  std::vector<Part> parts;
   auto run_segment = [&](const std::vector<Gate>& seg) {
     if (seg.empty()) return;
-    if (tile != TILE_NO) {
-      tile_segment(seg, n, o, dtype, tile, out);
-      return;
-    }
-    for (Sweep& s : fused_sweeps(seg, n, o, dtype)) out.push_back(std::move(s));
+    parts.emplace_back();
+    parts.back().seg = seg;
   };
   std::vector<Gate> seg;
   size_t i = 0;
@@ -621,7 +639,8 @@ std::vector<Sweep> plan_with(const std::vector<Gate>& in, uint32_t n, const qsvb
           for (size_t e = 0; e < 4; ++e) t.ang[e] = e < d ? std::arg(g.a[e * d + e]) : 0.0;
           s.terms.push_back(t);
         }
-        out.push_back(std::move(s));
+        parts.emplace_back();
+        parts.back().phase = std::move(s);
         i = j;
         continue;
       }
@@ -633,6 +652,22 @@ std::vector<Sweep> plan_with(const std::vector<Gate>& in, uint32_t n, const qsvb
   }
   run_segment(seg);
 
+  std::vector<std::vector<Sweep>> res(parts.size());
+  auto work = [&](size_t lo, size_t hi) {
+    for (size_t k = lo; k < hi; ++k) {
+      if (parts[k].seg.empty()) {
+        res[k].push_back(std::move(parts[k].phase));
+      } else if (tile != TILE_NO) {
+        tile_segment(parts[k].seg, n, o, dtype, tile, res[k]);
+      } else {
+        res[k] = fused_sweeps(parts[k].seg, n, o, dtype);
+      }
+    }
+  };
+  parallel_ranges(parts.size(), 4, work);
+  std::vector<Sweep> out;
+  for (auto& r : res)
+    for (Sweep& s : r) out.push_back(std::move(s));
   select_engines(out, n, o, dtype);
   return out;
 }

@@ -3,10 +3,13 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <complex>
 #include <cstdint>
+#include <future>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/qsvb.h"
@@ -132,6 +135,39 @@ Sweep classify_gate(const Gate& g);
 // The product of `ops` (applied in order) on the qubit list q (index bit j <-> q[j]), in FP64.
 Gate compose_gates(const std::vector<uint32_t>& q, const std::vector<const Gate*>& ops);
 uint64_t gate_mask(const Gate& g);
+
+// Host threads for planning. A thread's budget (0: the host's hardware threads, at most 16) caps
+// the threads its parallel loops take; the threads a loop spawns, and the calling thread while it
+// runs its share, have a budget of one, so loops nested inside them run serially. The learned
+// planner gives each candidate plan's thread its share of the host.
+extern thread_local uint32_t g_plan_threads;
+inline size_t plan_thread_budget() {
+  if (g_plan_threads) return g_plan_threads;
+  return std::min<size_t>(std::max(1u, std::thread::hardware_concurrency()), 16);
+}
+// fn(lo, hi) over [0, n) split into contiguous ranges, on up to plan_thread_budget() threads when
+// n >= min_items (else in the calling thread). Ranges are independent: results must not depend on
+// the split.
+template <class F> void parallel_ranges(size_t n, size_t min_items, F&& fn) {
+  const size_t nth = std::min(plan_thread_budget(), n);
+  if (n < min_items || nth < 2) {
+    fn(size_t(0), n);
+    return;
+  }
+  auto run = [&fn](size_t lo, size_t hi) {
+    g_plan_threads = 1;
+    fn(lo, hi);
+  };
+  std::vector<std::future<void>> fut;
+  for (size_t k = 1; k < nth; ++k) fut.push_back(std::async(std::launch::async, run, n * k / nth, n * (k + 1) / nth));
+  struct Restore {
+    uint32_t v;
+    ~Restore() { g_plan_threads = v; }
+  } restore{g_plan_threads};
+  g_plan_threads = 1;
+  fn(size_t(0), n / nth);
+  for (auto& f : fut) f.get();
+}
 // Tensor-core chain passes with qubit relabelling, then the permutation passes that restore every
 // qubit to its own state bit (chain_planner.cpp). max_mats: matrices per pass (1..3).
 std::vector<Sweep> plan_chain(const std::vector<Gate>& in, uint32_t n, uint32_t max_mats);
