@@ -97,7 +97,7 @@ bool is_diag(const Gate& g) {
 // A new row is accumulated 8 columns at a time in registers over all of the gate's nonzero
 // entries of that row (the same sums in the same order as one pass per entry, with a third of the
 // loads and stores). An AVX2 clone is chosen at load time where the host has it (no FMA: the
-// same roundings as the baseline build).
+// same roundings as the default SSE2 clone).
 __attribute__((target_clones("avx2", "default")))
 Gate compose(const std::vector<uint32_t>& q, const std::vector<const Gate*>& ops) {
   const size_t m = q.size(), dim = size_t(1) << m;
